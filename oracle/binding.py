@@ -1,0 +1,232 @@
+"""ctypes binding of the CPU checkers (TEST INFRASTRUCTURE).
+
+Used only by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference arm:
+  * liboracle.so          -- the plain-C restatement of the reference CPU L-BFGS-B
+                             (lbfgsb_oracle.c) with a per-iteration trace;
+  * _ref/libref_lbfgsb.so -- the reference's own culbfgsb/lbfgsbcpu.cpp built from the
+                             reference sources (Makefile here), the pin for the restatement.
+Both run the synthetic objective of objective.c on host arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libref_lbfgsb.so")
+
+
+class SummaryF64(C.Structure):
+    _fields_ = [("residual_g", C.c_double), ("residual_f", C.c_double),
+                ("residual_x", C.c_double), ("num_iteration", C.c_int), ("info", C.c_int)]
+
+
+class SummaryF32(C.Structure):
+    _fields_ = [("residual_g", C.c_float), ("residual_f", C.c_float),
+                ("residual_x", C.c_float), ("num_iteration", C.c_int), ("info", C.c_int)]
+
+
+class OptionF64(C.Structure):
+    _fields_ = [("machine_epsilon", C.c_double), ("machine_maximum", C.c_double),
+                ("step_scaling", C.c_double), ("eps_g", C.c_double), ("eps_f", C.c_double),
+                ("eps_x", C.c_double), ("hessian_approximate_dimension", C.c_int),
+                ("max_iteration", C.c_int)]
+
+
+class OptionF32(C.Structure):
+    _fields_ = [("machine_epsilon", C.c_float), ("machine_maximum", C.c_float),
+                ("step_scaling", C.c_float), ("eps_g", C.c_float), ("eps_f", C.c_float),
+                ("eps_x", C.c_float), ("hessian_approximate_dimension", C.c_int),
+                ("max_iteration", C.c_int)]
+
+
+class TraceRec(C.Structure):
+    _fields_ = [("iter", C.c_int), ("nint", C.c_int), ("nbreak", C.c_int), ("nfree", C.c_int),
+                ("nenter", C.c_int), ("nleave", C.c_int), ("col", C.c_int), ("head", C.c_int),
+                ("nfgv", C.c_int), ("ifun", C.c_int), ("iword", C.c_int), ("reset", C.c_int),
+                ("free_hash", C.c_ulonglong), ("at_lower", C.c_ulonglong),
+                ("at_upper", C.c_ulonglong), ("f", C.c_double), ("theta", C.c_double),
+                ("stp", C.c_double), ("dtm", C.c_double), ("tsum", C.c_double),
+                ("gd", C.c_double), ("gdold", C.c_double), ("dtd", C.c_double),
+                ("stpmx", C.c_double)]
+
+
+CB64 = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                   C.POINTER(C.c_double), C.POINTER(SummaryF64))
+CB32 = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                   C.POINTER(C.c_float), C.POINTER(SummaryF32))
+TRACE_CB = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(TraceRec))
+
+_TRACE_KEYS = [f for f, _ in TraceRec._fields_]
+
+
+def build(reference_dir: str | None = None, quiet: bool = True) -> None:
+    """Build liboracle.so, and the reference build when the reference tree is present."""
+    cmd = ["make", "-C", HERE, os.path.join(HERE, "liboracle.so")]
+    subprocess.run(cmd, check=True, capture_output=quiet)
+    ref_dir = reference_dir or "/root/reference"
+    if os.path.isfile(os.path.join(ref_dir, "culbfgsb", "lbfgsbcpu.cpp")):
+        subprocess.run(["make", "-C", HERE, "ref", f"REFERENCE_DIR={ref_dir}"], check=True,
+                       capture_output=quiet)
+
+
+_libs: dict[str, C.CDLL] = {}
+
+
+def _load(path: str) -> C.CDLL:
+    if path not in _libs:
+        if not os.path.exists(path):
+            build()
+        lib = C.CDLL(path)
+        _libs[path] = lib
+    return _libs[path]
+
+
+def oracle_lib() -> C.CDLL:
+    lib = _load(ORACLE_SO)
+    for sfx, opt, summ, cb in (("f64", OptionF64, SummaryF64, CB64),
+                               ("f32", OptionF32, SummaryF32, CB32)):
+        fn = getattr(lib, f"orc_lbfgsb_minimize_{sfx}")
+        fn.restype = None
+        real = C.c_double if sfx == "f64" else C.c_float
+        fn.argtypes = [C.c_int, C.POINTER(real), C.POINTER(C.c_int), C.POINTER(real),
+                       C.POINTER(real), C.POINTER(opt), cb, cb, cb, C.c_void_p, TRACE_CB,
+                       C.c_void_p, C.POINTER(summ)]
+    return lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib() -> C.CDLL:
+    lib = _load(REF_SO)
+    for sfx, opt, summ, cb in (("f64", OptionF64, SummaryF64, CB64),
+                               ("f32", OptionF32, SummaryF32, CB32)):
+        fn = getattr(lib, f"ref_lbfgsb_minimize_{sfx}")
+        fn.restype = None
+        real = C.c_double if sfx == "f64" else C.c_float
+        fn.argtypes = [C.c_int, C.POINTER(real), C.POINTER(C.c_int), C.POINTER(real),
+                       C.POINTER(real), C.POINTER(opt), cb, cb, cb, C.c_void_p,
+                       C.POINTER(summ)]
+    return lib
+
+
+def default_option(dtype) -> C.Structure:
+    """lbfgsbdefaultoption (culbfgsb/lbfgsb.cpp:43-66)."""
+    if np.dtype(dtype) == np.float64:
+        o = OptionF64(1e-15, np.finfo(np.float64).max, 1.0, 1e-15, 1e-15, 1e-15, 8, 1000)
+    else:
+        o = OptionF32(1e-8, np.finfo(np.float32).max, 1.0, 1e-15, 1e-15, 1e-15, 8, 1000)
+    return o
+
+
+@dataclass
+class RunResult:
+    x: np.ndarray
+    info: int
+    num_iteration: int
+    residual_g: float
+    residual_f: float
+    residual_x: float
+    evals: list = field(default_factory=list)    # (f, x-digest) at every funcgrad call
+    iters: list = field(default_factory=list)    # summary at every after-iteration call
+    trace: list = field(default_factory=list)    # oracle trace records (dicts)
+
+
+def _digest(a: np.ndarray) -> str:
+    import hashlib
+    return hashlib.sha1(np.ascontiguousarray(a).tobytes()).hexdigest()[:16]
+
+
+def host_objective(prob: dict, dtype):
+    """Host objective callback body for a problem dict: (xp, fp, gp) pointers -> fills f, g.
+
+    prob["kind"] == "synth" (default): the grid objective of objective.c with fields
+    kappa, w, t, b; "quad": the separable quadratic with vectors a, c."""
+    lib = _load(ORACLE_SO)
+    is64 = np.dtype(dtype) == np.float64
+    real = C.c_double if is64 else C.c_float
+    sfx = "f64" if is64 else "f32"
+    kind = prob.get("kind", "synth")
+    names = ("kappa", "w", "t", "b") if kind == "synth" else ("a", "c")
+    arrs = [np.ascontiguousarray(prob[k], dtype=np.float64) for k in names]
+    ptrs = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in arrs]
+    fn = getattr(lib, f"orc_{kind}_eval_{sfx}")
+    fn.restype = None
+    fn.argtypes = [C.c_int] + [C.POINTER(C.c_double)] * len(arrs) + [C.POINTER(real)] * 3
+    lead = int(prob["s"]) if kind == "synth" else int(prob["nbd"].size)
+
+    def evaluate_ptr(xp, fp, gp):
+        fn(lead, *ptrs, xp, fp, gp)
+
+    evaluate_ptr.keepalive = arrs  # type: ignore[attr-defined]
+    return evaluate_ptr
+
+
+def run_cpu(which: str, prob: dict, dtype=np.float64, x0=None, option=None, record=True,
+            trace=False, custom_stop_at: int | None = None) -> RunResult:
+    """Run the oracle ('oracle') or the reference build ('ref') on a synthetic problem."""
+    dtype = np.dtype(dtype)
+    is64 = dtype == np.float64
+    real = C.c_double if is64 else C.c_float
+    cbt = CB64 if is64 else CB32
+    summ = SummaryF64() if is64 else SummaryF32()
+    n = prob["nbd"].size
+    x = np.zeros(n, dtype=dtype) if x0 is None else np.array(x0, dtype=dtype)
+    l = np.ascontiguousarray(prob["l"], dtype=dtype)
+    u = np.ascontiguousarray(prob["u"], dtype=dtype)
+    nbd = np.ascontiguousarray(prob["nbd"], dtype=np.int32)
+    opt = option if option is not None else default_option(dtype)
+    ev = host_objective(prob, dtype)
+    res = RunResult(x=x, info=0, num_iteration=0, residual_g=0, residual_f=0, residual_x=0)
+
+    def fg(user, xp, fp, gp, sp):
+        ev(xp, fp, gp)
+        if record:
+            xa = np.ctypeslib.as_array(xp, shape=(n,))
+            res.evals.append((float(fp[0]), _digest(xa)))
+        return 0
+
+    def after(user, xp, fp, gp, sp):
+        if record:
+            s = sp[0]
+            res.iters.append((s.num_iteration, float(s.residual_g), float(s.residual_f),
+                              float(s.residual_x), float(fp[0])))
+        return 0
+
+    def stop(user, xp, fp, gp, sp):
+        return 1 if (custom_stop_at is not None and sp[0].num_iteration >= custom_stop_at) else 0
+
+    cb_fg, cb_after = cbt(fg), cbt(after)
+    cb_stop = cbt(stop) if custom_stop_at is not None else cbt()
+
+    def tr(user, recp):
+        r = recp[0]
+        res.trace.append({k: getattr(r, k) for k in _TRACE_KEYS})
+
+    sfx = "f64" if is64 else "f32"
+    P = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
+    if which == "oracle":
+        fn = getattr(oracle_lib(), f"orc_lbfgsb_minimize_{sfx}")
+        cb_tr = TRACE_CB(tr) if trace else TRACE_CB()
+        fn(n, P(x, real), P(nbd, C.c_int), P(l, real), P(u, real), C.byref(opt), cb_fg,
+           cb_after, cb_stop, None, cb_tr, None, C.byref(summ))
+    elif which == "ref":
+        fn = getattr(ref_lib(), f"ref_lbfgsb_minimize_{sfx}")
+        fn(n, P(x, real), P(nbd, C.c_int), P(l, real), P(u, real), C.byref(opt), cb_fg,
+           cb_after, cb_stop, None, C.byref(summ))
+    else:
+        raise ValueError(which)
+    res.x = x
+    res.info = summ.info
+    res.num_iteration = summ.num_iteration
+    res.residual_g = float(summ.residual_g)
+    res.residual_f = float(summ.residual_f)
+    res.residual_x = float(summ.residual_x)
+    return res

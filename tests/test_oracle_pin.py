@@ -1,0 +1,79 @@
+"""The oracle is pinned to the reference before anything is checked against it.
+
+1. Against the golden fixtures recorded from the reference's own CPU L-BFGS-B
+   (tests/golden/golden.json, made by tests/golden/make_golden.py from
+   culbfgsb/lbfgsbcpu.cpp): every funcgrad point (f and the bytes of x), every
+   after-iteration summary, the exit code and the final x must match bit for bit.
+2. Against the live reference build (oracle/_ref/libref_lbfgsb.so) on further seeds and
+   sizes, when that build is present.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import binding as B
+from cases import CASES, apply_options, make_case
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(HERE, "golden", "golden.json")
+GOLDEN_X = os.path.join(HERE, "golden", "golden_x.npz")
+
+
+@pytest.fixture(scope="module")
+def golden():
+    with open(GOLDEN) as fh:
+        return json.load(fh), np.load(GOLDEN_X)
+
+
+def _run(which, name, trace=False):
+    prob, dtype, x0, over, stop = make_case(name)
+    opt = apply_options(B.default_option(dtype), over)
+    return B.run_cpu(which, prob, dtype, x0=x0, option=opt, custom_stop_at=stop, trace=trace)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_matches_reference_golden(golden, name):
+    gj, gx = golden
+    g = gj[name]
+    r = _run("oracle", name)
+    assert r.info == g["info"]
+    assert r.num_iteration == g["num_iteration"]
+    assert [list(e) for e in r.evals] == [list(e) for e in g["evals"]]
+    assert [list(e) for e in r.iters] == [list(e) for e in g["iters"]]
+    assert hashlib.sha1(r.x.tobytes()).hexdigest()[:16] == g["x_sha1"]
+    np.testing.assert_array_equal(r.x, gx[name])
+    assert r.residual_g == g["residual_g"]
+
+
+def test_golden_covers_the_walk_and_errors(golden):
+    """The fixture set exercises breakpoint walks, truncated subspace steps, the
+    entering/leaving corrections and every exit code the CPU path produces."""
+    gj, _ = golden
+    infos = {gj[c]["info"] for c in CASES}
+    assert {-1, 0, 1, 4, 5} <= infos
+    tr = _run("oracle", "synth_s64_f64_b001", trace=True).trace
+    assert max(t["nint"] for t in tr) > 10
+    assert sum(t["iword"] == 1 for t in tr) > 10
+    assert sum(t["nenter"] for t in tr) > 0 and sum(t["nleave"] for t in tr) > 0
+
+
+@pytest.mark.skipif(not B.ref_available(), reason="reference build not present")
+@pytest.mark.parametrize("s,seed,bound,dtype", [
+    (24, 21, 0.015, np.float64), (24, 22, 0.015, np.float32), (40, 23, 1.0, np.float64),
+    (40, 24, 0.03, np.float64), (48, 25, 0.01, np.float32)])
+def test_oracle_matches_live_reference(s, seed, bound, dtype):
+    import synth
+    prob = synth.synth_problem(s, seed=seed)
+    prob["l"] = prob["l"] * bound
+    prob["u"] = prob["u"] * bound
+    opt = B.default_option(dtype)
+    opt.eps_f = opt.eps_g = opt.eps_x = 1e-8
+    a = B.run_cpu("ref", prob, dtype, option=opt)
+    b = B.run_cpu("oracle", prob, dtype, option=opt)
+    assert a.evals == b.evals
+    assert a.iters == b.iters
+    np.testing.assert_array_equal(a.x, b.x)
+    assert a.info == b.info
