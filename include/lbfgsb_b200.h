@@ -1,0 +1,199 @@
+/*
+ * lbfgsb_b200.h -- C ABI of the B200 (sm_100a) L-BFGS-B library (liblbfgsb_b200.so).
+ *
+ * The entry points take plain pointers and sizes.  Vectors x, l, u and the int array nbd
+ * are DEVICE pointers of length n, as in the reference's LCM_CUDA mode (README "Usage";
+ * culbfgsb.h:157-163).  Streams are passed as void* (a cudaStream_t; NULL is the legacy
+ * default stream, which is what the reference uses).  The C++ drop-in surface of the
+ * reference (culbfgsb.h: LBFGSB_CUDA_OPTION/STATE/SUMMARY, lbfgsbcuda::lbfgsbminimize,
+ * lbfgsbdefaultoption) is include/culbfgsb.h, a header-only adapter over these calls.
+ *
+ * Return value of every lbfgsb_b200_* call: an LBFGSB_B200_* status.  The optimisation
+ * outcome is summary->info with the reference's codes (culbfgsb.h:131-138):
+ *   -2 abnormal termination in the line search, -1 wrong parameters (also: mode
+ *   LCM_NO_ACCELERATION, which this GPU-only library does not provide), 0 stopped by the
+ *   user's stopping callback, 1 relative decrease of f <= eps_f, 2 step <= eps_x,
+ *   4 projected gradient <= eps_g, 5 iteration limit.
+ * Unlike the reference's GPU driver (lbfgsbcuda.cpp:393, which forces info = 0), info
+ * reports the real reason the solve stopped, as the reference's CPU driver does.
+ */
+#ifndef LBFGSB_B200_H_
+#define LBFGSB_B200_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBFGSB_B200_OK 0
+#define LBFGSB_B200_ERR_ARGUMENT 1   /* null pointer or unsupported mode */
+#define LBFGSB_B200_ERR_CUDA 2       /* a CUDA call failed; see lbfgsb_b200_last_error() */
+#define LBFGSB_B200_ERR_CALLBACK 3   /* reserved */
+
+/* culbfgsb.h:31 */
+#define LBFGSB_B200_MODE_NO_ACCELERATION 0
+#define LBFGSB_B200_MODE_CUDA 1
+
+/* LBFGSB_CUDA_OPTION<double> (culbfgsb.h:33-44), same field order and layout. */
+typedef struct {
+  double machine_epsilon;
+  double machine_maximum;
+  double step_scaling;
+  double eps_g;
+  double eps_f;
+  double eps_x;
+  int hessian_approximate_dimension;
+  int max_iteration;
+  int mode;
+} lbfgsb_b200_option_f64;
+
+typedef struct {
+  float machine_epsilon;
+  float machine_maximum;
+  float step_scaling;
+  float eps_g;
+  float eps_f;
+  float eps_x;
+  int hessian_approximate_dimension;
+  int max_iteration;
+  int mode;
+} lbfgsb_b200_option_f32;
+
+/* LBFGSB_CUDA_SUMMARY<real> (culbfgsb.h:46-53). */
+typedef struct {
+  double residual_g;
+  double residual_f;
+  double residual_x;
+  int num_iteration;
+  int info;
+} lbfgsb_b200_summary_f64;
+
+typedef struct {
+  float residual_g;
+  float residual_f;
+  float residual_x;
+  int num_iteration;
+  int info;
+} lbfgsb_b200_summary_f32;
+
+/* The callbacks of LBFGSB_CUDA_STATE (culbfgsb.h:55-67) with a user pointer: x and g are
+ * device pointers of length n, f is a host scalar, stream is the solver's stream.
+ * funcgrad fills *f and g at x; its return value is ignored, as in the reference.
+ * customized_stopping returning nonzero stops the solve with info = 0.  Callbacks other
+ * than funcgrad must not modify x or g. */
+typedef int (*lbfgsb_b200_callback_f64)(void* user, double* x, double* f, double* g,
+                                        void* stream, const lbfgsb_b200_summary_f64* summary);
+typedef int (*lbfgsb_b200_callback_f32)(void* user, float* x, float* f, float* g,
+                                        void* stream, const lbfgsb_b200_summary_f32* summary);
+
+/* lbfgsbdefaultoption (culbfgsb/lbfgsb.cpp:43-66). */
+void lbfgsb_b200_default_option_f64(lbfgsb_b200_option_f64* option);
+void lbfgsb_b200_default_option_f32(lbfgsb_b200_option_f32* option);
+
+/* lbfgsbcuda::lbfgsbminimize<double|float> with mode LCM_CUDA (culbfgsb.h:157-163,
+ * dispatch lbfgsb.cpp:24-42, driver lbfgsbcuda.cpp:39-441).  The iteration follows the
+ * reference's L-BFGS-B 2.1 algorithm as implemented in lbfgsbcpu.cpp:117-465 (full
+ * breakpoint walk for the Cauchy point, subspace step truncated at the first bound).
+ * x is updated in place with the final iterate.  after_iteration and
+ * customized_stopping may be NULL.  The workspace (about 6 vectors of n reals, 18 of n
+ * history elements, n bytes + n bits) is allocated on `stream` for the duration of the
+ * call. */
+int lbfgsb_b200_minimize_f64(int n, double* x, const int* nbd, const double* l,
+                             const double* u, const lbfgsb_b200_option_f64* option,
+                             lbfgsb_b200_callback_f64 funcgrad,
+                             lbfgsb_b200_callback_f64 after_iteration,
+                             lbfgsb_b200_callback_f64 customized_stopping, void* user,
+                             void* stream, lbfgsb_b200_summary_f64* summary);
+int lbfgsb_b200_minimize_f32(int n, float* x, const int* nbd, const float* l, const float* u,
+                             const lbfgsb_b200_option_f32* option,
+                             lbfgsb_b200_callback_f32 funcgrad,
+                             lbfgsb_b200_callback_f32 after_iteration,
+                             lbfgsb_b200_callback_f32 customized_stopping, void* user,
+                             void* stream, lbfgsb_b200_summary_f32* summary);
+
+/* ---- extensions (no counterpart in the reference) ---------------------------------- */
+
+/* One record per accepted iteration, mirroring the CPU oracle's trace: the state the step
+ * was computed from (col, head, theta, Cauchy-point and free-set statistics) and the
+ * line-search outcome. */
+typedef struct {
+  int iter, nint, nbreak, nfree, nenter, nleave, col, head, nfgv, ifun, iword, reset;
+  unsigned long long free_hash, at_lower, at_upper;
+  double f, theta, stp, dtm, tsum, gd, gdold, dtd, stpmx;
+  double f1_0, f2_0;  /* Cauchy f' and f'' before the first breakpoint */
+  double dbg[8];      /* p(1), p(col+1), c(1), c(col+1), (Mc)(1), (Mc)(col+1), sy(1,1), wt(1,1) */
+} lbfgsb_b200_trace_record;
+typedef void (*lbfgsb_b200_trace_callback)(void* user, const lbfgsb_b200_trace_record* rec);
+
+/* Precision forms of the f32 entry point:
+ *   0 plain f32 (vectors, history and scalars in float, like the reference's float path)
+ *   1 mixed: f32 vectors and history, f64 small-matrix, Cauchy and line-search scalars
+ *   2 mixed with bf16 history storage */
+#define LBFGSB_B200_FORM_PLAIN 0
+#define LBFGSB_B200_FORM_MIXED 1
+#define LBFGSB_B200_FORM_MIXED_BF16 2
+
+typedef struct {
+  int form;                           /* f32 entry point only */
+  int profile;                        /* 1: time every kernel with CUDA events */
+  lbfgsb_b200_trace_callback trace;   /* may be NULL */
+  void* trace_user;
+} lbfgsb_b200_ext;
+
+int lbfgsb_b200_minimize_ext_f64(int n, double* x, const int* nbd, const double* l,
+                                 const double* u, const lbfgsb_b200_option_f64* option,
+                                 lbfgsb_b200_callback_f64 funcgrad,
+                                 lbfgsb_b200_callback_f64 after_iteration,
+                                 lbfgsb_b200_callback_f64 customized_stopping, void* user,
+                                 void* stream, const lbfgsb_b200_ext* ext,
+                                 lbfgsb_b200_summary_f64* summary);
+int lbfgsb_b200_minimize_ext_f32(int n, float* x, const int* nbd, const float* l,
+                                 const float* u, const lbfgsb_b200_option_f32* option,
+                                 lbfgsb_b200_callback_f32 funcgrad,
+                                 lbfgsb_b200_callback_f32 after_iteration,
+                                 lbfgsb_b200_callback_f32 customized_stopping, void* user,
+                                 void* stream, const lbfgsb_b200_ext* ext,
+                                 lbfgsb_b200_summary_f32* summary);
+
+/* Statistics of the calling thread's last solve. */
+#define LBFGSB_B200_MAX_KERNELS 16
+typedef struct {
+  int kernels;                       /* number of named kernels below */
+  char name[LBFGSB_B200_MAX_KERNELS][32];
+  long long launches[LBFGSB_B200_MAX_KERNELS];
+  double ms[LBFGSB_B200_MAX_KERNELS];  /* summed CUDA-event time (profile = 1 only) */
+  double bytes[LBFGSB_B200_MAX_KERNELS];  /* algorithmic DRAM bytes of one launch */
+  long long total_launches;          /* all kernels the solver launched */
+  long long host_syncs;              /* stream synchronisations of the solver */
+  long long evaluations;             /* funcgrad calls */
+  double bytes_per_iteration_model;  /* algorithmic bytes of one steady-state iteration */
+} lbfgsb_b200_stats;
+int lbfgsb_b200_last_stats(lbfgsb_b200_stats* out);
+
+/* Message of the last LBFGSB_B200_ERR_CUDA on the calling thread ("" if none). */
+const char* lbfgsb_b200_last_error(void);
+
+/* ---- synthetic objective (test and benchmark glue, no reference counterpart) ---------
+ * f(x) = sum_k 0.5*kappa_k*((x_{i+1,j}-x_k)^2 + (x_{i,j+1}-x_k)^2)
+ *      + h^2 * sum_k [w_k*softplus(x_k - t_k) - b_k*x_k + 0.05*cos(3*x_k)]
+ * on an s x s grid (k = j*s + i, h = 1/(s+1), zero Dirichlet neighbours).  Fields are
+ * given as host double arrays of length s*s.  The returned handle is the `user` pointer
+ * of the matching funcgrad callback, which computes g on the device and f (deterministic
+ * order, accumulated in double) and synchronises the stream to return f on the host. */
+void* lbfgsb_b200_synth_create(int s, const double* kappa, const double* w, const double* t,
+                               const double* b, int single_precision_fields);
+void lbfgsb_b200_synth_destroy(void* handle);
+int lbfgsb_b200_synth_funcgrad_f64(void* handle, double* x, double* f, double* g, void* stream,
+                                   const lbfgsb_b200_summary_f64* summary);
+int lbfgsb_b200_synth_funcgrad_f32(void* handle, float* x, float* f, float* g, void* stream,
+                                   const lbfgsb_b200_summary_f32* summary);
+
+/* Plain blocking copies for bindings without their own CUDA runtime (kind: 1 host to
+ * device, 2 device to host, 3 device to device). */
+int lbfgsb_b200_copy(void* dst, const void* src, size_t bytes, int kind);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LBFGSB_B200_H_ */

@@ -1,0 +1,623 @@
+// driver.cu -- host driver and C ABI of the sm_100a L-BFGS-B library.
+//
+// The outer loop restates the reference's CPU driver (culbfgsb/lbfgsbcpu.cpp:117-465)
+// over the device passes of passes.cuh / walk.cuh.  All solver state stays on the
+// device; the host reads a small control header twice per iteration: once after the
+// subspace step (to call the user's funcgrad at the trial point) and once after each
+// function evaluation (the line-search decision and the stopping-test quantities).  The
+// reference's GPU driver synchronises about 15 times and launches 30-60 kernels and
+// cuBLAS/Thrust calls per iteration (lbfgsbcuda.cpp:212-390); this one launches 5.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/lbfgsb_b200.h"
+#include "passes.cuh"
+#include "walk.cuh"
+
+namespace lbfgsb_b200 {
+
+thread_local std::string g_last_error;
+thread_local lbfgsb_b200_stats g_last_stats;
+
+struct CudaFailure {
+  cudaError_t err;
+  const char* call;
+  int line;
+};
+#define CK(call)                                              \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) throw CudaFailure{e_, #call, __LINE__}; \
+  } while (0)
+
+enum KernelId {
+  KID_INIT,
+  KID_PROJGR,
+  KID_BEGIN,
+  KID_GCP,
+  KID_WALK_GATHER,
+  KID_WALK,
+  KID_FREEV,
+  KID_SUBDIR,
+  KID_SUBAPPLY,
+  KID_TRIAL,
+  KID_POST,
+  KID_COUNT
+};
+static const char* kKernelNames[KID_COUNT] = {
+    "k_init",      "k_projgr",    "k_begin_iteration", "k_gcp_scan",
+    "k_walk_gather", "k_walk",    "k_freev_formk",     "k_subsm_dir",
+    "k_subsm_apply", "k_trial",   "k_post_eval"};
+
+template <typename R>
+struct Api;
+template <>
+struct Api<double> {
+  using Opt = lbfgsb_b200_option_f64;
+  using Sum = lbfgsb_b200_summary_f64;
+  using Cb = lbfgsb_b200_callback_f64;
+};
+template <>
+struct Api<float> {
+  using Opt = lbfgsb_b200_option_f32;
+  using Sum = lbfgsb_b200_summary_f32;
+  using Cb = lbfgsb_b200_callback_f32;
+};
+
+// Launch bookkeeping: counts every launch, and with profiling brackets it with events.
+class Launcher {
+ public:
+  Launcher(cudaStream_t s, bool profile) : s_(s), profile_(profile) {
+    std::fill(count_, count_ + KID_COUNT, 0LL);
+  }
+  ~Launcher() {
+    for (auto& e : pool_) cudaEventDestroy(e);
+  }
+  template <typename F>
+  void run(int kid, F&& launch) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (profile_) {
+      a = event();
+      b = event();
+      CK(cudaEventRecord(a, s_));
+    }
+    launch();
+    CK(cudaGetLastError());
+    if (profile_) {
+      CK(cudaEventRecord(b, s_));
+      timed_.push_back({kid, a, b});
+    }
+    count_[kid]++;
+  }
+  void collect(lbfgsb_b200_stats* st) {
+    for (int k = 0; k < KID_COUNT; k++) {
+      st->launches[k] = count_[k];
+      st->total_launches += count_[k];
+      st->ms[k] = 0;
+    }
+    for (auto& t : timed_) {
+      float ms = 0;
+      if (cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess) st->ms[t.kid] += ms;
+    }
+  }
+
+ private:
+  struct Timed {
+    int kid;
+    cudaEvent_t a, b;
+  };
+  cudaEvent_t event() {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    pool_.push_back(e);
+    return e;
+  }
+  cudaStream_t s_;
+  bool profile_;
+  long long count_[KID_COUNT];
+  std::vector<Timed> timed_;
+  std::vector<cudaEvent_t> pool_;
+};
+
+// Owns the device workspace of one solve.
+template <typename R, typename H, typename S>
+struct Workspace {
+  cudaStream_t s = nullptr;
+  std::vector<void*> blocks;
+  R* X[3] = {nullptr, nullptr, nullptr};
+  R* G[2] = {nullptr, nullptr};
+  R* dsub = nullptr;
+  H* ws = nullptr;
+  H* wy = nullptr;
+  int8_t* code = nullptr;
+  uint32_t* fbits = nullptr;
+  DevState<S>* st = nullptr;
+  DevState<S>* hs = nullptr;  // pinned mirror
+  double* part = nullptr;
+  unsigned int* ticket = nullptr;
+  double* wl_t = nullptr;
+  int* wl_i = nullptr;
+  unsigned int* wl_n = nullptr;
+
+  template <typename T>
+  T* alloc(size_t count) {
+    void* p = nullptr;
+    CK(cudaMallocAsync(&p, std::max<size_t>(count, 1) * sizeof(T), s));
+    blocks.push_back(p);
+    return static_cast<T*>(p);
+  }
+  ~Workspace() {
+    for (void* p : blocks) cudaFreeAsync(p, s);
+    if (hs) cudaFreeHost(hs);
+  }
+};
+
+static int device_sms() {
+  int dev = 0, sms = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  return sms;
+}
+
+template <typename K>
+static int grid_for(K kernel, int n, int threads) {
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0));
+  per_sm = std::max(per_sm, 1);
+  long long want = ((long long)n + threads - 1) / threads;
+  long long cap = (long long)device_sms() * per_sm;
+  return (int)std::max<long long>(1, std::min(want, cap));
+}
+
+template <typename R, typename H, typename S>
+static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
+                 const typename Api<R>::Opt* opt, typename Api<R>::Cb funcgrad,
+                 typename Api<R>::Cb after_iter, typename Api<R>::Cb custom_stop, void* user,
+                 cudaStream_t stream, const lbfgsb_b200_ext* ext,
+                 typename Api<R>::Sum* summary) {
+  using Sum = typename Api<R>::Sum;
+  g_last_error.clear();
+  std::memset(&g_last_stats, 0, sizeof(g_last_stats));
+  if (!opt || !summary || !x_user || !nbd || !l || !u) return LBFGSB_B200_ERR_ARGUMENT;
+  if (opt->mode != LBFGSB_B200_MODE_CUDA) {
+    summary->info = -1;
+    return LBFGSB_B200_ERR_ARGUMENT;
+  }
+  const int m = std::min(opt->hessian_approximate_dimension, kMaxM);
+  // errclb's scalar checks and the driver's option checks (lbfgsbcpu.cpp:258-264, 879-890)
+  if (n <= 0 || m <= 0 || m > n || opt->eps_f < 0 || opt->max_iteration < 0 ||
+      opt->eps_g < 0 || opt->eps_x < 0) {
+    summary->info = -1;
+    return LBFGSB_B200_OK;
+  }
+  if (!funcgrad) {  // the reference's GPU driver rejects a missing callback (lbfgsbcuda.cpp:28-33)
+    summary->info = -1;
+    return LBFGSB_B200_ERR_ARGUMENT;
+  }
+  const bool profile = ext && ext->profile;
+  lbfgsb_b200_trace_callback trace = ext ? ext->trace : nullptr;
+  void* trace_user = ext ? ext->trace_user : nullptr;
+
+  Workspace<R, H, S> w;
+  w.s = stream;
+  Launcher L(stream, profile);
+  long long syncs = 0, evals = 0;
+  try {
+    const size_t N = (size_t)n;
+    for (int k = 0; k < 3; k++) w.X[k] = w.template alloc<R>(N);
+    for (int k = 0; k < 2; k++) w.G[k] = w.template alloc<R>(N);
+    w.dsub = w.template alloc<R>(N);
+    w.ws = w.template alloc<H>(N * kSlots);
+    w.wy = w.template alloc<H>(N * kSlots);
+    w.code = w.template alloc<int8_t>(N);
+    const size_t words = (N + 31) / 32 + 1;
+    w.fbits = w.template alloc<uint32_t>(words);
+    w.st = w.template alloc<DevState<S>>(1);
+    w.ticket = w.template alloc<unsigned int>(1);
+    CK(cudaMallocHost(&w.hs, sizeof(DevState<S>)));
+
+    Ctx<R, H, S> c;
+    c.n = n;
+    c.l = l;
+    c.u = u;
+    c.nbd = nbd;
+    c.ws = w.ws;
+    c.wy = w.wy;
+    c.code = w.code;
+    c.fbits = w.fbits;
+    c.dsub = w.dsub;
+    c.st = w.st;
+    c.ticket = w.ticket;
+    c.wl_t = nullptr;
+    c.wl_i = nullptr;
+    c.wl_n = nullptr;
+
+    const int g_gcp = grid_for(k_gcp_scan<R, H, S>, n, kThreads);
+    const int g_freev = grid_for(k_freev_formk<R, H, S>, n, kThreads);
+    const int g_dir = grid_for(k_subsm_dir<R, H, S>, n, kThreads);
+    const int g_apply = grid_for(k_subsm_apply<R, H, S>, n, kThreads);
+    const int g_post = grid_for(k_post_eval<R, H, S>, n, kThreads);
+    const int g_proj = grid_for(k_projgr<R, H, S>, n, kThreads);
+    const int g_max = std::max({g_gcp, g_freev, g_dir, g_apply, g_post, g_proj});
+    w.part = w.template alloc<double>((size_t)g_max * 256);
+    c.part = w.part;
+    const int g_elem = (int)std::min<long long>(((long long)n + 255) / 256, (long long)device_sms() * 8);
+
+    // history slots start at zero so that unused positions read as finite values
+    CK(cudaMemsetAsync(w.ws, 0, N * kSlots * sizeof(H), stream));
+    CK(cudaMemsetAsync(w.wy, 0, N * kSlots * sizeof(H), stream));
+    CK(cudaMemsetAsync(w.fbits, 0, words * sizeof(uint32_t), stream));
+    CK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned int), stream));
+
+    DevState<S>& hs = *w.hs;
+    std::memset(&hs, 0, sizeof(hs));
+    hs.n = n;
+    hs.m = m;
+    hs.boxed = 1;
+    hs.head = 1;
+    hs.theta = 1;
+    hs.iword = -1;
+    hs.big = (S)1.0e10;
+    for (int r = 1; r <= m; r++) hs.phys[r] = r - 1;
+    hs.spare = m;
+    CK(cudaMemcpyAsync(w.st, &hs, sizeof(hs), cudaMemcpyHostToDevice, stream));
+    const size_t header = offsetof(DevState<S>, big);
+    auto pull = [&]() {
+      CK(cudaMemcpyAsync(w.hs, w.st, header, cudaMemcpyDeviceToHost, stream));
+      CK(cudaStreamSynchronize(stream));
+      syncs++;
+    };
+
+    R* xcur = w.X[0];
+    R* zb = w.X[1];
+    R* tb = w.X[2];
+    R* gcur = w.G[0];
+    R* gnew = w.G[1];
+    int info = 0;
+    bool finished = false;
+    auto finish = [&](int code) {
+      summary->info = code;
+      finished = true;
+    };
+
+    // errclb's per-variable checks and lbfgsbactive, into the solver's x buffer
+    L.run(KID_INIT, [&] {
+      k_init<R, S><<<g_elem, 256, 0, stream>>>(n, x_user, xcur, nbd, l, u, w.st);
+    });
+    pull();
+    if (hs.input_error) {
+      summary->info = -1;  // x is left as given (lbfgsbcpu.cpp:259-264)
+      CK(cudaStreamSynchronize(stream));
+      goto done;
+    }
+    {
+      const bool cnstnd = hs.cnstnd != 0;
+      R f = 0;
+      funcgrad(user, xcur, &f, gcur, (void*)stream, summary);
+      evals++;
+      L.run(KID_PROJGR, [&] {
+        k_projgr<R, H, S><<<g_proj, kThreads, 0, stream>>>(c, xcur, gcur, (S)f);
+      });
+      pull();
+      summary->residual_g = (R)hs.sbgnrm;
+      if (hs.sbgnrm <= (S)opt->eps_g) finish(4);
+
+      int reset = 0;
+      DevState<S> snap;
+      while (!finished) {
+        L.run(KID_BEGIN, [&] { k_begin_iteration<S><<<1, 1, 0, stream>>>(w.st, reset); });
+        const int reset_before = reset;
+        reset = 0;
+        const int col_now = reset_before ? 0 : hs.col;
+        const bool uncon = !cnstnd && col_now > 0;
+        auto subspace = [&]() {
+          L.run(KID_FREEV, [&] {
+            k_freev_formk<R, H, S><<<g_freev, kThreads, 0, stream>>>(c, xcur, gcur);
+          });
+          L.run(KID_SUBDIR, [&] {
+            k_subsm_dir<R, H, S><<<g_dir, kThreads, 0, stream>>>(c, xcur, gcur);
+          });
+          L.run(KID_SUBAPPLY, [&] {
+            k_subsm_apply<R, H, S><<<g_apply, kThreads, 0, stream>>>(c, xcur, gcur, zb);
+          });
+        };
+        if (!uncon) {
+          L.run(KID_GCP, [&] { k_gcp_scan<R, H, S><<<g_gcp, kThreads, 0, stream>>>(c, xcur, gcur); });
+        }
+        subspace();
+        pull();
+        if (hs.gcp_state == GCP_WALK && hs.internal_fail == 0) {
+          if (!c.wl_t) {
+            w.wl_t = w.template alloc<double>(N);
+            w.wl_i = w.template alloc<int>(N);
+            w.wl_n = w.template alloc<unsigned int>(1);
+            c.wl_t = w.wl_t;
+            c.wl_i = w.wl_i;
+            c.wl_n = w.wl_n;
+          }
+          CK(cudaMemsetAsync(w.wl_n, 0, sizeof(unsigned int), stream));
+          L.run(KID_WALK_GATHER, [&] {
+            k_walk_gather<R, H, S><<<g_elem, kThreads, 0, stream>>>(c, xcur, gcur);
+          });
+          L.run(KID_WALK, [&] { k_walk<R, H, S><<<1, kWalkThreads, 0, stream>>>(c, xcur, gcur); });
+          subspace();
+          pull();
+        }
+        if (hs.internal_fail != 0) {  // cauchy/formk/cmprlb/subsm failed: reset (297-341)
+          reset = 1;
+          continue;
+        }
+        snap = hs;
+        if (trace) {  // the trace also reports a few entries of the small matrices
+          CK(cudaMemcpyAsync(&snap, w.st, sizeof(snap), cudaMemcpyDeviceToHost, stream));
+          CK(cudaStreamSynchronize(stream));
+        }
+        if (hs.ls_info != 0) {
+          // g'd >= 0 at the start of the line search: x, g, f stay (359-387)
+          if (hs.col == 0) {
+            finish(-2);
+            break;
+          }
+          reset = 1;
+          continue;
+        }
+        // line search (347-358)
+        R* xt = zb;
+        bool quirk = false;
+        while (true) {
+          if (hs.stp == S(1)) {
+            xt = zb;
+          } else {
+            L.run(KID_TRIAL, [&] {
+              k_trial<R, S><<<g_elem, 256, 0, stream>>>(n, xcur, zb, tb, w.st);
+            });
+            xt = tb;
+          }
+          funcgrad(user, xt, &f, gnew, (void*)stream, summary);
+          evals++;
+          L.run(KID_POST, [&] {
+            k_post_eval<R, H, S><<<g_post, kThreads, 0, stream>>>(c, xcur, zb, xt, gnew, gcur,
+                                                                  (S)f, 0);
+          });
+          pull();
+          if (hs.ls_task != 1) break;
+          if (hs.iback >= 20) {
+            quirk = true;
+            break;
+          }
+        }
+        if (quirk) {
+          // the reference leaves the search after 20 backtracks with x at the new,
+          // unevaluated trial point and f, g of the previous one (352-358)
+          if (hs.stp == S(1)) {
+            xt = zb;
+          } else {
+            L.run(KID_TRIAL, [&] {
+              k_trial<R, S><<<g_elem, 256, 0, stream>>>(n, xcur, zb, tb, w.st);
+            });
+            xt = tb;
+          }
+          L.run(KID_POST, [&] {
+            k_post_eval<R, H, S><<<g_post, kThreads, 0, stream>>>(c, xcur, zb, xt, gnew, gcur,
+                                                                  (S)f, 1);
+          });
+          pull();
+        }
+        if (xt == zb)
+          std::swap(xcur, zb);
+        else
+          std::swap(xcur, tb);
+        std::swap(gcur, gnew);
+        summary->num_iteration = hs.iter;
+        if (trace) {
+          lbfgsb_b200_trace_record rec;
+          rec.iter = hs.iter;
+          rec.nint = snap.nint;
+          rec.nbreak = snap.gcp_state == GCP_SKIPPED ? 0 : snap.nbreak;
+          rec.nfree = snap.nfree;
+          rec.nenter = snap.nenter;
+          rec.nleave = snap.nleave;
+          rec.col = snap.col;
+          rec.head = snap.head;
+          rec.nfgv = hs.nfgv + 1;  // the oracle counts the first evaluation too
+          rec.ifun = hs.ifun;
+          rec.iword = snap.subsm_active ? snap.iword : -1;
+          rec.reset = reset_before;
+          rec.free_hash = snap.free_hash;
+          rec.at_lower = snap.at_lower;
+          rec.at_upper = snap.at_upper;
+          rec.f = (double)hs.f;
+          rec.theta = (double)snap.theta;
+          rec.stp = (double)hs.stp;
+          rec.dtm = (double)snap.dtm;
+          rec.tsum = (double)snap.tsum;
+          rec.gd = (double)hs.gd;
+          rec.gdold = (double)hs.gdold;
+          rec.dtd = (double)hs.dtd;
+          rec.stpmx = (double)hs.stpmx;
+          rec.f1_0 = (double)snap.f1_0;
+          rec.f2_0 = (double)snap.f2_0;
+          const int cc = snap.col;
+          rec.dbg[0] = cc > 0 ? (double)snap.p[1] : 0;
+          rec.dbg[1] = cc > 0 ? (double)snap.p[cc + 1] : 0;
+          rec.dbg[2] = cc > 0 ? (double)snap.c[1] : 0;
+          rec.dbg[3] = cc > 0 ? (double)snap.c[cc + 1] : 0;
+          rec.dbg[4] = cc > 0 ? (double)snap.mc[1] : 0;
+          rec.dbg[5] = cc > 0 ? (double)snap.mc[cc + 1] : 0;
+          rec.dbg[6] = cc > 0 ? (double)snap.sy[0] : 0;
+          rec.dbg[7] = cc > 0 ? (double)snap.wt[0] : 0;
+          trace(trace_user, &rec);
+        }
+        if (after_iter) after_iter(user, xcur, &f, gcur, (void*)stream, summary);
+        // stopping tests in the reference's order (394-429)
+        summary->residual_g = (R)hs.sbgnrm;
+        if (hs.sbgnrm <= (S)opt->eps_g) {
+          finish(4);
+          break;
+        }
+        summary->residual_x = (R)hs.tf;
+        if (hs.tf <= (S)opt->eps_x) {
+          finish(2);
+          break;
+        }
+        {
+          const S fold = hs.fold, fc = hs.f;
+          const S ddum = smax<S>(sabs(fold), smax<S>(sabs(fc), S(1)));
+          summary->residual_f = (R)((fold - fc) / ddum);
+          if (fold - fc <= (S)opt->eps_f * ddum) {
+            finish(1);
+            break;
+          }
+        }
+        if (hs.iter > opt->max_iteration && opt->max_iteration > 0) {
+          finish(5);
+          break;
+        }
+        if (custom_stop && custom_stop(user, xcur, &f, gcur, (void*)stream, summary)) {
+          finish(0);
+          break;
+        }
+        if (hs.internal_fail != 0) {  // formt failed (451-459)
+          reset = 1;
+          continue;
+        }
+      }
+      (void)info;
+    }
+    CK(cudaMemcpyAsync(x_user, xcur, N * sizeof(R), cudaMemcpyDeviceToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+  done:
+    lbfgsb_b200_stats& st = g_last_stats;
+    st.kernels = KID_COUNT;
+    for (int k = 0; k < KID_COUNT; k++) {
+      std::snprintf(st.name[k], sizeof(st.name[k]), "%s", kKernelNames[k]);
+    }
+    L.collect(&st);
+    st.host_syncs = syncs;
+    st.evaluations = evals;
+    // algorithmic bytes of one launch (steady state, all variables free, col = m)
+    const double Rb = sizeof(R), Hb = sizeof(H), hist = 2.0 * m * Hb, nn = (double)n;
+    st.bytes[KID_GCP] = nn * (4 * Rb + 4 + hist + 1);
+    st.bytes[KID_FREEV] = nn * (2 * Rb + hist + 1 + 0.25);
+    st.bytes[KID_SUBDIR] = nn * (5 * Rb + hist + 5);
+    st.bytes[KID_SUBAPPLY] = nn * (6 * Rb + 5);
+    st.bytes[KID_POST] = nn * (6 * Rb + 4 + hist + 2 * Hb);
+    st.bytes[KID_TRIAL] = nn * 3 * Rb;
+    st.bytes[KID_WALK_GATHER] = nn * (4 * Rb + 4);
+    st.bytes[KID_PROJGR] = nn * (4 * Rb + 4);
+    st.bytes[KID_INIT] = nn * (4 * Rb + 4);
+    st.bytes_per_iteration_model = st.bytes[KID_GCP] + st.bytes[KID_FREEV] +
+                                   st.bytes[KID_SUBDIR] + st.bytes[KID_SUBAPPLY] +
+                                   st.bytes[KID_POST];
+  } catch (const CudaFailure& e) {
+    char buf[256];
+    std::snprintf(buf, sizeof(buf), "%s failed at driver.cu:%d: %s", e.call, e.line,
+                  cudaGetErrorString(e.err));
+    g_last_error = buf;
+    return LBFGSB_B200_ERR_CUDA;
+  }
+  return LBFGSB_B200_OK;
+}
+
+template <typename R, typename Opt>
+static void default_option(Opt* o, R meps, R mmax) {
+  o->eps_f = o->eps_g = o->eps_x = (R)1e-15;
+  o->hessian_approximate_dimension = 8;
+  o->machine_epsilon = meps;
+  o->machine_maximum = mmax;
+  o->max_iteration = 1000;
+  o->mode = LBFGSB_B200_MODE_CUDA;
+  o->step_scaling = (R)1.0;
+}
+
+}  // namespace lbfgsb_b200
+
+using namespace lbfgsb_b200;
+
+extern "C" {
+
+void lbfgsb_b200_default_option_f64(lbfgsb_b200_option_f64* o) {
+  if (o) default_option<double>(o, 1e-15, 1.7976931348623157e308);
+}
+void lbfgsb_b200_default_option_f32(lbfgsb_b200_option_f32* o) {
+  if (o) default_option<float>(o, 1e-8f, 3.40282347e38f);
+}
+
+int lbfgsb_b200_minimize_ext_f64(int n, double* x, const int* nbd, const double* l,
+                                 const double* u, const lbfgsb_b200_option_f64* option,
+                                 lbfgsb_b200_callback_f64 funcgrad,
+                                 lbfgsb_b200_callback_f64 after_iteration,
+                                 lbfgsb_b200_callback_f64 customized_stopping, void* user,
+                                 void* stream, const lbfgsb_b200_ext* ext,
+                                 lbfgsb_b200_summary_f64* summary) {
+  return solve<double, double, double>(n, x, nbd, l, u, option, funcgrad, after_iteration,
+                                       customized_stopping, user, (cudaStream_t)stream, ext,
+                                       summary);
+}
+
+int lbfgsb_b200_minimize_ext_f32(int n, float* x, const int* nbd, const float* l,
+                                 const float* u, const lbfgsb_b200_option_f32* option,
+                                 lbfgsb_b200_callback_f32 funcgrad,
+                                 lbfgsb_b200_callback_f32 after_iteration,
+                                 lbfgsb_b200_callback_f32 customized_stopping, void* user,
+                                 void* stream, const lbfgsb_b200_ext* ext,
+                                 lbfgsb_b200_summary_f32* summary) {
+  const int form = ext ? ext->form : LBFGSB_B200_FORM_PLAIN;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (form == LBFGSB_B200_FORM_MIXED)
+    return solve<float, float, double>(n, x, nbd, l, u, option, funcgrad, after_iteration,
+                                       customized_stopping, user, s, ext, summary);
+  if (form == LBFGSB_B200_FORM_MIXED_BF16)
+    return solve<float, __nv_bfloat16, double>(n, x, nbd, l, u, option, funcgrad,
+                                               after_iteration, customized_stopping, user, s,
+                                               ext, summary);
+  return solve<float, float, float>(n, x, nbd, l, u, option, funcgrad, after_iteration,
+                                    customized_stopping, user, s, ext, summary);
+}
+
+int lbfgsb_b200_minimize_f64(int n, double* x, const int* nbd, const double* l,
+                             const double* u, const lbfgsb_b200_option_f64* option,
+                             lbfgsb_b200_callback_f64 funcgrad,
+                             lbfgsb_b200_callback_f64 after_iteration,
+                             lbfgsb_b200_callback_f64 customized_stopping, void* user,
+                             void* stream, lbfgsb_b200_summary_f64* summary) {
+  return lbfgsb_b200_minimize_ext_f64(n, x, nbd, l, u, option, funcgrad, after_iteration,
+                                      customized_stopping, user, stream, nullptr, summary);
+}
+
+int lbfgsb_b200_minimize_f32(int n, float* x, const int* nbd, const float* l, const float* u,
+                             const lbfgsb_b200_option_f32* option,
+                             lbfgsb_b200_callback_f32 funcgrad,
+                             lbfgsb_b200_callback_f32 after_iteration,
+                             lbfgsb_b200_callback_f32 customized_stopping, void* user,
+                             void* stream, lbfgsb_b200_summary_f32* summary) {
+  return lbfgsb_b200_minimize_ext_f32(n, x, nbd, l, u, option, funcgrad, after_iteration,
+                                      customized_stopping, user, stream, nullptr, summary);
+}
+
+int lbfgsb_b200_last_stats(lbfgsb_b200_stats* out) {
+  if (!out) return LBFGSB_B200_ERR_ARGUMENT;
+  *out = g_last_stats;
+  return LBFGSB_B200_OK;
+}
+
+const char* lbfgsb_b200_last_error(void) { return g_last_error.c_str(); }
+
+int lbfgsb_b200_copy(void* dst, const void* src, size_t bytes, int kind) {
+  cudaMemcpyKind k = kind == 1   ? cudaMemcpyHostToDevice
+                     : kind == 2 ? cudaMemcpyDeviceToHost
+                                 : cudaMemcpyDeviceToDevice;
+  cudaError_t e = cudaMemcpy(dst, src, bytes, k);
+  if (e != cudaSuccess) {
+    g_last_error = cudaGetErrorString(e);
+    return LBFGSB_B200_ERR_CUDA;
+  }
+  return LBFGSB_B200_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,931 @@
+// passes.cuh -- the streaming passes of one L-BFGS-B iteration on sm_100a.
+//
+// One iteration of the reference's outer loop (culbfgsb/lbfgsbcpu.cpp:279-462) is cut into
+// five grid-wide passes over the n-vectors and the slot-major S/Y history, each ending
+// in a deterministic reduction whose last CTA runs the scalar / small-matrix epilogue:
+//
+//   A  k_gcp_scan        cauchy's scan (lbfgsbcpu.cpp:634-701): iwhere, d = -g, p = W'd,
+//                        f', breakpoints; epilogue: f'', dtm, first-breakpoint test
+//                        (the full breakpoint walk, when needed, is walk.cuh)
+//   B  k_freev_formk     freev (1135-1173) as a bitmask, the formk products (972-1054:
+//                        new row over F/A, entering/leaving corrections), cmprlb's reduced
+//                        gradient r (819-869) and subsm's W'r (1446-1458); epilogue:
+//                        formk assembly + factorisation, the two K solves
+//   C  k_subsm_dir       subsm's direction (1472-1483) and the step to the first bound
+//                        (1484-1516) as an arg-min reduction
+//   D  k_subsm_apply     the truncated step (1517-1533), d = z - x, and lnsrlb's start
+//                        (1263-1320): dtd, stpmx, g'd; epilogue: dcsrch start
+//   E  k_post_eval       after each function evaluation: g'd and dcsrch (1312-1338); on
+//                        acceptance the stopping-test quantities (projgr, |dx|, rr) and
+//                        matupd/formt (1341-1387, 1105-1133), with (s, y) written to a
+//                        spare history slot that the epilogue commits to the ring
+//
+// Elementwise arithmetic that feeds a comparison or a stored vector repeats the
+// reference's operations in its order (the build uses -fmad=false, so no FMA is
+// contracted); reductions accumulate in double with explicit fma().
+#pragma once
+
+#include "common.cuh"
+#include "reduce.cuh"
+#include "small.cuh"
+#include "state.cuh"
+
+namespace lbfgsb_b200 {
+
+template <typename R, typename H, typename S>
+struct Ctx {
+  int n;
+  const R* __restrict__ l;
+  const R* __restrict__ u;
+  const int* __restrict__ nbd;
+  H* ws;             // kSlots slot-major arrays of n
+  H* wy;
+  int8_t* code;      // iwhere codes
+  uint32_t* fbits;   // free set of the last freev, one bit per variable
+  R* dsub;           // subspace direction on the free set
+  DevState<S>* st;
+  double* part;      // reduction rows
+  unsigned int* ticket;
+  double* wl_t;      // breakpoint list (walk)
+  int* wl_i;
+  unsigned int* wl_n;
+};
+
+// Physical slot pointers of ring positions 1..kMaxM counted from head.
+template <typename H, typename S>
+__device__ __forceinline__ void ring_ptrs(const DevState<S>* st, const H* base, int n,
+                                          const H* (&out)[kMaxM]) {
+  const int m = st->m, head = st->head;
+#pragma unroll
+  for (int j = 0; j < kMaxM; j++) {
+    int r = (head - 1 + j) % m + 1;
+    out[j] = base + (size_t)st->phys[r] * (size_t)n;
+  }
+}
+
+// cauchy's per-variable classification (lbfgsbcpu.cpp:635-663) and breakpoint
+// (675-699).  Returns the iwhere code; sets has_bp/t for a movable variable with a
+// breakpoint.  The static codes -1 (nbd 0) and 3 (l == u) come from nbd, l, u, which is
+// what lbfgsbactive stored (467-515).
+template <typename R>
+__device__ __forceinline__ int classify(R x, R g, R l, R u, int nb, bool& has_bp, R& t) {
+  const R neggi = -g;
+  has_bp = false;
+  t = R(0);
+  if (nb == 0) return IW_UNB;
+  if (nb == 2 && rsub(u, l) <= R(0)) return IW_FIX;
+  R tl = 0, tu = 0;
+  if (nb <= 2) tl = rsub(x, l);
+  if (nb >= 2) tu = rsub(u, x);
+  const bool xlower = nb <= 2 && tl <= R(0);
+  const bool xupper = nb >= 2 && tu <= R(0);
+  int code = IW_FREE;
+  if (xlower) {
+    if (neggi <= R(0)) code = IW_LOW;
+  } else if (xupper) {
+    if (neggi >= R(0)) code = IW_UPP;
+  } else if (fabs((double)neggi) <= 0.0) {
+    code = IW_ZERO;
+  }
+  if (code == IW_FREE) {
+    if (nb <= 2 && neggi < R(0)) {
+      has_bp = true;
+      t = rdiv(tl, -neggi);
+    } else if (nb >= 2 && neggi > R(0)) {
+      has_bp = true;
+      t = rdiv(tu, neggi);
+    }
+  }
+  return code;
+}
+
+// The generalized Cauchy point of one variable, rebuilt from its code: xcp = x + tsum*d
+// for a variable that moves along d = -g (lbfgsbcpu.cpp:813), its bound when the walk
+// fixed it (755-761), x otherwise.
+template <typename R, typename S>
+__device__ __forceinline__ R gcp_point(int code, R x, R g, R l, R u, S tsum) {
+  if (code == IW_FREE || code == IW_UNB) {
+    const S d = (S)(-g);
+    return (R)((S)x + tsum * d);
+  }
+  if (code == IW_WALK_LOW) return l;
+  if (code == IW_WALK_UPP) return u;
+  return x;
+}
+
+// cmprlb's reduced gradient of one free variable (lbfgsbcpu.cpp:842-867), in the
+// reference's operation order.  uncon: the !cnstnd && col > 0 branch (r = -g).
+template <typename R, typename S>
+__device__ __forceinline__ S reduced_grad(bool uncon, R x, R z, R g, int col,
+                                          const S (&yv)[kMaxM], const S (&sv)[kMaxM],
+                                          const S* a1, const S* a2) {
+  if (uncon) return -(S)g;
+  S r = -a1[kMaxM] * ((S)z - (S)x) - (S)g;  // a1[kMaxM] holds theta
+#pragma unroll
+  for (int j = 0; j < kMaxM; j++)
+    if (j < col) r = r + yv[j] * a1[j] + sv[j] * a2[j];
+  return r;
+}
+
+// ------------------------------------------------------------------------------------
+// A: the Cauchy-point scan.
+template <typename R, typename H, typename S>
+__global__ void __launch_bounds__(kThreads) k_gcp_scan(Ctx<R, H, S> c, const R* __restrict__ x,
+                                                       const R* __restrict__ g) {
+  DevState<S>* st = c.st;
+  const int n = c.n, col = st->col;
+  const H *Y[kMaxM], *Sl[kMaxM];
+  ring_ptrs(st, c.wy, n, Y);
+  ring_ptrs(st, c.ws, n, Sl);
+  // sums: [0] sum neggi^2, [1..16] p (y part 1..8, s part 9..16), [17] nbreak,
+  // [18] movable variables without breakpoint; max: [0] any such with g != 0;
+  // min pair: smallest breakpoint
+  constexpr int NS = 19, NX = 1, NM = 1;
+  double s[NS], xm[NX];
+  MinPair mn[NM];
+#pragma unroll
+  for (int k = 0; k < NS; k++) s[k] = 0.0;
+  xm[0] = 0.0;
+  mn[0] = MinPair{INFINITY, kNoIndex};
+  for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < n;
+       i += (long long)gridDim.x * kThreads) {
+    const R xi = x[i], gi = g[i], li = c.l[i], ui = c.u[i];
+    const int nb = c.nbd[i];
+    bool has_bp;
+    R t;
+    const int code = classify(xi, gi, li, ui, nb, has_bp, t);
+    c.code[i] = (int8_t)code;
+    if (code == IW_FREE || code == IW_UNB) {
+      const double neggi = -(double)gi;
+      s[0] = fma(neggi, neggi, s[0]);
+#pragma unroll
+      for (int j = 0; j < kMaxM; j++) {
+        if (j < col) {
+          s[1 + j] = fma((double)HistTraits<H>::load(Y[j] + i), neggi, s[1 + j]);
+          s[9 + j] = fma((double)HistTraits<H>::load(Sl[j] + i), neggi, s[9 + j]);
+        }
+      }
+      if (has_bp) {
+        s[17] += 1.0;
+        mn[0] = minpair(mn[0], MinPair{(double)t, i});
+      } else {
+        s[18] += 1.0;
+        if (neggi != 0.0) xm[0] = 1.0;
+      }
+    }
+  }
+  constexpr int W = NS + NX + 2 * NM;
+  double lo[1] = {0.0};
+  cta_reduce_to_row<NS, NX, NM, 0>(s, xm, mn, lo, c.part, W);
+  if (!last_cta(c.ticket)) return;
+  __shared__ double red[W];
+  fold_rows(c.part, gridDim.x, W, NS, NX, NM, red);
+  __shared__ SmallWork<S> sw;
+  if (threadIdx.x != 0) return;
+
+  // epilogue: lbfgsbcpu.cpp:702-733 and the first breakpoint test of the walk (745-747)
+  const S theta = st->theta;
+  const S f1 = -(S)red[0];
+  const int col2 = 2 * col;
+  for (int j = 1; j <= col; j++) {
+    st->p[j] = (S)red[j];
+    st->p[col + j] = (S)red[8 + j];
+  }
+  if (theta != S(1))
+    for (int j = col + 1; j <= col2; j++) st->p[j] *= theta;
+  st->nbreak = (int)red[17];
+  st->nfree_mov = (int)red[18];
+  st->bnded = red[19] > 0.0 ? 0 : 1;
+  st->internal_fail = 0;
+  if (st->nbreak == 0 && st->nfree_mov == 0) {
+    // xcp = x; c is left as it was (lbfgsbcpu.cpp:706-708), and cmprlb still applies the
+    // current middle matrix to it
+    st->gcp_state = GCP_EARLY;
+    st->tsum = 0;
+    if (col > 0) {
+      int info = 0;
+      sbmv(st->sy, st->wt, col, st->c, st->mc, &info, sw.work);
+      if (info != 0) st->internal_fail = -8;
+    }
+    return;
+  }
+  for (int j = 1; j <= col2; j++) st->c[j] = 0;
+  S f2 = -theta * f1;
+  const S f2org = f2;
+  if (col > 0) {
+    S* v = sw.v;
+    int info = 0;
+    sbmv(st->sy, st->wt, col, st->p, v, &info, sw.work);
+    if (info != 0) {
+      st->internal_fail = info;
+      return;
+    }
+    f2 = f2 - sdot(&v[1], 1, &st->p[1], 1, col2);
+  }
+  S dtm = -f1 / f2;
+  st->f1 = f1;
+  st->f2 = f2;
+  st->f1_0 = f1;
+  st->f2_0 = f2;
+  st->f2org = f2org;
+  st->tsum = 0;
+  st->tj = 0;
+  st->nint = 1;
+  st->nleft = st->nbreak;
+  if (st->nbreak != 0) {
+    st->bkmin = (S)red[NS + NX];
+    st->ibkmin = (int)red[NS + NX + 1];
+    if (!(dtm < st->bkmin - S(0))) {
+      st->dtm = dtm;
+      st->gcp_state = GCP_WALK;  // at least one breakpoint is passed
+      return;
+    }
+  }
+  if (dtm <= S(0)) dtm = 0;
+  st->dtm = dtm;
+  st->tsum = st->tsum + dtm;
+  for (int j = 1; j <= col2; j++) st->c[j] += dtm * st->p[j];
+  if (col > 0) {
+    int info = 0;
+    sbmv(st->sy, st->wt, col, st->c, st->mc, &info, sw.work);  // cmprlb's M c (852)
+    if (info != 0) st->internal_fail = -8;
+  }
+  st->gcp_state = GCP_DONE;
+}
+
+// ------------------------------------------------------------------------------------
+// B: freev + formk products + reduced gradient + W'r.  One warp handles 32 consecutive
+// variables per step so that the free-set bitmask is read and written a word at a time.
+constexpr int kLaneOwned = 5;  // 136 correction products over 32 lanes
+
+// Output q of the 136 entering/leaving products: kind 0 y_a y_b (a >= b, q < 36),
+// kind 1 s_a s_b (a >= b, q < 72), kind 2 s_a y_b (q < 136), kind 3 unused.
+__host__ __device__ inline void corr_map(int q, int& kind, int& a, int& b) {
+  if (q < 72) {
+    kind = q < 36 ? 0 : 1;
+    int t = q < 36 ? q : q - 36;
+    a = 0;
+    while ((a + 1) * (a + 2) / 2 <= t) a++;
+    b = t - a * (a + 1) / 2;
+  } else if (q < 136) {
+    kind = 2;
+    a = (q - 72) / kMaxM;
+    b = (q - 72) % kMaxM;
+  } else {
+    kind = 3;
+    a = b = 0;
+  }
+}
+
+template <typename R, typename H, typename S>
+__global__ void __launch_bounds__(kThreads) k_freev_formk(Ctx<R, H, S> c, const R* __restrict__ x,
+                                                          const R* __restrict__ g) {
+  DevState<S>* st = c.st;
+  if (st->gcp_state == GCP_WALK || st->internal_fail != 0) return;
+  const int n = c.n, col = st->col, iter = st->iter;
+  const bool uncon = st->uncon_branch != 0;
+  const bool track = !uncon && iter > 0 && st->cnstnd;
+  const bool updatd = st->updatd != 0;
+  const S theta = st->theta, tsum = st->tsum;
+  const H *Y[kMaxM], *Sl[kMaxM];
+  ring_ptrs(st, c.wy, n, Y);
+  ring_ptrs(st, c.ws, n, Sl);
+  S a1[kMaxM + 1], a2[kMaxM];
+#pragma unroll
+  for (int j = 0; j < kMaxM; j++) {
+    a1[j] = (j < col) ? st->mc[1 + j] : S(0);
+    a2[j] = (j < col) ? theta * st->mc[col + 1 + j] : S(0);
+  }
+  a1[kMaxM] = theta;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int kWarps = kThreads / 32;
+  // sums: [0..7] sum_F y_j r, [8..15] sum_F s_j r, [16..23] yy_new, [24..31] ss_new,
+  // [32..39] sy_row, [40..47] sy_col, [48] nfree, [49] nenter, [50] nleave,
+  // [51] at lower, [52] at upper
+  constexpr int NS = 53;
+  double s[NS];
+#pragma unroll
+  for (int k = 0; k < NS; k++) s[k] = 0.0;
+  double corr[kLaneOwned];
+#pragma unroll
+  for (int k = 0; k < kLaneOwned; k++) corr[k] = 0.0;
+  unsigned long long hash = 0;
+  __shared__ double bc[kWarps][2 * kMaxM];
+  const int newest = col - 1;
+  int ck[kLaneOwned], ca[kLaneOwned], cb[kLaneOwned];
+#pragma unroll
+  for (int k = 0; k < kLaneOwned; k++) corr_map(lane + 32 * k, ck[k], ca[k], cb[k]);
+
+  for (long long base = ((long long)blockIdx.x * kWarps + warp) * 32; base < n;
+       base += (long long)gridDim.x * kWarps * 32) {
+    const long long i = base + lane;
+    const bool valid = i < n;
+    int code = IW_LOW;
+    if (valid) code = c.code[i];
+    const bool fnow = valid && (uncon || iw_free(code));
+    const uint32_t word = c.fbits[base >> 5];
+    const bool fprev = (word >> lane) & 1u;
+    const bool enter = track && valid && !fprev && fnow;
+    const bool leave = track && valid && fprev && !fnow;
+    const uint32_t newword = __ballot_sync(0xffffffffu, fnow);
+    if (!uncon && lane == 0) c.fbits[base >> 5] = newword;
+    S yv[kMaxM], sv[kMaxM];
+#pragma unroll
+    for (int j = 0; j < kMaxM; j++) {
+      yv[j] = (valid && j < col) ? (S)HistTraits<H>::load(Y[j] + i) : S(0);
+      sv[j] = (valid && j < col) ? (S)HistTraits<H>::load(Sl[j] + i) : S(0);
+    }
+    if (valid) {
+      if (fnow) {
+        s[48] += 1.0;
+        hash += mix64((unsigned long long)i);
+        const R xi = x[i], gi = g[i];
+        const R zi = uncon ? xi : gcp_point<R, S>(code, xi, gi, R(0), R(0), tsum);
+        const S r = reduced_grad<R, S>(uncon, xi, zi, gi, col, yv, sv, a1, a2);
+#pragma unroll
+        for (int j = 0; j < kMaxM; j++) {
+          if (j < col) {
+            s[j] = fma((double)yv[j], (double)r, s[j]);
+            s[8 + j] = fma((double)sv[j], (double)r, s[8 + j]);
+          }
+        }
+        if (updatd) {
+          double ynew = 0;
+#pragma unroll
+          for (int j = 0; j < kMaxM; j++)
+            if (j == newest) ynew = (double)yv[j];
+#pragma unroll
+          for (int j = 0; j < kMaxM; j++) {
+            if (j < col) {
+              s[16 + j] = fma(ynew, (double)yv[j], s[16 + j]);
+              s[40 + j] = fma((double)sv[j], ynew, s[40 + j]);
+            }
+          }
+        }
+      } else {
+        if (code == IW_LOW || code == IW_WALK_LOW) s[51] += 1.0;
+        if (code == IW_UPP || code == IW_WALK_UPP) s[52] += 1.0;
+        if (updatd) {
+          double snew = 0;
+#pragma unroll
+          for (int j = 0; j < kMaxM; j++)
+            if (j == newest) snew = (double)sv[j];
+#pragma unroll
+          for (int j = 0; j < kMaxM; j++) {
+            if (j < col) {
+              s[24 + j] = fma(snew, (double)sv[j], s[24 + j]);
+              s[32 + j] = fma(snew, (double)yv[j], s[32 + j]);
+            }
+          }
+        }
+      }
+      if (enter) s[49] += 1.0;
+      if (leave) s[50] += 1.0;
+    }
+    // entering (+) / leaving (-) corrections, one changed variable at a time per warp
+    uint32_t changed = __ballot_sync(0xffffffffu, enter || leave);
+    while (changed) {
+      const int src = __ffs(changed) - 1;
+      changed &= changed - 1;
+      const double sign = __shfl_sync(0xffffffffu, enter ? 1.0 : -1.0, src);
+#pragma unroll
+      for (int j = 0; j < kMaxM; j++) {
+        const double yj = __shfl_sync(0xffffffffu, (double)yv[j], src);
+        const double sj = __shfl_sync(0xffffffffu, (double)sv[j], src);
+        if (lane == 0) {
+          bc[warp][j] = yj;
+          bc[warp][kMaxM + j] = sj;
+        }
+      }
+      __syncwarp();
+#pragma unroll
+      for (int k = 0; k < kLaneOwned; k++) {
+        const int kind = ck[k];
+        if (kind < 3) {
+          const int a = ca[k], b = cb[k];
+          double va, vb;
+          if (kind == 0) {
+            va = bc[warp][a];
+            vb = bc[warp][b];
+          } else if (kind == 1) {
+            va = bc[warp][kMaxM + a];
+            vb = bc[warp][kMaxM + b];
+          } else {
+            va = bc[warp][kMaxM + a];
+            vb = bc[warp][b];
+          }
+          corr[k] = fma(sign * va, vb, corr[k]);
+        }
+      }
+      __syncwarp();
+    }
+  }
+  // the free-set hash sums mod 2^64 (order free), one atomic per warp
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) hash += __shfl_xor_sync(0xffffffffu, hash, o);
+  if (lane == 0 && hash != 0) atomicAdd(&st->free_hash_acc, hash);
+
+  constexpr int W = NS + 32 * kLaneOwned;
+  double xm[1] = {0.0};
+  MinPair mn[1] = {MinPair{0.0, 0}};
+  cta_reduce_to_row<NS, 0, 0, kLaneOwned>(s, xm, mn, corr, c.part, W);
+  if (!last_cta(c.ticket)) return;
+  __shared__ double red[W];
+  fold_rows(c.part, gridDim.x, W, W, 0, 0, red);
+  __shared__ SmallWork<S> sw;
+  if (threadIdx.x != 0) return;
+
+  // epilogue: freev's counts and wrk (1143-1161), formk (907-1103), subsm's K solves
+  // (1459-1471)
+  const int nfree = (int)red[48];
+  if (!uncon) {
+    st->nfree = nfree;
+    st->nenter = (int)red[49];
+    st->nleave = (int)red[50];
+    st->wrk = (st->nleave > 0 || st->nenter > 0 || updatd) ? 1 : 0;
+  } else {
+    st->wrk = updatd ? 1 : 0;
+    st->nenter = 0;
+    st->nleave = 0;
+  }
+  st->free_hash = st->free_hash_acc;
+  st->free_hash_acc = 0;
+  st->at_lower = (unsigned long long)red[51];
+  st->at_upper = (unsigned long long)red[52];
+  st->subsm_active = (st->nfree != 0 && col != 0) ? 1 : 0;
+  if (!st->subsm_active) return;
+  if (st->wrk) {
+    FormkSums<S>& fs = sw.fs;
+    for (int j = 0; j < kMaxM; j++) {
+      fs.yy_new[j] = (S)red[16 + j];
+      fs.ss_new[j] = (S)red[24 + j];
+      fs.sy_row[j] = (S)red[32 + j];
+      fs.sy_col[j] = (S)red[40 + j];
+    }
+    for (int q = 0; q < 32 * kLaneOwned; q++) {
+      int kind, a, b;
+      corr_map(q, kind, a, b);
+      if (kind >= 3) continue;
+      const S v = (S)red[NS + q];
+      if (kind == 0) fs.dyy[a][b] = v;
+      if (kind == 1) fs.dss[a][b] = v;
+      if (kind == 2) fs.dsy[a][b] = v;
+    }
+    const int info = sformk<S>(st->m, col, st->updatd, st->iupdat, theta, st->sy, st->wn,
+                               st->wn1, fs, sw.work, sw.wm);
+    if (info != 0) {
+      st->internal_fail = info;
+      return;
+    }
+  }
+  S* wv = sw.wv;
+  for (int j = 1; j <= col; j++) {
+    wv[j] = (S)red[j - 1];
+    wv[col + j] = theta * (S)red[8 + j - 1];
+  }
+  int info = 0;
+  sdtrsl(st->wn, 2 * kMaxM, 2 * col, wv, 11, &info);
+  if (info != 0) {
+    st->internal_fail = info;
+    return;
+  }
+  for (int j = 1; j <= col; j++) wv[j] = -wv[j];
+  sdtrsl(st->wn, 2 * kMaxM, 2 * col, wv, 1, &info);
+  if (info != 0) {
+    st->internal_fail = info;
+    return;
+  }
+  for (int j = 1; j <= 2 * col; j++) st->wv[j] = wv[j];
+}
+
+// ------------------------------------------------------------------------------------
+// C: subspace direction on the free set and the step to the first bound it meets.
+template <typename R, typename H, typename S>
+__global__ void __launch_bounds__(kThreads) k_subsm_dir(Ctx<R, H, S> c, const R* __restrict__ x,
+                                                        const R* __restrict__ g) {
+  DevState<S>* st = c.st;
+  if (st->gcp_state == GCP_WALK || st->internal_fail != 0 || !st->subsm_active) return;
+  const int n = c.n, col = st->col;
+  const bool uncon = st->uncon_branch != 0;
+  const S theta = st->theta, tsum = st->tsum;
+  const H *Y[kMaxM], *Sl[kMaxM];
+  ring_ptrs(st, c.wy, n, Y);
+  ring_ptrs(st, c.ws, n, Sl);
+  S a1[kMaxM + 1], a2[kMaxM], w1[kMaxM], w2[kMaxM];
+#pragma unroll
+  for (int j = 0; j < kMaxM; j++) {
+    a1[j] = (j < col) ? st->mc[1 + j] : S(0);
+    a2[j] = (j < col) ? theta * st->mc[col + 1 + j] : S(0);
+    w1[j] = (j < col) ? st->wv[1 + j] : S(0);
+    w2[j] = (j < col) ? st->wv[col + 1 + j] : S(0);
+  }
+  a1[kMaxM] = theta;
+  MinPair mn[1] = {MinPair{INFINITY, kNoIndex}};
+  for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < n;
+       i += (long long)gridDim.x * kThreads) {
+    const int code = c.code[i];
+    if (!(uncon || iw_free(code))) continue;
+    S yv[kMaxM], sv[kMaxM];
+#pragma unroll
+    for (int j = 0; j < kMaxM; j++) {
+      yv[j] = (j < col) ? (S)HistTraits<H>::load(Y[j] + i) : S(0);
+      sv[j] = (j < col) ? (S)HistTraits<H>::load(Sl[j] + i) : S(0);
+    }
+    const R xi = x[i], gi = g[i];
+    const R li = c.l[i], ui = c.u[i];
+    const R zi = uncon ? xi : gcp_point<R, S>(code, xi, gi, li, ui, tsum);
+    S d = reduced_grad<R, S>(uncon, xi, zi, gi, col, yv, sv, a1, a2);
+#pragma unroll
+    for (int j = 0; j < kMaxM; j++)
+      if (j < col) d = d + yv[j] * w1[j] / theta + sv[j] * w2[j];
+    d = d / theta;
+    const R dr = (R)d;
+    c.dsub[i] = dr;
+    // candidate step to the bound (1486-1516), filtered as for alpha = 1
+    const int nb = c.nbd[i];
+    const S dk = (S)dr;
+    if (nb != 0) {
+      double cand = INFINITY;
+      if (dk < S(0) && nb <= 2) {
+        const S temp2 = (S)li - (S)zi;
+        if (temp2 >= S(0))
+          cand = 0.0;
+        else if (dk * S(1) < temp2)
+          cand = (double)(temp2 / dk);
+      } else if (dk > S(0) && nb >= 2) {
+        const S temp2 = (S)ui - (S)zi;
+        if (temp2 <= S(0))
+          cand = 0.0;
+        else if (dk * S(1) > temp2)
+          cand = (double)(temp2 / dk);
+      }
+      mn[0] = minpair(mn[0], MinPair{cand, i});
+    }
+  }
+  constexpr int W = 2;
+  double sdum[1] = {0.0}, xdum[1] = {0.0}, ldum[1] = {0.0};
+  cta_reduce_to_row<0, 0, 1, 0>(sdum, xdum, mn, ldum, c.part, W);
+  if (!last_cta(c.ticket)) return;
+  __shared__ double red[W];
+  fold_rows(c.part, gridDim.x, W, 0, 0, 1, red);
+  if (threadIdx.x != 0) return;
+  const S cand = (S)red[0];
+  if (cand < S(1)) {
+    st->alpha = cand;
+    st->ibd = (int)red[1];
+    st->iword = 1;
+  } else {
+    st->alpha = 1;
+    st->ibd = -1;
+    st->iword = 0;
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// D: apply the subspace step, form z and d = z - x, and start the line search.
+template <typename R, typename H, typename S>
+__global__ void __launch_bounds__(kThreads) k_subsm_apply(Ctx<R, H, S> c, const R* __restrict__ x,
+                                                          const R* __restrict__ g, R* __restrict__ z) {
+  DevState<S>* st = c.st;
+  if (st->gcp_state == GCP_WALK || st->internal_fail != 0) return;
+  const int n = c.n;
+  const bool uncon = st->uncon_branch != 0;
+  const bool sub = st->subsm_active != 0;
+  const S alpha = sub ? st->alpha : S(1), tsum = st->tsum;
+  const long long ibd = sub ? st->ibd : -1;
+  const bool want_stpmx = st->cnstnd && st->iter > 0;
+  const R big = (R)1.0e10;
+  double s[2] = {0.0, 0.0};
+  MinPair mn[1] = {MinPair{INFINITY, kNoIndex}};
+  for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < n;
+       i += (long long)gridDim.x * kThreads) {
+    const R xi = x[i], gi = g[i], li = c.l[i], ui = c.u[i];
+    const int code = c.code[i];
+    R zi = uncon ? xi : gcp_point<R, S>(code, xi, gi, li, ui, tsum);
+    if (sub && (uncon || iw_free(code))) {
+      S dk = (S)c.dsub[i];
+      if (i == ibd) {
+        if (dk > S(0)) {
+          zi = ui;
+          dk = 0;
+        } else if (dk < S(0)) {
+          zi = li;
+          dk = 0;
+        }
+      }
+      zi = (R)((S)zi + alpha * dk);
+    }
+    z[i] = zi;
+    const R d = rsub(zi, xi);
+    s[0] = fma((double)d, (double)d, s[0]);
+    s[1] = fma((double)gi, (double)d, s[1]);
+    if (want_stpmx) {
+      const int nb = c.nbd[i];
+      if (nb != 0) {
+        double cand = INFINITY;
+        if (d < R(0) && nb <= 2) {
+          const R a2 = rsub(li, xi);
+          if (a2 >= R(0))
+            cand = 0.0;
+          else if (rmul(d, big) < a2)
+            cand = (double)rdiv(a2, d);
+        } else if (d > R(0) && nb >= 2) {
+          const R a2 = rsub(ui, xi);
+          if (a2 <= R(0))
+            cand = 0.0;
+          else if (rmul(d, big) > a2)
+            cand = (double)rdiv(a2, d);
+        }
+        mn[0] = minpair(mn[0], MinPair{cand, i});
+      }
+    }
+  }
+  constexpr int W = 4;
+  double xdum[1] = {0.0}, ldum[1] = {0.0};
+  cta_reduce_to_row<2, 0, 1, 0>(s, xdum, mn, ldum, c.part, W);
+  if (!last_cta(c.ticket)) return;
+  __shared__ double red[W];
+  fold_rows(c.part, gridDim.x, W, 2, 0, 1, red);
+  if (threadIdx.x != 0) return;
+
+  // lnsrlb with task != 1 (1263-1311), then its first dcsrch call (1312-1338)
+  const S sbig = (S)1.0e10;
+  st->dtd = (S)red[0];
+  st->dnrm = ssqrt(st->dtd);
+  st->stpmx = sbig;
+  if (st->cnstnd) {
+    if (st->iter == 0)
+      st->stpmx = 1;
+    else if ((S)red[2] < st->stpmx)
+      st->stpmx = (S)red[2];
+  }
+  if (st->iter == 0 && !st->boxed)
+    st->stp = smin((S)1 / st->dnrm, st->stpmx);
+  else
+    st->stp = 1;
+  st->fold = st->f;
+  st->ifun = 0;
+  st->iback = 0;
+  st->csave = 0;
+  st->gd = (S)red[1];
+  st->gdold = st->gd;
+  st->ls_info = 0;
+  if (st->gd >= S(0)) {
+    st->ls_info = -4;
+    return;
+  }
+  sdcsrch<S>(st->f, st->gd, st->stp, (S)1.0e-3, (S)0.9, (S)0.1, (S)0, st->stpmx, st->csave,
+             st->ls);
+  st->xstep = st->stp * st->dnrm;
+  if (st->csave != 4 && st->csave != 3) {
+    st->ls_task = 1;
+    st->ifun = st->ifun + 1;
+    st->nfgv = st->nfgv + 1;
+    st->iback = st->ifun - 1;
+  } else {
+    st->ls_task = 5;
+  }
+}
+
+// Trial point x = stp*d + t with d = z - t (lbfgsbcpu.cpp:1332-1334).
+template <typename R, typename S>
+__global__ void k_trial(int n, const R* __restrict__ t, const R* __restrict__ z, R* __restrict__ xt,
+                        const DevState<S>* st) {
+  const R stp = (R)st->stp;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const R ti = t[i];
+    const R d = rsub(z[i], ti);
+    xt[i] = radd(rmul(stp, d), ti);
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// E: after a function evaluation at xt (gradient gt; t and go are the point and the
+// gradient where the line search started).
+template <typename R, typename H, typename S>
+__global__ void __launch_bounds__(kThreads) k_post_eval(Ctx<R, H, S> c, const R* __restrict__ t,
+                                                        const R* __restrict__ z,
+                                                        const R* __restrict__ xt,
+                                                        const R* __restrict__ gt,
+                                                        const R* __restrict__ go, S f,
+                                                        int force_accept) {
+  DevState<S>* st = c.st;
+  const int n = c.n, col = st->col;
+  const R stp = (R)st->stp;
+  const bool unit = st->stp == S(1);
+  const H *Y[kMaxM], *Sl[kMaxM];
+  ring_ptrs(st, c.wy, n, Y);
+  ring_ptrs(st, c.ws, n, Sl);
+  H* ysp = c.wy + (size_t)st->spare * n;
+  H* ssp = c.ws + (size_t)st->spare * n;
+  // sums: [0] g'd, [1] |xold - x|^2, [2] y'y, [3..10] s'y_j, [11..18] s_j's; max: |proj g|
+  constexpr int NS = 19, NX = 1;
+  double s[NS], xm[NX] = {0.0};
+#pragma unroll
+  for (int k = 0; k < NS; k++) s[k] = 0.0;
+  for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < n;
+       i += (long long)gridDim.x * kThreads) {
+    const R ti = t[i], zi = z[i], xi = xt[i], gi = gt[i], gold = go[i];
+    const R d = rsub(zi, ti);
+    s[0] = fma((double)gi, (double)d, s[0]);
+    // projgr (1389-1414)
+    const int nb = c.nbd[i];
+    R pg = gi;
+    if (nb != 0) {
+      if (gi < R(0)) {
+        if (nb >= 2) pg = smax<R>(rsub(xi, c.u[i]), gi);
+      } else {
+        if (nb <= 2) pg = smin<R>(rsub(xi, c.l[i]), gi);
+      }
+    }
+    const double apg = fabs((double)pg);
+    xm[0] = (apg > xm[0]) ? apg : xm[0];
+    const R xd = rsub(ti, xi);
+    s[1] = fma((double)xd, (double)xd, s[1]);
+    const R y = rsub(gi, gold);
+    s[2] = fma((double)y, (double)y, s[2]);
+    const R sv = unit ? d : rmul(d, stp);
+#pragma unroll
+    for (int j = 0; j < kMaxM; j++) {
+      if (j < col) {
+        s[3 + j] = fma((double)sv, (double)HistTraits<H>::load(Y[j] + i), s[3 + j]);
+        s[11 + j] = fma((double)HistTraits<H>::load(Sl[j] + i), (double)sv, s[11 + j]);
+      }
+    }
+    ssp[i] = HistTraits<H>::from((double)sv);
+    ysp[i] = HistTraits<H>::from((double)y);
+  }
+  constexpr int W = NS + NX;
+  MinPair mdum[1] = {MinPair{0.0, 0}};
+  double ldum[1] = {0.0};
+  cta_reduce_to_row<NS, NX, 0, 0>(s, xm, mdum, ldum, c.part, W);
+  if (!last_cta(c.ticket)) return;
+  __shared__ double red[W];
+  fold_rows(c.part, gridDim.x, W, NS, NX, 0, red);
+  if (threadIdx.x != 0) return;
+
+  st->f = f;
+  st->gd = (S)red[0];
+  if (!force_accept) {
+    // lnsrlb with task == 1 (1312-1338)
+    sdcsrch<S>(f, st->gd, st->stp, (S)1.0e-3, (S)0.9, (S)0.1, (S)0, st->stpmx, st->csave,
+               st->ls);
+    st->xstep = st->stp * st->dnrm;
+    if (st->csave != 4 && st->csave != 3) {
+      st->ls_task = 1;
+      st->ifun = st->ifun + 1;
+      st->nfgv = st->nfgv + 1;
+      st->iback = st->ifun - 1;
+      return;
+    }
+    st->ls_task = 5;
+  }
+  // accepted: quantities of the stopping tests (394-417)
+  st->iter = st->iter + 1;
+  st->sbgnrm = (S)red[NS];
+  st->tf = ssqrt((S)red[1]);
+  st->rr = (S)red[2];
+  // the update (431-461), carried out ahead of the host-side tests; if a test stops the
+  // solve the updated memory is simply discarded
+  S dr, ddum;
+  const S sstp = st->stp;
+  if (sstp == S(1)) {
+    dr = st->gd - st->gdold;
+    ddum = -st->gdold;
+  } else {
+    dr = (st->gd - st->gdold) * sstp;
+    ddum = -st->gdold * sstp;
+  }
+  st->dr = dr;
+  st->ddum_dr = ddum;
+  st->internal_fail = 0;
+  if ((double)dr <= 5e-16 * (double)ddum) {
+    st->updatd = 0;
+    return;
+  }
+  st->updatd = 1;
+  st->iupdat = st->iupdat + 1;
+  const int m = st->m;
+  int shifted = 0;
+  if (st->iupdat <= m) {
+    st->col = st->iupdat;
+    st->itail = (st->head + st->iupdat - 2) % m + 1;
+  } else {
+    st->itail = st->itail % m + 1;
+    st->head = st->head % m + 1;
+    shifted = 1;
+  }
+  const int old = st->phys[st->itail];
+  st->phys[st->itail] = st->spare;
+  st->spare = old;
+  st->theta = st->rr / dr;
+  const int ncol = st->col;
+  constexpr int ld = kMaxM;
+  if (st->iupdat > m) {
+    for (int j = 1; j <= ncol - 1; j++) {
+      for (int i = 1; i <= j; i++) LB_AT(st->ss, ld, i, j) = LB_AT(st->ss, ld, i + 1, j + 1);
+      for (int i = j; i <= ncol - 1; i++) LB_AT(st->sy, ld, i, j) = LB_AT(st->sy, ld, i + 1, j + 1);
+    }
+  }
+  for (int j = 1; j <= ncol - 1; j++) {
+    LB_AT(st->sy, ld, ncol, j) = (S)red[3 + j - 1 + shifted];
+    LB_AT(st->ss, ld, j, ncol) = (S)red[11 + j - 1 + shifted];
+  }
+  LB_AT(st->ss, ld, ncol, ncol) = (sstp == S(1)) ? st->dtd : sstp * sstp * st->dtd;
+  LB_AT(st->sy, ld, ncol, ncol) = dr;
+  const int info = sformt<S>(st->wt, st->sy, st->ss, ncol, st->theta);
+  if (info != 0) st->internal_fail = info;
+}
+
+// ------------------------------------------------------------------------------------
+// Set-up: errclb (871-905), lbfgsbactive (467-515) into the solver's x buffer.
+template <typename R, typename S>
+__global__ void k_init(int n, const R* __restrict__ x_in, R* __restrict__ x, const int* __restrict__ nbd,
+                       const R* __restrict__ l, const R* __restrict__ u, DevState<S>* st) {
+  int err = 0, any_c = 0, not_boxed = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int nb = nbd[i];
+    const R li = l[i], ui = u[i];
+    R xi = x_in[i];
+    if (nb < 0 || nb > 3) err |= 1;
+    if (nb == 2 && li > ui) err |= 2;
+    if (nb > 0) {
+      if (nb <= 2 && xi <= li) {
+        if (xi < li) xi = li;
+      } else if (nb >= 2 && xi >= ui) {
+        if (xi > ui) xi = ui;
+      }
+    }
+    x[i] = xi;
+    if (nb != 2) not_boxed = 1;
+    if (nb != 0) any_c = 1;
+  }
+  err = __reduce_or_sync(0xffffffffu, err);
+  any_c = __reduce_or_sync(0xffffffffu, any_c);
+  not_boxed = __reduce_or_sync(0xffffffffu, not_boxed);
+  if ((threadIdx.x & 31) == 0) {
+    if (err) atomicOr(&st->input_error, err);
+    if (any_c) atomicOr(&st->cnstnd, 1);
+    if (not_boxed) atomicAnd(&st->boxed, 0);
+  }
+}
+
+// projgr at the start point (lbfgsbcpu.cpp:272-273); also records f.
+template <typename R, typename H, typename S>
+__global__ void __launch_bounds__(kThreads) k_projgr(Ctx<R, H, S> c, const R* __restrict__ x,
+                                                     const R* __restrict__ g, S f) {
+  double xm[1] = {0.0};
+  for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < c.n;
+       i += (long long)gridDim.x * kThreads) {
+    const R xi = x[i], gi = g[i];
+    const int nb = c.nbd[i];
+    R pg = gi;
+    if (nb != 0) {
+      if (gi < R(0)) {
+        if (nb >= 2) pg = smax<R>(rsub(xi, c.u[i]), gi);
+      } else {
+        if (nb <= 2) pg = smin<R>(rsub(xi, c.l[i]), gi);
+      }
+    }
+    const double a = fabs((double)pg);
+    xm[0] = (a > xm[0]) ? a : xm[0];
+  }
+  double sdum[1] = {0.0}, ldum[1] = {0.0};
+  MinPair mdum[1] = {MinPair{0.0, 0}};
+  cta_reduce_to_row<0, 1, 0, 0>(sdum, xm, mdum, ldum, c.part, 1);
+  if (!last_cta(c.ticket)) return;
+  __shared__ double red[1];
+  fold_rows(c.part, gridDim.x, 1, 0, 1, 0, red);
+  if (threadIdx.x != 0) return;
+  c.st->sbgnrm = (S)red[0];
+  c.st->f = f;
+}
+
+// The memory reset of the reference driver (col = 0, head = 1, theta = 1, iupdat = 0,
+// updatd = false), and the branch flags of the next iteration.
+template <typename S>
+__global__ void k_begin_iteration(DevState<S>* st, int reset) {
+  if (reset) {
+    st->col = 0;
+    st->head = 1;
+    st->theta = 1;
+    st->iupdat = 0;
+    st->updatd = 0;
+  }
+  st->internal_fail = 0;
+  st->uncon_branch = (!st->cnstnd && st->col > 0) ? 1 : 0;
+  st->subsm_active = 0;
+  st->iword = -1;
+  st->free_hash = 0;
+  st->ls_info = 0;
+  if (st->uncon_branch) {
+    // z = x, wrk = updatd, nint = 0 (lbfgsbcpu.cpp:281-284)
+    st->gcp_state = GCP_SKIPPED;
+    st->tsum = 0;
+    st->nint = 0;
+  }
+}
+
+}  // namespace lbfgsb_b200

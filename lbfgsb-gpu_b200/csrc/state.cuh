@@ -1,0 +1,59 @@
+// state.cuh -- the solver's device-resident state and reduction scratch.
+//
+// Every scalar the reference keeps in local variables of lbfgsbminimize
+// (culbfgsb/lbfgsbcpu.cpp:132-245: col, head, itail, iupdat, theta, the line-search
+// scalars, the dcsrch save arrays, the m x m and 2m x 2m matrices) lives here, in device
+// memory, and is advanced by the epilogues of the streaming passes.  The host reads the
+// control header (everything before `big`) after each synchronisation point.
+#pragma once
+
+#include "common.cuh"
+#include "small.cuh"
+
+namespace lbfgsb_b200 {
+
+// gcp_state
+enum : int { GCP_DONE = 0, GCP_WALK = 1, GCP_EARLY = 2, GCP_SKIPPED = 3 };
+// ls_task: 1 = evaluate f, g at the trial point, 5 = the line search has converged
+// fail codes (internal_fail): nonzero requests the memory reset of the reference driver.
+
+template <typename S>
+struct DevState {
+  // ---------------- control header (copied to the host) ----------------
+  int n, m, cnstnd, boxed;
+  int col, head, itail, iupdat, updatd;
+  int iter, ifun, iback, nfgv, ls_info, ls_task, csave;
+  int gcp_state, nint, bnded, iword, subsm_active, wrk, uncon_branch;
+  int internal_fail;   // 0, or the info code of a failed small-matrix step
+  int input_error;     // errclb: bit 0 nbd out of range, bit 1 l > u on a boxed variable
+  int ibkmin, ibd;
+  int nbreak, nleft, nfree_mov, nfree, nenter, nleave;
+  int pad0;
+  unsigned long long free_hash, free_hash_acc, at_lower, at_upper;
+  S theta, f, fold, gd, gdold, stp, dnrm, dtd, xstep, stpmx;
+  S sbgnrm, tf, rr, dr, ddum_dr;
+  S f1, f2, f2org, dtm, tsum, tj, bkmin, alpha, f1_0, f2_0;
+  // ---------------- large part ----------------
+  S big;  // marks the end of the header
+  int phys[kMaxM + 1];  // physical history slot of ring index r = 1..m
+  int spare;            // physical slot receiving the speculative (s, y) pair
+  S sy[kMaxM * kMaxM], ss[kMaxM * kMaxM], wt[kMaxM * kMaxM];
+  S wn[4 * kMaxM * kMaxM], wn1[4 * kMaxM * kMaxM];
+  S p[2 * kMaxM + 1], c[2 * kMaxM + 1], mc[2 * kMaxM + 1], wv[2 * kMaxM + 1];  // 1-based
+  S prod_sy[kMaxM], prod_ss[kMaxM];  // s'y_j and s_j's of the pending pair, old positions
+  LineSearchSave<S> ls;
+};
+
+// A (value, index) pair reduced by minimum value, ties to the lower index.  kNoIndex
+// marks "no candidate" (exactly representable in the double rows of the reduction).
+constexpr long long kNoIndex = 1LL << 62;
+struct MinPair {
+  double v;
+  long long i;
+};
+__host__ __device__ __forceinline__ MinPair minpair(MinPair a, MinPair b) {
+  if (b.v < a.v || (b.v == a.v && b.i < a.i)) return b;
+  return a;
+}
+
+}  // namespace lbfgsb_b200

@@ -1,0 +1,309 @@
+"""ctypes binding of liblbfgsb_b200.so for tests, smoke and bench.
+
+The library itself is C++/CUDA behind the C ABI of include/lbfgsb_b200.h; this module only
+loads it (and fails loudly if it has not been built: there is no fallback), mirrors the
+structs, and offers a small driver that runs one solve on device buffers allocated with
+torch.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import hashlib
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblbfgsb_b200.so")
+
+MODE_NO_ACCELERATION, MODE_CUDA = 0, 1
+FORM_PLAIN, FORM_MIXED, FORM_MIXED_BF16 = 0, 1, 2
+MAX_KERNELS = 16
+
+
+class OptionF64(C.Structure):
+    _fields_ = [("machine_epsilon", C.c_double), ("machine_maximum", C.c_double),
+                ("step_scaling", C.c_double), ("eps_g", C.c_double), ("eps_f", C.c_double),
+                ("eps_x", C.c_double), ("hessian_approximate_dimension", C.c_int),
+                ("max_iteration", C.c_int), ("mode", C.c_int)]
+
+
+class OptionF32(C.Structure):
+    _fields_ = [("machine_epsilon", C.c_float), ("machine_maximum", C.c_float),
+                ("step_scaling", C.c_float), ("eps_g", C.c_float), ("eps_f", C.c_float),
+                ("eps_x", C.c_float), ("hessian_approximate_dimension", C.c_int),
+                ("max_iteration", C.c_int), ("mode", C.c_int)]
+
+
+class SummaryF64(C.Structure):
+    _fields_ = [("residual_g", C.c_double), ("residual_f", C.c_double),
+                ("residual_x", C.c_double), ("num_iteration", C.c_int), ("info", C.c_int)]
+
+
+class SummaryF32(C.Structure):
+    _fields_ = [("residual_g", C.c_float), ("residual_f", C.c_float),
+                ("residual_x", C.c_float), ("num_iteration", C.c_int), ("info", C.c_int)]
+
+
+class TraceRecord(C.Structure):
+    _fields_ = [("iter", C.c_int), ("nint", C.c_int), ("nbreak", C.c_int), ("nfree", C.c_int),
+                ("nenter", C.c_int), ("nleave", C.c_int), ("col", C.c_int), ("head", C.c_int),
+                ("nfgv", C.c_int), ("ifun", C.c_int), ("iword", C.c_int), ("reset", C.c_int),
+                ("free_hash", C.c_ulonglong), ("at_lower", C.c_ulonglong),
+                ("at_upper", C.c_ulonglong), ("f", C.c_double), ("theta", C.c_double),
+                ("stp", C.c_double), ("dtm", C.c_double), ("tsum", C.c_double),
+                ("gd", C.c_double), ("gdold", C.c_double), ("dtd", C.c_double),
+                ("stpmx", C.c_double), ("f1_0", C.c_double), ("f2_0", C.c_double),
+                ("dbg", C.c_double * 8)]
+
+
+TRACE_CB = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(TraceRecord))
+
+
+class Ext(C.Structure):
+    _fields_ = [("form", C.c_int), ("profile", C.c_int), ("trace", TRACE_CB),
+                ("trace_user", C.c_void_p)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("kernels", C.c_int), ("name", (C.c_char * 32) * MAX_KERNELS),
+                ("launches", C.c_longlong * MAX_KERNELS), ("ms", C.c_double * MAX_KERNELS),
+                ("bytes", C.c_double * MAX_KERNELS), ("total_launches", C.c_longlong),
+                ("host_syncs", C.c_longlong), ("evaluations", C.c_longlong),
+                ("bytes_per_iteration_model", C.c_double)]
+
+
+CB64 = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                   C.POINTER(C.c_double), C.c_void_p, C.POINTER(SummaryF64))
+CB32 = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                   C.POINTER(C.c_float), C.c_void_p, C.POINTER(SummaryF32))
+
+# every symbol include/lbfgsb_b200.h declares
+EXPORTS = [
+    "lbfgsb_b200_default_option_f64", "lbfgsb_b200_default_option_f32",
+    "lbfgsb_b200_minimize_f64", "lbfgsb_b200_minimize_f32",
+    "lbfgsb_b200_minimize_ext_f64", "lbfgsb_b200_minimize_ext_f32",
+    "lbfgsb_b200_last_stats", "lbfgsb_b200_last_error", "lbfgsb_b200_synth_create",
+    "lbfgsb_b200_synth_destroy", "lbfgsb_b200_synth_funcgrad_f64",
+    "lbfgsb_b200_synth_funcgrad_f32", "lbfgsb_b200_copy",
+]
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load the built library; raises if it is missing (build with build.py)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with lbfgsb-gpu_b200/build.py "
+                           "(there is no CPU fallback)")
+    lib = C.CDLL(LIB_PATH)
+    for sfx, real, opt, summ, cb in (("f64", C.c_double, OptionF64, SummaryF64, CB64),
+                                     ("f32", C.c_float, OptionF32, SummaryF32, CB32)):
+        fn = getattr(lib, f"lbfgsb_b200_minimize_ext_{sfx}")
+        fn.restype = C.c_int
+        fn.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                       C.POINTER(opt), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                       C.c_void_p, C.POINTER(Ext), C.POINTER(summ)]
+        fn = getattr(lib, f"lbfgsb_b200_minimize_{sfx}")
+        fn.restype = C.c_int
+        fn.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                       C.POINTER(opt), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                       C.c_void_p, C.POINTER(summ)]
+        fn = getattr(lib, f"lbfgsb_b200_default_option_{sfx}")
+        fn.restype = None
+        fn.argtypes = [C.POINTER(opt)]
+    lib.lbfgsb_b200_last_stats.restype = C.c_int
+    lib.lbfgsb_b200_last_stats.argtypes = [C.POINTER(Stats)]
+    lib.lbfgsb_b200_last_error.restype = C.c_char_p
+    lib.lbfgsb_b200_synth_create.restype = C.c_void_p
+    lib.lbfgsb_b200_synth_create.argtypes = [C.c_int] + [C.c_void_p] * 4 + [C.c_int]
+    lib.lbfgsb_b200_synth_destroy.restype = None
+    lib.lbfgsb_b200_synth_destroy.argtypes = [C.c_void_p]
+    lib.lbfgsb_b200_copy.restype = C.c_int
+    lib.lbfgsb_b200_copy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
+    _lib = lib
+    return lib
+
+
+def default_option(dtype):
+    lib = load()
+    if np.dtype(dtype) == np.float64:
+        o = OptionF64()
+        lib.lbfgsb_b200_default_option_f64(C.byref(o))
+    else:
+        o = OptionF32()
+        lib.lbfgsb_b200_default_option_f32(C.byref(o))
+    return o
+
+
+def last_stats() -> dict:
+    st = Stats()
+    load().lbfgsb_b200_last_stats(C.byref(st))
+    out = {"kernels": {}, "total_launches": st.total_launches, "host_syncs": st.host_syncs,
+           "evaluations": st.evaluations,
+           "bytes_per_iteration_model": st.bytes_per_iteration_model}
+    for k in range(st.kernels):
+        name = bytes(st.name[k]).split(b"\0", 1)[0].decode()
+        out["kernels"][name] = {"launches": st.launches[k], "ms": st.ms[k],
+                                "bytes": st.bytes[k]}
+    return out
+
+
+class SynthObjective:
+    """The device objective of csrc/objective.cu for a synth.py problem."""
+
+    def __init__(self, prob: dict, single_precision_fields: bool = False):
+        lib = load()
+        self._fields = [np.ascontiguousarray(prob[k], dtype=np.float64)
+                        for k in ("kappa", "w", "t", "b")]
+        self.handle = lib.lbfgsb_b200_synth_create(
+            int(prob["s"]), *[a.ctypes.data for a in self._fields],
+            1 if single_precision_fields else 0)
+        if not self.handle:
+            raise RuntimeError("lbfgsb_b200_synth_create failed")
+        self.f64 = C.cast(lib.lbfgsb_b200_synth_funcgrad_f64, C.c_void_p).value
+        self.f32 = C.cast(lib.lbfgsb_b200_synth_funcgrad_f32, C.c_void_p).value
+
+    def close(self):
+        if self.handle:
+            load().lbfgsb_b200_synth_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _digest(a: np.ndarray) -> str:
+    return hashlib.sha1(np.ascontiguousarray(a).tobytes()).hexdigest()[:16]
+
+
+@dataclass
+class GpuResult:
+    x: np.ndarray
+    info: int
+    num_iteration: int
+    residual_g: float
+    residual_f: float
+    residual_x: float
+    status: int
+    evals: list = field(default_factory=list)
+    iters: list = field(default_factory=list)
+    trace: list = field(default_factory=list)
+    stats: dict = field(default_factory=dict)
+
+
+_TRACE_KEYS = [f for f, _ in TraceRecord._fields_]
+
+
+def solve(prob: dict, dtype=np.float64, x0=None, option=None, objective: str = "host",
+          form: int = FORM_PLAIN, trace: bool = False, record: bool = True,
+          custom_stop_at: int | None = None, profile: bool = False, stream=None) -> GpuResult:
+    """One solve on the GPU through the C ABI.
+
+    objective="host": funcgrad copies x to the host and evaluates the CPU objective of
+    oracle/objective.c (so f and g are bit-identical to what the oracle sees);
+    objective="device": the device objective of csrc/objective.cu (synthetic problems).
+    """
+    import torch
+
+    lib = load()
+    dtype = np.dtype(dtype)
+    is64 = dtype == np.float64
+    tdt = torch.float64 if is64 else torch.float32
+    n = int(prob["nbd"].size)
+    dev = torch.device("cuda:0")
+    x_np = np.zeros(n, dtype=dtype) if x0 is None else np.asarray(x0, dtype=dtype)
+    x = torch.from_numpy(np.ascontiguousarray(x_np)).to(dev)
+    l = torch.from_numpy(np.ascontiguousarray(prob["l"], dtype=dtype)).to(dev)
+    u = torch.from_numpy(np.ascontiguousarray(prob["u"], dtype=dtype)).to(dev)
+    nbd = torch.from_numpy(np.ascontiguousarray(prob["nbd"], dtype=np.int32)).to(dev)
+    opt = option if option is not None else default_option(dtype)
+    summ = SummaryF64() if is64 else SummaryF32()
+    cbt = CB64 if is64 else CB32
+    res = GpuResult(x=x_np, info=0, num_iteration=0, residual_g=0, residual_f=0,
+                    residual_x=0, status=0)
+    keep = []
+    user = None
+    if objective == "host":
+        import sys
+        repo = os.path.dirname(HERE)
+        if repo not in sys.path:
+            sys.path.insert(0, repo)
+        from oracle import binding as OB  # test glue: the CPU objective of the oracle
+        ev = OB.host_objective(prob, dtype)
+        hx = np.zeros(n, dtype=dtype)
+        hg = np.zeros(n, dtype=dtype)
+        real = C.c_double if is64 else C.c_float
+        fbox = (real * 1)()
+
+        def fg(_user, xp, fp, gp, _stream, _sp):
+            torch.cuda.current_stream().synchronize()
+            lib.lbfgsb_b200_copy(hx.ctypes.data, C.cast(xp, C.c_void_p), hx.nbytes, 2)
+            ev(hx.ctypes.data_as(C.POINTER(real)), fbox, hg.ctypes.data_as(C.POINTER(real)))
+            lib.lbfgsb_b200_copy(C.cast(gp, C.c_void_p), hg.ctypes.data, hg.nbytes, 1)
+            fp[0] = fbox[0]
+            if record:
+                res.evals.append((float(fbox[0]), _digest(hx)))
+            return 0
+
+        cb = cbt(fg)
+        keep.append(cb)
+        fg_ptr = C.cast(cb, C.c_void_p).value
+    elif objective == "device":
+        so = SynthObjective(prob, single_precision_fields=not is64)
+        keep.append(so)
+        user = so.handle
+        fg_ptr = so.f64 if is64 else so.f32
+    else:
+        raise ValueError(objective)
+
+    def after(_user, xp, fp, gp, _stream, sp):
+        if record:
+            s = sp[0]
+            res.iters.append((s.num_iteration, float(s.residual_g), float(s.residual_f),
+                              float(s.residual_x), float(fp[0])))
+        return 0
+
+    def stop(_user, xp, fp, gp, _stream, sp):
+        return 1 if (custom_stop_at is not None and sp[0].num_iteration >= custom_stop_at) else 0
+
+    cb_after = cbt(after)
+    keep.append(cb_after)
+    after_ptr = C.cast(cb_after, C.c_void_p).value if record else None
+    stop_ptr = None
+    if custom_stop_at is not None:
+        cb_stop = cbt(stop)
+        keep.append(cb_stop)
+        stop_ptr = C.cast(cb_stop, C.c_void_p).value
+
+    def tr(_user, rp):
+        r = rp[0]
+        res.trace.append({k: (list(getattr(r, k)) if k == 'dbg' else getattr(r, k)) for k in _TRACE_KEYS})
+
+    cb_tr = TRACE_CB(tr) if trace else TRACE_CB()
+    keep.append(cb_tr)
+    ext = Ext(form, 1 if profile else 0, cb_tr, None)
+    sfx = "f64" if is64 else "f32"
+    fn = getattr(lib, f"lbfgsb_b200_minimize_ext_{sfx}")
+    torch.cuda.synchronize()
+    status = fn(n, x.data_ptr(), nbd.data_ptr(), l.data_ptr(), u.data_ptr(), C.byref(opt),
+                fg_ptr, after_ptr, stop_ptr, user, stream, C.byref(ext), C.byref(summ))
+    torch.cuda.synchronize()
+    if status != 0:
+        raise RuntimeError(f"lbfgsb_b200 status {status}: {lib.lbfgsb_b200_last_error()}")
+    res.status = status
+    res.x = x.cpu().numpy()
+    res.info = summ.info
+    res.num_iteration = summ.num_iteration
+    res.residual_g = float(summ.residual_g)
+    res.residual_f = float(summ.residual_f)
+    res.residual_x = float(summ.residual_x)
+    res.stats = last_stats()
+    return res

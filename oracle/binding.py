@@ -53,7 +53,8 @@ class TraceRec(C.Structure):
                 ("at_upper", C.c_ulonglong), ("f", C.c_double), ("theta", C.c_double),
                 ("stp", C.c_double), ("dtm", C.c_double), ("tsum", C.c_double),
                 ("gd", C.c_double), ("gdold", C.c_double), ("dtd", C.c_double),
-                ("stpmx", C.c_double)]
+                ("stpmx", C.c_double), ("f1_0", C.c_double), ("f2_0", C.c_double),
+                ("dbg", C.c_double * 8)]
 
 
 CB64 = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
@@ -208,7 +209,7 @@ def run_cpu(which: str, prob: dict, dtype=np.float64, x0=None, option=None, reco
 
     def tr(user, recp):
         r = recp[0]
-        res.trace.append({k: getattr(r, k) for k in _TRACE_KEYS})
+        res.trace.append({k: (list(getattr(r, k)) if k == 'dbg' else getattr(r, k)) for k in _TRACE_KEYS})
 
     sfx = "f64" if is64 else "f32"
     P = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731

@@ -253,7 +253,7 @@ static void FN(hpsolb)(int n, REAL* t, int* iorder, int iheap) {
 
 typedef struct {
   int nbreak, nint, early; /* early: returned before the walk (no breakpoints, no free) */
-  REAL dtm, tsum;
+  REAL dtm, tsum, f1_0, f2_0;
 } FN(gcp_out);
 
 /* lbfgsbcauchy, lbfgsbcpu.cpp:567-817: generalized Cauchy point by the sequential
@@ -350,6 +350,8 @@ static void FN(cauchy)(int n, const REAL* x, const REAL* l, const REAL* u, const
     f2 = f2 - FN(dot)(&V1(v, 1), 1, &V1(p, 1), 1, col2);
   }
   dtm = -f1 / f2;
+  out->f1_0 = f1;
+  out->f2_0 = f2;
   tsum = 0;
   *nint = 1;
   if (nbreak != 0) {
@@ -1172,6 +1174,8 @@ void CAT2(orc_lbfgsb_minimize, SFX)(int n, REAL* x_, const int* nbd_, const REAL
     gout.nbreak = 0;
     gout.dtm = 0;
     gout.tsum = 0;
+    gout.f1_0 = 0;
+    gout.f2_0 = 0;
     nenter = 0;
     ileave = n + 1;
     if (!cnstnd && col > 0) {
@@ -1247,6 +1251,16 @@ void CAT2(orc_lbfgsb_minimize, SFX)(int n, REAL* x_, const int* nbd_, const REAL
     rec.theta = theta;
     rec.dtm = gout.dtm;
     rec.tsum = gout.tsum;
+    rec.f1_0 = gout.f1_0;
+    rec.f2_0 = gout.f2_0;
+    rec.dbg[0] = col > 0 ? wa[1] : 0;
+    rec.dbg[1] = col > 0 ? wa[col + 1] : 0;
+    rec.dbg[2] = col > 0 ? wa[2 * m + 1] : 0;
+    rec.dbg[3] = col > 0 ? wa[2 * m + col + 1] : 0;
+    rec.dbg[4] = 0;
+    rec.dbg[5] = 0;
+    rec.dbg[6] = col > 0 ? sy[0] : 0;
+    rec.dbg[7] = col > 0 ? wt[0] : 0;
     rec.iword = iword;
     rec.reset = reset_pending;
     reset_pending = 0;

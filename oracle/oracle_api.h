@@ -67,6 +67,8 @@ typedef struct {
   unsigned long long free_hash; /* sum over free i of mix64(i) (order-free hash) */
   unsigned long long at_lower, at_upper; /* counts of iwhere==1 / iwhere==2 after GCP */
   double f, theta, stp, dtm, tsum, gd, gdold, dtd, stpmx;
+  double f1_0, f2_0; /* Cauchy f' and f'' before the first breakpoint */
+  double dbg[8];     /* p(1), p(col+1), c(1), c(col+1), (Mc)(1), (Mc)(col+1), sy(1,1), wt(1,1) */
 } orc_trace_rec;
 
 typedef void (*orc_trace_cb)(void* user, const orc_trace_rec* rec);
