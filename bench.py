@@ -1,0 +1,405 @@
+"""Benchmark of the L-BFGS-B iteration at n = 4096^2 (the headline config).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--side S] [--dtype f64|f32]
+
+A step is one L-BFGS-B iteration (Cauchy point, subspace step, line search with its
+function evaluations, memory update) of the plain solve of the synthetic bounded problem
+of lbfgsb-gpu_b200/synth.py on an S x S grid (default 4096: n = 16,777,216), FP64.  The
+tolerances eps_f = eps_g = eps_x are 0 so every run performs exactly W + K iterations
+(the stopping tests still run every iteration).  The FP64 form is the headline: in FP32
+f ~ 0.45 cannot resolve this problem's per-iteration decrease (~1e-8 relative) at this
+size and the reference's f-test ends the solve after one iteration, in the reference as
+here.
+
+ours:      W untimed iterations, then exactly K iterations timed with CUDA events on the
+           solver's stream between two after-iteration callbacks (barrier + synchronize on
+           both sides), inputs resident in HBM (vectors far larger than the 126 MB L2).
+           e2e: the same K iterations through the C ABI from pinned host buffers, the
+           host-to-device copies of x0, l, u, nbd and the objective's fields and the
+           device-to-host copy of x inside the timed region.
+reference: the reference's own CPU L-BFGS-B (culbfgsb/lbfgsbcpu.cpp built into
+           oracle/_ref/) on the same problem on the host, single thread (the reference has
+           no threading), a bounded number of iterations.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+for _p in (REPO, os.path.join(REPO, "lbfgsb-gpu_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+UNIT = "iters/s"
+
+
+def peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-element DRAM bytes per launch, from a committed ncu capture summary."""
+    try:
+        with open(os.path.join(REPO, "profiles", "ncu_traffic.json")) as fh:
+            return json.load(fh)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"bench_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[0]) for r in rows]
+        mx = float(rows[0][1])
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for name, v in zip(names, r[4:8]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def make_problem(side: int, seed: int = 0):
+    import synth
+    return synth.synth_problem(side, seed=seed)
+
+
+def run_ours(args, rank: int, world: int, dist):
+    import torch
+    import lbfgsb_b200 as LB
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    lib = LB.load()
+    is64 = args.dtype == "f64"
+    dt = np.float64 if is64 else np.float32
+    tdt = torch.float64 if is64 else torch.float32
+    prob = make_problem(args.side, seed=rank)
+    n = prob["nbd"].size
+    W, K = args.warmup, args.steps
+
+    def option(iters):
+        o = LB.default_option(dt)
+        o.eps_f = o.eps_g = o.eps_x = 0.0
+        o.max_iteration = iters - 1  # the solve stops after iteration `iters`
+        return o
+
+    so = LB.SynthObjective(prob, single_precision_fields=not is64)
+    fg = so.f64 if is64 else so.f32
+    x = torch.zeros(n, dtype=tdt, device=dev)
+    l = torch.from_numpy(prob["l"].astype(dt)).to(dev)
+    u = torch.from_numpy(prob["u"].astype(dt)).to(dev)
+    nbd = torch.from_numpy(prob["nbd"]).to(dev)
+    cbt = LB.CB64 if is64 else LB.CB32
+    summ_t = LB.SummaryF64 if is64 else LB.SummaryF32
+    minimize = lib.lbfgsb_b200_minimize_ext_f64 if is64 else lib.lbfgsb_b200_minimize_ext_f32
+
+    def solve(iters, after=None, profile=False):
+        x.zero_()
+        summ = summ_t()
+        ext = LB.Ext(0, 1 if profile else 0, LB.TRACE_CB(), None)
+        st = minimize(n, x.data_ptr(), nbd.data_ptr(), l.data_ptr(), u.data_ptr(),
+                      C.byref(option(iters)), fg, after, None, so.handle, None, C.byref(ext),
+                      C.byref(summ))
+        torch.cuda.synchronize()
+        if st != 0:
+            raise RuntimeError(f"status {st}: {lib.lbfgsb_b200_last_error()}")
+        return summ, LB.last_stats()
+
+    # warm the whole path once (allocator pool, module load)
+    solve(2)
+
+    # ---- headline: K iterations after W, timed between after-iteration callbacks ----
+    ev = {"start": torch.cuda.Event(enable_timing=True), "end": torch.cuda.Event(enable_timing=True)}
+
+    def after_cb(_user, _x, _f, _g, _stream, sp):
+        it = sp[0].num_iteration
+        if it == W:
+            torch.cuda.synchronize()
+            if dist is not None:
+                dist.barrier()
+            ev["start"].record()
+        elif it == W + K:
+            ev["end"].record()
+            ev["end"].synchronize()
+        return 0
+
+    cb = cbt(after_cb)
+    sampler = ClockSampler(dev.index)
+    with sampler:
+        summ, st_plain = solve(W + K, after=C.cast(cb, C.c_void_p).value)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ms = ev["start"].elapsed_time(ev["end"])
+    if summ.num_iteration != W + K:
+        raise RuntimeError(f"solve stopped early: {summ.num_iteration} iterations, info {summ.info}")
+
+    # ---- per-kernel device times of the K steady-state iterations (profiled runs) ----
+    _, st_w = solve(W, profile=True)
+    _, st_wk = solve(W + K, profile=True)
+    kern = {}
+    for name, v in st_wk["kernels"].items():
+        launches = v["launches"] - st_w["kernels"][name]["launches"]
+        kms = v["ms"] - st_w["kernels"][name]["ms"]
+        if launches > 0:
+            kern[name] = {"launches": launches, "ms": kms, "bytes": v["bytes"]}
+    evals_k = st_wk["evaluations"] - st_w["evaluations"]
+    launches_k = st_wk["total_launches"] - st_w["total_launches"] + evals_k  # + objective
+
+    # ---- e2e through the C ABI from pinned host buffers ----
+    hx = torch.zeros(n, dtype=tdt).pin_memory()
+    hl = torch.from_numpy(prob["l"].astype(dt)).pin_memory()
+    hu = torch.from_numpy(prob["u"].astype(dt)).pin_memory()
+    hn = torch.from_numpy(prob["nbd"]).pin_memory()
+    hout = torch.empty(n, dtype=tdt).pin_memory()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    dx = hx.to(dev, non_blocking=True)
+    dl = hl.to(dev, non_blocking=True)
+    du = hu.to(dev, non_blocking=True)
+    dn = hn.to(dev, non_blocking=True)
+    so2 = LB.SynthObjective(prob, single_precision_fields=not is64)  # uploads the fields
+    summ2 = summ_t()
+    st = (lib.lbfgsb_b200_minimize_f64 if is64 else lib.lbfgsb_b200_minimize_f32)(
+        n, dx.data_ptr(), dn.data_ptr(), dl.data_ptr(), du.data_ptr(), C.byref(option(K)),
+        so2.f64 if is64 else so2.f32, None, None, so2.handle, None, C.byref(summ2))
+    hout.copy_(dx, non_blocking=True)
+    e1.record()
+    e1.synchronize()
+    if st != 0:
+        raise RuntimeError(f"status {st}")
+    e2e_ms = e0.elapsed_time(e1)
+    so2.close()
+    field_bytes = 4 * n * (4 if not is64 else 8)
+    h2d = hx.nbytes + hl.nbytes + hu.nbytes + hn.nbytes + field_bytes
+    d2h = hout.nbytes + 8 * summ2.num_iteration  # x and the per-evaluation f
+    so.close()
+
+    # ---- gather over ranks (max time) ----
+    t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms, e2e_ms = float(t[0]), float(t[1])
+    return {"ms": ms, "kern": kern, "launches_k": launches_k, "evals_k": evals_k,
+            "clocks": sampler.summary(), "e2e_ms": e2e_ms, "e2e_iters": summ2.num_iteration,
+            "h2d": h2d, "d2h": d2h, "n": n,
+            "model_bytes_iter": st_wk["bytes_per_iteration_model"]}
+
+
+def cpu_reference(side: int, dtype: str, warm: int, timed: int, budget_s: float = 60.0):
+    """The reference's CPU path (oracle/_ref, built from culbfgsb/lbfgsbcpu.cpp) on the same
+    problem; iterations timed between after-iteration callbacks, single thread."""
+    from oracle import binding as OB
+    if not OB.ref_available():
+        return None
+    dt = np.float64 if dtype == "f64" else np.float32
+    prob = make_problem(side)
+    prob["kind"] = "synth"
+    opt = OB.default_option(dt)
+    opt.eps_f = opt.eps_g = opt.eps_x = 0.0
+    lib = OB.ref_lib()
+    ev = OB.host_objective(prob, dt)
+    n = prob["nbd"].size
+    x = np.zeros(n, dtype=dt)
+    l = prob["l"].astype(dt)
+    u = prob["u"].astype(dt)
+    nbd = prob["nbd"].astype(np.int32)
+    marks = {}
+    real = C.c_double if dt == np.float64 else C.c_float
+    cbt = OB.CB64 if dt == np.float64 else OB.CB32
+    summ = OB.SummaryF64() if dt == np.float64 else OB.SummaryF32()
+    t_start = [time.perf_counter()]
+
+    def fg(_u, xp, fp, gp, _s):
+        ev(xp, fp, gp)
+        return 0
+
+    def after(_u, xp, fp, gp, sp):
+        marks[sp[0].num_iteration] = time.perf_counter()
+        return 0
+
+    def stop(_u, xp, fp, gp, sp):
+        it = sp[0].num_iteration
+        done = it >= warm + timed or (it > warm and time.perf_counter() - marks[warm] > budget_s)
+        return 1 if done else 0
+
+    cbs = [cbt(fg), cbt(after), cbt(stop)]
+    P = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
+    opt.max_iteration = warm + timed + 1
+    fn = getattr(lib, "ref_lbfgsb_minimize_" + dtype)
+    fn(n, P(x, real), P(nbd, C.c_int), P(l, real), P(u, real), C.byref(opt), cbs[0], cbs[1],
+       cbs[2], None, C.byref(summ))
+    last = max(marks)
+    iters = last - warm
+    secs = marks[last] - marks[warm]
+    return {"value": iters / secs, "iters": iters, "secs": secs, "n": n}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--side", type=int, default=4096)
+    ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    global METRIC
+    METRIC = f"L-BFGS-B iterations/s at n={args.side}^2"
+    config = {"workload": f"plain L-BFGS-B solve, synthetic bounded grid problem {args.side}x{args.side} "
+                          f"(n={args.side * args.side}), m=8, 80% boxed / 10% lower / 10% free",
+              "side": args.side, "n": args.side * args.side, "m": 8, "instances_per_gpu": 1,
+              "l2": "inputs larger than L2 (every n-vector > 126 MB)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        warm = 1
+        timed = max(1, min(args.steps, 3))
+        r = cpu_reference(args.side, args.dtype, warm, timed)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "reference CPU build oracle/_ref/libref_lbfgsb.so is missing"}))
+            return
+        line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "impl": "reference",
+                "n_gpus": args.gpus, "steps": r["iters"], "warmup": warm,
+                "ms_per_step": 1000.0 / r["value"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
+                "config": config,
+                "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": 1, "kind": "reference",
+                                 "sample": f"{r['iters']} iterations after {warm} of the full "
+                                           f"n={r['n']} problem, reference lbfgsbcpu.cpp, 1 thread"},
+                "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as td
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = td
+    try:
+        r = run_ours(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+    if rank != 0:
+        return
+    K = args.steps
+    value = world * K / (r["ms"] / 1000.0)
+    hbm, hbm_kind = peaks()
+    kern = r["kern"]
+    top = max(kern.items(), key=lambda kv: kv[1]["ms"]) if kern else None
+    roof = None
+    if top:
+        name, v = top
+        avg_s = v["ms"] / v["launches"] / 1000.0
+        achieved = v["bytes"] / avg_s / 1e9
+        tr = ncu_traffic()
+        traffic = None
+        if tr and name in tr.get("bytes_per_element", {}):
+            traffic = tr["bytes_per_element"][name] * r["n"]
+        roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm,
+                "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                "peak_source": f"{hbm_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "algorithmic_bytes_per_launch": v["bytes"], "avg_launch_ms": avg_s * 1000.0}
+    per_kernel = {k: {"launches": v["launches"], "avg_ms": v["ms"] / v["launches"],
+                      "share": v["ms"] / sum(x["ms"] for x in kern.values()),
+                      "GBps": (v["bytes"] / (v["ms"] / v["launches"] / 1000.0) / 1e9) if v["bytes"] else None}
+                  for k, v in kern.items()}
+    solver_ms = sum(v["ms"] for v in kern.values())
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        c = cpu_reference(args.side, args.dtype, 1, 2)
+        if c:
+            cpu = {"value": c["value"], "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"{c['iters']} iterations (after 1) of the same n={c['n']} problem, "
+                             "reference lbfgsbcpu.cpp built from source, 1 thread"}
+    e2e_iters = max(1, r["e2e_iters"])
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": r["ms"] / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
+        "config": config,
+        "e2e": {"value": world * e2e_iters / (r["e2e_ms"] / 1000.0), "unit": UNIT,
+                "h2d_bytes_per_step": r["h2d"] / e2e_iters,
+                "d2h_bytes_per_step": r["d2h"] / e2e_iters},
+        "gpu_launches": r["launches_k"],
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": r["clocks"],
+        "solver_kernels_ms_per_step": solver_ms / K,
+        "evaluations_per_step": r["evals_k"] / K,
+        "hbm_GBps_model": r["model_bytes_iter"] / (solver_ms / K / 1000.0) / 1e9 if solver_ms else None,
+        "kernels": per_kernel,
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -99,6 +99,17 @@ def make_case(name: str):
         a = 1.0 + 0.1 * (k % 5)
         c = np.where(k % 4 == 0, x0, 0.8 * np.sin(3.0 * k))
         return _quad(n, a, c, np.full(n, -0.3), np.full(n, 0.3), np.full(n, 2, np.int32)), f64, x0, tight, None
+    if name in ("quad_walk_many_f64", "quad_walk_many_f32"):
+        # ~3000 breakpoints are passed by the first Cauchy step (more than one 1024-chunk of
+        # the device walk), then the walk stops inside the remaining segment
+        n = 4096
+        k = np.arange(n)
+        far = k % 4 != 3
+        sign = np.where(k % 2 == 0, 1.0, -1.0)
+        c = np.where(far, 3.0 * sign * (1.0 + k / n), 0.5 * sign)
+        a = 1.0 + 0.25 * ((k * 7) % 5)
+        return (_quad(n, a, c, np.full(n, -1.0), np.full(n, 1.0), np.full(n, 2, np.int32)),
+                (f64 if name.endswith("64") else f32), None, tight, None)
     if name == "err_nbd4":
         p = _synth(4)
         p["nbd"][3] = 4
@@ -121,7 +132,8 @@ CASES = [
     "synth_s20_f64_boxed", "synth_s20_f64_nbd13", "synth_s20_f64_fixedeq",
     "synth_s20_f64_x0out", "synth_s32_f64_maxit7", "synth_s16_f64_custom3",
     "synth_s64_f64_b001", "synth_s64_f32_b002", "quad_ties_f64", "quad_ties_f32",
-    "quad_zero_grad_f64", "err_nbd4", "err_l_gt_u", "err_n_lt_m",
+    "quad_zero_grad_f64", "quad_walk_many_f64", "quad_walk_many_f32", "err_nbd4",
+    "err_l_gt_u", "err_n_lt_m",
 ]
 
 
