@@ -164,6 +164,30 @@ static int device_sms() {
   return sms;
 }
 
+// Launch shape of a staged-tile pass: as many ring stages as fit a shared-memory budget
+// (2..8), the dynamic shared memory that needs, and a grid of resident CTAs.
+struct PassCfg {
+  int grid = 1, stages = 2, smem = 0, threads = 0;
+};
+constexpr int kConsWide = 512;    // consumer threads of the staged passes
+constexpr int kConsNarrow = 256;  // ... of the pass with the most accumulators
+constexpr int kRingBudget = 176 * 1024;
+
+template <typename K>
+static PassCfg pass_cfg(K kernel, int cap, long long n, int threads) {
+  PassCfg p;
+  p.threads = threads;
+  p.stages = std::max(2, std::min(8, kRingBudget / cap));
+  p.smem = ring_bytes(p.stages, cap);
+  CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, p.smem));
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, p.smem));
+  per_sm = std::max(per_sm, 1);
+  const long long tiles = (n + kTile - 1) / kTile;
+  p.grid = (int)std::max<long long>(1, std::min<long long>(tiles, (long long)device_sms() * per_sm));
+  return p;
+}
+
 template <typename K>
 static int grid_for(K kernel, int n, int threads) {
   int per_sm = 0;
@@ -212,8 +236,9 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
     for (int k = 0; k < 3; k++) w.X[k] = w.template alloc<R>(N);
     for (int k = 0; k < 2; k++) w.G[k] = w.template alloc<R>(N);
     w.dsub = w.template alloc<R>(N);
-    w.ws = w.template alloc<H>(N * kSlots);
-    w.wy = w.template alloc<H>(N * kSlots);
+    const size_t ld = ((N + kTile - 1) / kTile) * kTile;  // 16-byte aligned slots
+    w.ws = w.template alloc<H>(ld * kSlots);
+    w.wy = w.template alloc<H>(ld * kSlots);
     w.code = w.template alloc<int8_t>(N);
     const size_t words = (N + 31) / 32 + 1;
     w.fbits = w.template alloc<uint32_t>(words);
@@ -221,13 +246,40 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
     w.ticket = w.template alloc<unsigned int>(1);
     CK(cudaMallocHost(&w.hs, sizeof(DevState<S>)));
 
+    // the staged passes copy l, u and nbd in 16-byte aligned tiles
+    const R* la = l;
+    const R* ua = u;
+    const int* nbda = nbd;
+    auto misaligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) != 0; };
+    if (misaligned(l) || misaligned(u) || misaligned(nbd)) {
+      R* lc = w.template alloc<R>(N);
+      R* uc = w.template alloc<R>(N);
+      int* nc = w.template alloc<int>(N);
+      CK(cudaMemcpyAsync(lc, l, N * sizeof(R), cudaMemcpyDeviceToDevice, stream));
+      CK(cudaMemcpyAsync(uc, u, N * sizeof(R), cudaMemcpyDeviceToDevice, stream));
+      CK(cudaMemcpyAsync(nc, nbd, N * sizeof(int), cudaMemcpyDeviceToDevice, stream));
+      la = lc;
+      ua = uc;
+      nbda = nc;
+    }
+
+    // every stream the staged passes copy with cp.async.bulk starts on a 16-byte boundary
+    for (const void* p : {(const void*)la, (const void*)ua, (const void*)nbda, (const void*)w.X[0],
+                          (const void*)w.X[1], (const void*)w.X[2], (const void*)w.G[0],
+                          (const void*)w.G[1], (const void*)w.dsub, (const void*)w.code,
+                          (const void*)w.fbits, (const void*)w.ws, (const void*)w.wy}) {
+      if (misaligned(p)) throw CudaFailure{cudaErrorMisalignedAddress, "workspace alignment", __LINE__};
+    }
+
     Ctx<R, H, S> c;
     c.n = n;
-    c.l = l;
-    c.u = u;
-    c.nbd = nbd;
+    c.l = la;
+    c.u = ua;
+    c.nbd = nbda;
     c.ws = w.ws;
     c.wy = w.wy;
+    c.ld = (long long)ld;
+    c.stages = 2;
     c.code = w.code;
     c.fbits = w.fbits;
     c.dsub = w.dsub;
@@ -237,13 +289,20 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
     c.wl_i = nullptr;
     c.wl_n = nullptr;
 
-    const int g_gcp = grid_for(k_gcp_scan<R, H, S>, n, kThreads);
-    const int g_freev = grid_for(k_freev_formk<R, H, S>, n, kThreads);
-    const int g_dir = grid_for(k_subsm_dir<R, H, S>, n, kThreads);
-    const int g_apply = grid_for(k_subsm_apply<R, H, S>, n, kThreads);
-    const int g_post = grid_for(k_post_eval<R, H, S>, n, kThreads);
+    const int hsz = (int)sizeof(H);
+    const PassCfg p_gcp = pass_cfg(k_gcp_scan<R, H, S, kConsWide>,
+                                   stage_capacity(StageBytes<R>::gcp, 0, m, hsz), n, kConsWide + 32);
+    const PassCfg p_freev =
+        pass_cfg(k_freev_formk<R, H, S, kConsNarrow>,
+                 stage_capacity(StageBytes<R>::freev, kTile / 8, m, hsz), n, kConsNarrow + 32);
+    const PassCfg p_dir = pass_cfg(k_subsm_dir<R, H, S, kConsWide>,
+                                   stage_capacity(StageBytes<R>::dir, 0, m, hsz), n, kConsWide + 32);
+    const PassCfg p_apply = pass_cfg(k_subsm_apply<R, H, S, kConsWide>,
+                                     stage_capacity(StageBytes<R>::apply, 0, 0, hsz), n, kConsWide + 32);
+    const PassCfg p_post = pass_cfg(k_post_eval<R, H, S, kConsWide>,
+                                    stage_capacity(StageBytes<R>::post, 0, m, hsz), n, kConsWide + 32);
     const int g_proj = grid_for(k_projgr<R, H, S>, n, kThreads);
-    const int g_max = std::max({g_gcp, g_freev, g_dir, g_apply, g_post, g_proj});
+    const int g_max = std::max({p_gcp.grid, p_freev.grid, p_dir.grid, p_apply.grid, p_post.grid, g_proj});
     w.part = w.template alloc<double>((size_t)g_max * 256);
     c.part = w.part;
     const int g_elem = (int)std::min<long long>(((long long)n + 255) / 256, (long long)device_sms() * 8);
@@ -271,6 +330,7 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
       CK(cudaMemcpyAsync(w.hs, w.st, header, cudaMemcpyDeviceToHost, stream));
       CK(cudaStreamSynchronize(stream));
       syncs++;
+      if (w.hs->device_error) throw CudaFailure{cudaErrorLaunchTimeout, "staged-tile wait", __LINE__};
     };
 
     R* xcur = w.X[0];
@@ -317,17 +377,23 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
         const bool uncon = !cnstnd && col_now > 0;
         auto subspace = [&]() {
           L.run(KID_FREEV, [&] {
-            k_freev_formk<R, H, S><<<g_freev, kThreads, 0, stream>>>(c, xcur, gcur);
+            c.stages = p_freev.stages;
+            k_freev_formk<R, H, S, kConsNarrow><<<p_freev.grid, p_freev.threads, p_freev.smem, stream>>>(c, xcur, gcur);
           });
           L.run(KID_SUBDIR, [&] {
-            k_subsm_dir<R, H, S><<<g_dir, kThreads, 0, stream>>>(c, xcur, gcur);
+            c.stages = p_dir.stages;
+            k_subsm_dir<R, H, S, kConsWide><<<p_dir.grid, p_dir.threads, p_dir.smem, stream>>>(c, xcur, gcur);
           });
           L.run(KID_SUBAPPLY, [&] {
-            k_subsm_apply<R, H, S><<<g_apply, kThreads, 0, stream>>>(c, xcur, gcur, zb);
+            c.stages = p_apply.stages;
+            k_subsm_apply<R, H, S, kConsWide><<<p_apply.grid, p_apply.threads, p_apply.smem, stream>>>(c, xcur, gcur, zb);
           });
         };
         if (!uncon) {
-          L.run(KID_GCP, [&] { k_gcp_scan<R, H, S><<<g_gcp, kThreads, 0, stream>>>(c, xcur, gcur); });
+          L.run(KID_GCP, [&] {
+            c.stages = p_gcp.stages;
+            k_gcp_scan<R, H, S, kConsWide><<<p_gcp.grid, p_gcp.threads, p_gcp.smem, stream>>>(c, xcur, gcur);
+          });
         }
         subspace();
         pull();
@@ -381,8 +447,9 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
           funcgrad(user, xt, &f, gnew, (void*)stream, summary);
           evals++;
           L.run(KID_POST, [&] {
-            k_post_eval<R, H, S><<<g_post, kThreads, 0, stream>>>(c, xcur, zb, xt, gnew, gcur,
-                                                                  (S)f, 0);
+            c.stages = p_post.stages;
+            k_post_eval<R, H, S, kConsWide><<<p_post.grid, p_post.threads, p_post.smem, stream>>>(c, xcur, zb, xt, gnew,
+                                                                              gcur, (S)f, 0);
           });
           pull();
           if (hs.ls_task != 1) break;
@@ -403,8 +470,9 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
             xt = tb;
           }
           L.run(KID_POST, [&] {
-            k_post_eval<R, H, S><<<g_post, kThreads, 0, stream>>>(c, xcur, zb, xt, gnew, gcur,
-                                                                  (S)f, 1);
+            c.stages = p_post.stages;
+            k_post_eval<R, H, S, kConsWide><<<p_post.grid, p_post.threads, p_post.smem, stream>>>(c, xcur, zb, xt, gnew,
+                                                                              gcur, (S)f, 1);
           });
           pull();
         }

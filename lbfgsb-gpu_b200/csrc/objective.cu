@@ -89,10 +89,10 @@ __global__ void __launch_bounds__(kThreads) k_synth(int s, const R* __restrict__
   }
   double sarr[1] = {acc}, xd[1] = {0.0}, ld[1] = {0.0};
   MinPair md[1] = {MinPair{0.0, 0}};
-  cta_reduce_to_row<1, 0, 0, 0>(sarr, xd, md, ld, part, 1);
+  cta_reduce_to_row<kThreads, 1, 0, 0, 0>(sarr, xd, md, ld, part, 1);
   if (!last_cta(ticket)) return;
   __shared__ double red[1];
-  fold_rows(part, gridDim.x, 1, 1, 0, 0, red);
+  fold_rows<kThreads>(part, gridDim.x, 1, 1, 0, 0, red);
   if (threadIdx.x == 0) *fout = red[0];
 }
 

@@ -29,6 +29,7 @@
 #include "reduce.cuh"
 #include "small.cuh"
 #include "state.cuh"
+#include "tiles.cuh"
 
 namespace lbfgsb_b200 {
 
@@ -38,8 +39,10 @@ struct Ctx {
   const R* __restrict__ l;
   const R* __restrict__ u;
   const int* __restrict__ nbd;
-  H* ws;             // kSlots slot-major arrays of n
+  H* ws;             // kSlots slot-major arrays, slot stride ld elements
   H* wy;
+  long long ld;      // history slot stride (n rounded up to a multiple of kTile)
+  int stages;        // depth of the staged-tile ring of the passes
   int8_t* code;      // iwhere codes
   uint32_t* fbits;   // free set of the last freev, one bit per variable
   R* dsub;           // subspace direction on the free set
@@ -53,13 +56,71 @@ struct Ctx {
 
 // Physical slot pointers of ring positions 1..kMaxM counted from head.
 template <typename H, typename S>
-__device__ __forceinline__ void ring_ptrs(const DevState<S>* st, const H* base, int n,
+__device__ __forceinline__ void ring_ptrs(const DevState<S>* st, const H* base, long long ld,
                                           const H* (&out)[kMaxM]) {
   const int m = st->m, head = st->head;
 #pragma unroll
   for (int j = 0; j < kMaxM; j++) {
     int r = (head - 1 + j) % m + 1;
-    out[j] = base + (size_t)st->phys[r] * (size_t)n;
+    out[j] = base + (size_t)st->phys[r] * (size_t)ld;
+  }
+}
+
+// Bytes per element of the scalar streams each pass stages (the history columns add
+// 2*col*sizeof(H) per element, the free-set bits 32 bytes per tile).
+template <typename R>
+struct StageBytes {
+  static constexpr int gcp = 4 * (int)sizeof(R) + 4;        // x g l u nbd
+  static constexpr int freev = 1 + 2 * (int)sizeof(R);      // code x g
+  static constexpr int dir = 1 + 4 * (int)sizeof(R) + 4;    // code x g l u nbd
+  static constexpr int apply = 1 + 5 * (int)sizeof(R) + 4;  // code x g l u dsub nbd
+  static constexpr int post = 7 * (int)sizeof(R) + 4;       // t z g go l u nbd (+ xt)
+};
+// Shared-memory ring capacity of one stage for a pass with `scalar` bytes per element.
+__host__ __device__ inline int stage_capacity(int scalar, int extra_tile, int m, int hsize) {
+  return kTile * scalar + extra_tile + 2 * m * kTile * hsize;
+}
+__host__ __device__ inline int ring_bytes(int stages, int cap) { return stages * cap + 16 * stages; }
+
+__device__ __forceinline__ int add_stream(StreamSet& ss, const void* base, int tile_bytes) {
+  const int j = ss.count++;
+  ss.src[j] = static_cast<const unsigned char*>(base);
+  ss.tile_bytes[j] = tile_bytes;
+  ss.off[j] = ss.stage_bytes;
+  ss.stage_bytes += tile_bytes;
+  return j;
+}
+
+// Appends the col y-columns, then the col s-columns, of the ring (positions 1..col from
+// head); returns the stage offsets of the first y and s column.
+template <typename R, typename H, typename S>
+__device__ __forceinline__ void add_history(StreamSet& ss, const Ctx<R, H, S>& c,
+                                            const DevState<S>* st, int& hy, int& hs) {
+  const int col = st->col, m = st->m, head = st->head;
+  const int hb = kTile * (int)sizeof(H);
+  hy = ss.stage_bytes;
+  for (int j = 0; j < col; j++) {
+    const int r = (head - 1 + j) % m + 1;
+    add_stream(ss, c.wy + (size_t)st->phys[r] * (size_t)c.ld, hb);
+  }
+  hs = ss.stage_bytes;
+  for (int j = 0; j < col; j++) {
+    const int r = (head - 1 + j) % m + 1;
+    add_stream(ss, c.ws + (size_t)st->phys[r] * (size_t)c.ld, hb);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T stage_at(const unsigned char* buf, int off, int e) {
+  return reinterpret_cast<const T*>(buf + off)[e];
+}
+template <typename H>
+__device__ __forceinline__ double hist_at(const unsigned char* buf, int off, int e) {
+  const H v = reinterpret_cast<const H*>(buf + off)[e];
+  if constexpr (sizeof(H) == 2) {
+    return (double)__bfloat162float(v);
+  } else {
+    return (double)v;
   }
 }
 
@@ -129,14 +190,11 @@ __device__ __forceinline__ S reduced_grad(bool uncon, R x, R z, R g, int col,
 
 // ------------------------------------------------------------------------------------
 // A: the Cauchy-point scan.
-template <typename R, typename H, typename S>
-__global__ void __launch_bounds__(kThreads) k_gcp_scan(Ctx<R, H, S> c, const R* __restrict__ x,
+template <typename R, typename H, typename S, int CONS>
+__global__ void __launch_bounds__(CONS + 32) k_gcp_scan(Ctx<R, H, S> c, const R* __restrict__ x,
                                                        const R* __restrict__ g) {
   DevState<S>* st = c.st;
   const int n = c.n, col = st->col;
-  const H *Y[kMaxM], *Sl[kMaxM];
-  ring_ptrs(st, c.wy, n, Y);
-  ring_ptrs(st, c.ws, n, Sl);
   // sums: [0] sum neggi^2, [1..16] p (y part 1..8, s part 9..16), [17] nbreak,
   // [18] movable variables without breakpoint; max: [0] any such with g != 0;
   // min pair: smallest breakpoint
@@ -147,13 +205,34 @@ __global__ void __launch_bounds__(kThreads) k_gcp_scan(Ctx<R, H, S> c, const R* 
   for (int k = 0; k < NS; k++) s[k] = 0.0;
   xm[0] = 0.0;
   mn[0] = MinPair{INFINITY, kNoIndex};
-  for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < n;
-       i += (long long)gridDim.x * kThreads) {
-    const R xi = x[i], gi = g[i], li = c.l[i], ui = c.u[i];
-    const int nb = c.nbd[i];
+
+  extern __shared__ __align__(128) unsigned char dyn[];
+  __shared__ StreamSet ss;
+  __shared__ int s_hy, s_hs;
+  if (threadIdx.x == 0) {
+    ss.count = 0;
+    ss.stage_bytes = 0;
+    add_stream(ss, x, kTile * (int)sizeof(R));
+    add_stream(ss, g, kTile * (int)sizeof(R));
+    add_stream(ss, c.l, kTile * (int)sizeof(R));
+    add_stream(ss, c.u, kTile * (int)sizeof(R));
+    add_stream(ss, c.nbd, kTile * 4);
+    add_history(ss, c, st, s_hy, s_hs);
+  }
+  __syncthreads();
+  const int o_x = ss.off[0], o_g = ss.off[1], o_l = ss.off[2], o_u = ss.off[3], o_nb = ss.off[4];
+  const int hy = s_hy, hs = s_hs, hb = kTile * (int)sizeof(H);
+  const int cap = stage_capacity(StageBytes<R>::gcp, 0, st->m, (int)sizeof(H));
+  run_tiles<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
+            &st->device_error, [&](const unsigned char* buf, long long t, int valid, int e) {
+    if (e >= valid) return;
+    const long long i = t * kTile + e;
+    const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
+    const R li = stage_at<R>(buf, o_l, e), ui = stage_at<R>(buf, o_u, e);
+    const int nb = stage_at<int>(buf, o_nb, e);
     bool has_bp;
-    R t;
-    const int code = classify(xi, gi, li, ui, nb, has_bp, t);
+    R tb;
+    const int code = classify(xi, gi, li, ui, nb, has_bp, tb);
     c.code[i] = (int8_t)code;
     if (code == IW_FREE || code == IW_UNB) {
       const double neggi = -(double)gi;
@@ -161,25 +240,25 @@ __global__ void __launch_bounds__(kThreads) k_gcp_scan(Ctx<R, H, S> c, const R* 
 #pragma unroll
       for (int j = 0; j < kMaxM; j++) {
         if (j < col) {
-          s[1 + j] = fma((double)HistTraits<H>::load(Y[j] + i), neggi, s[1 + j]);
-          s[9 + j] = fma((double)HistTraits<H>::load(Sl[j] + i), neggi, s[9 + j]);
+          s[1 + j] = fma(hist_at<H>(buf, hy + j * hb, e), neggi, s[1 + j]);
+          s[9 + j] = fma(hist_at<H>(buf, hs + j * hb, e), neggi, s[9 + j]);
         }
       }
       if (has_bp) {
         s[17] += 1.0;
-        mn[0] = minpair(mn[0], MinPair{(double)t, i});
+        mn[0] = minpair(mn[0], MinPair{(double)tb, i});
       } else {
         s[18] += 1.0;
         if (neggi != 0.0) xm[0] = 1.0;
       }
     }
-  }
+  });
   constexpr int W = NS + NX + 2 * NM;
   double lo[1] = {0.0};
-  cta_reduce_to_row<NS, NX, NM, 0>(s, xm, mn, lo, c.part, W);
+  cta_reduce_to_row<CONS + 32, NS, NX, NM, 0>(s, xm, mn, lo, c.part, W);
   if (!last_cta(c.ticket)) return;
   __shared__ double red[W];
-  fold_rows(c.part, gridDim.x, W, NS, NX, NM, red);
+  fold_rows<CONS + 32>(c.part, gridDim.x, W, NS, NX, NM, red);
   __shared__ SmallWork<S> sw;
   if (threadIdx.x != 0) return;
 
@@ -277,8 +356,8 @@ __host__ __device__ inline void corr_map(int q, int& kind, int& a, int& b) {
   }
 }
 
-template <typename R, typename H, typename S>
-__global__ void __launch_bounds__(kThreads) k_freev_formk(Ctx<R, H, S> c, const R* __restrict__ x,
+template <typename R, typename H, typename S, int CONS>
+__global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const R* __restrict__ x,
                                                           const R* __restrict__ g) {
   DevState<S>* st = c.st;
   if (st->gcp_state == GCP_WALK || st->internal_fail != 0) return;
@@ -287,18 +366,15 @@ __global__ void __launch_bounds__(kThreads) k_freev_formk(Ctx<R, H, S> c, const 
   const bool track = !uncon && iter > 0 && st->cnstnd;
   const bool updatd = st->updatd != 0;
   const S theta = st->theta, tsum = st->tsum;
-  const H *Y[kMaxM], *Sl[kMaxM];
-  ring_ptrs(st, c.wy, n, Y);
-  ring_ptrs(st, c.ws, n, Sl);
-  S a1[kMaxM + 1], a2[kMaxM];
-#pragma unroll
-  for (int j = 0; j < kMaxM; j++) {
+  __shared__ S a1[kMaxM + 1], a2[kMaxM];  // cmprlb's coefficients (uniform over the grid)
+  if (threadIdx.x < kMaxM) {
+    const int j = threadIdx.x;
     a1[j] = (j < col) ? st->mc[1 + j] : S(0);
     a2[j] = (j < col) ? theta * st->mc[col + 1 + j] : S(0);
+    if (j == 0) a1[kMaxM] = theta;
   }
-  a1[kMaxM] = theta;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int kWarps = kThreads / 32;
+  constexpr int kWarps = CONS / 32;
   // sums: [0..7] sum_F y_j r, [8..15] sum_F s_j r, [16..23] yy_new, [24..31] ss_new,
   // [32..39] sy_row, [40..47] sy_col, [48] nfree, [49] nenter, [50] nleave,
   // [51] at lower, [52] at upper
@@ -316,30 +392,48 @@ __global__ void __launch_bounds__(kThreads) k_freev_formk(Ctx<R, H, S> c, const 
 #pragma unroll
   for (int k = 0; k < kLaneOwned; k++) corr_map(lane + 32 * k, ck[k], ca[k], cb[k]);
 
-  for (long long base = ((long long)blockIdx.x * kWarps + warp) * 32; base < n;
-       base += (long long)gridDim.x * kWarps * 32) {
-    const long long i = base + lane;
-    const bool valid = i < n;
+  extern __shared__ __align__(128) unsigned char dyn[];
+  __shared__ StreamSet ss;
+  __shared__ int s_hy, s_hs;
+  if (threadIdx.x == 0) {
+    ss.count = 0;
+    ss.stage_bytes = 0;
+    add_stream(ss, c.code, kTile);
+    add_stream(ss, c.fbits, kTile / 8);
+    add_stream(ss, x, kTile * (int)sizeof(R));
+    add_stream(ss, g, kTile * (int)sizeof(R));
+    add_history(ss, c, st, s_hy, s_hs);
+  }
+  __syncthreads();
+  const int o_code = ss.off[0], o_bits = ss.off[1], o_x = ss.off[2], o_g = ss.off[3];
+  const int hy = s_hy, hs = s_hs, hb = kTile * (int)sizeof(H);
+  const int cap = stage_capacity(StageBytes<R>::freev, kTile / 8, st->m, (int)sizeof(H));
+  run_tiles<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
+            &st->device_error, [&](const unsigned char* buf, long long t, int valid, int e) {
+    // the whole warp runs every call (ballots); word e/32 of the tile's free-set bits
+    const long long i = t * kTile + e;
+    const bool ok = e < valid;
     int code = IW_LOW;
-    if (valid) code = c.code[i];
-    const bool fnow = valid && (uncon || iw_free(code));
-    const uint32_t word = c.fbits[base >> 5];
+    if (ok) code = stage_at<int8_t>(buf, o_code, e);
+    const bool fnow = ok && (uncon || iw_free(code));
+    const int wi = e >> 5;
+    const uint32_t word = stage_at<uint32_t>(buf, o_bits, wi);
     const bool fprev = (word >> lane) & 1u;
-    const bool enter = track && valid && !fprev && fnow;
-    const bool leave = track && valid && fprev && !fnow;
+    const bool enter = track && ok && !fprev && fnow;
+    const bool leave = track && ok && fprev && !fnow;
     const uint32_t newword = __ballot_sync(0xffffffffu, fnow);
-    if (!uncon && lane == 0) c.fbits[base >> 5] = newword;
+    if (!uncon && lane == 0 && wi * 32 < valid) c.fbits[t * (kTile / 32) + wi] = newword;
     S yv[kMaxM], sv[kMaxM];
 #pragma unroll
     for (int j = 0; j < kMaxM; j++) {
-      yv[j] = (valid && j < col) ? (S)HistTraits<H>::load(Y[j] + i) : S(0);
-      sv[j] = (valid && j < col) ? (S)HistTraits<H>::load(Sl[j] + i) : S(0);
+      yv[j] = (ok && j < col) ? (S)hist_at<H>(buf, hy + j * hb, e) : S(0);
+      sv[j] = (ok && j < col) ? (S)hist_at<H>(buf, hs + j * hb, e) : S(0);
     }
-    if (valid) {
+    if (ok) {
       if (fnow) {
         s[48] += 1.0;
         hash += mix64((unsigned long long)i);
-        const R xi = x[i], gi = g[i];
+        const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
         const R zi = uncon ? xi : gcp_point<R, S>(code, xi, gi, R(0), R(0), tsum);
         const S r = reduced_grad<R, S>(uncon, xi, zi, gi, col, yv, sv, a1, a2);
 #pragma unroll
@@ -419,7 +513,7 @@ __global__ void __launch_bounds__(kThreads) k_freev_formk(Ctx<R, H, S> c, const 
       }
       __syncwarp();
     }
-  }
+  });
   // the free-set hash sums mod 2^64 (order free), one atomic per warp
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) hash += __shfl_xor_sync(0xffffffffu, hash, o);
@@ -428,10 +522,10 @@ __global__ void __launch_bounds__(kThreads) k_freev_formk(Ctx<R, H, S> c, const 
   constexpr int W = NS + 32 * kLaneOwned;
   double xm[1] = {0.0};
   MinPair mn[1] = {MinPair{0.0, 0}};
-  cta_reduce_to_row<NS, 0, 0, kLaneOwned>(s, xm, mn, corr, c.part, W);
+  cta_reduce_to_row<CONS + 32, NS, 0, 0, kLaneOwned>(s, xm, mn, corr, c.part, W);
   if (!last_cta(c.ticket)) return;
   __shared__ double red[W];
-  fold_rows(c.part, gridDim.x, W, W, 0, 0, red);
+  fold_rows<CONS + 32>(c.part, gridDim.x, W, W, 0, 0, red);
   __shared__ SmallWork<S> sw;
   if (threadIdx.x != 0) return;
 
@@ -500,39 +594,58 @@ __global__ void __launch_bounds__(kThreads) k_freev_formk(Ctx<R, H, S> c, const 
 
 // ------------------------------------------------------------------------------------
 // C: subspace direction on the free set and the step to the first bound it meets.
-template <typename R, typename H, typename S>
-__global__ void __launch_bounds__(kThreads) k_subsm_dir(Ctx<R, H, S> c, const R* __restrict__ x,
+template <typename R, typename H, typename S, int CONS>
+__global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c, const R* __restrict__ x,
                                                         const R* __restrict__ g) {
   DevState<S>* st = c.st;
   if (st->gcp_state == GCP_WALK || st->internal_fail != 0 || !st->subsm_active) return;
   const int n = c.n, col = st->col;
   const bool uncon = st->uncon_branch != 0;
   const S theta = st->theta, tsum = st->tsum;
-  const H *Y[kMaxM], *Sl[kMaxM];
-  ring_ptrs(st, c.wy, n, Y);
-  ring_ptrs(st, c.ws, n, Sl);
-  S a1[kMaxM + 1], a2[kMaxM], w1[kMaxM], w2[kMaxM];
-#pragma unroll
-  for (int j = 0; j < kMaxM; j++) {
+  __shared__ S a1[kMaxM + 1], a2[kMaxM], w1[kMaxM], w2[kMaxM];  // uniform coefficients
+  if (threadIdx.x < kMaxM) {
+    const int j = threadIdx.x;
     a1[j] = (j < col) ? st->mc[1 + j] : S(0);
     a2[j] = (j < col) ? theta * st->mc[col + 1 + j] : S(0);
     w1[j] = (j < col) ? st->wv[1 + j] : S(0);
     w2[j] = (j < col) ? st->wv[col + 1 + j] : S(0);
+    if (j == 0) a1[kMaxM] = theta;
   }
-  a1[kMaxM] = theta;
   MinPair mn[1] = {MinPair{INFINITY, kNoIndex}};
-  for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < n;
-       i += (long long)gridDim.x * kThreads) {
-    const int code = c.code[i];
-    if (!(uncon || iw_free(code))) continue;
+
+  extern __shared__ __align__(128) unsigned char dyn[];
+  __shared__ StreamSet ss;
+  __shared__ int s_hy, s_hs;
+  if (threadIdx.x == 0) {
+    ss.count = 0;
+    ss.stage_bytes = 0;
+    add_stream(ss, c.code, kTile);
+    add_stream(ss, x, kTile * (int)sizeof(R));
+    add_stream(ss, g, kTile * (int)sizeof(R));
+    add_stream(ss, c.l, kTile * (int)sizeof(R));
+    add_stream(ss, c.u, kTile * (int)sizeof(R));
+    add_stream(ss, c.nbd, kTile * 4);
+    add_history(ss, c, st, s_hy, s_hs);
+  }
+  __syncthreads();
+  const int o_code = ss.off[0], o_x = ss.off[1], o_g = ss.off[2], o_l = ss.off[3];
+  const int o_u = ss.off[4], o_nb = ss.off[5];
+  const int hy = s_hy, hs = s_hs, hb = kTile * (int)sizeof(H);
+  const int cap = stage_capacity(StageBytes<R>::dir, 0, st->m, (int)sizeof(H));
+  run_tiles<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
+            &st->device_error, [&](const unsigned char* buf, long long t, int valid, int e) {
+    if (e >= valid) return;
+    const long long i = t * kTile + e;
+    const int code = stage_at<int8_t>(buf, o_code, e);
+    if (!(uncon || iw_free(code))) return;
     S yv[kMaxM], sv[kMaxM];
 #pragma unroll
     for (int j = 0; j < kMaxM; j++) {
-      yv[j] = (j < col) ? (S)HistTraits<H>::load(Y[j] + i) : S(0);
-      sv[j] = (j < col) ? (S)HistTraits<H>::load(Sl[j] + i) : S(0);
+      yv[j] = (j < col) ? (S)hist_at<H>(buf, hy + j * hb, e) : S(0);
+      sv[j] = (j < col) ? (S)hist_at<H>(buf, hs + j * hb, e) : S(0);
     }
-    const R xi = x[i], gi = g[i];
-    const R li = c.l[i], ui = c.u[i];
+    const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
+    const R li = stage_at<R>(buf, o_l, e), ui = stage_at<R>(buf, o_u, e);
     const R zi = uncon ? xi : gcp_point<R, S>(code, xi, gi, li, ui, tsum);
     S d = reduced_grad<R, S>(uncon, xi, zi, gi, col, yv, sv, a1, a2);
 #pragma unroll
@@ -542,7 +655,7 @@ __global__ void __launch_bounds__(kThreads) k_subsm_dir(Ctx<R, H, S> c, const R*
     const R dr = (R)d;
     c.dsub[i] = dr;
     // candidate step to the bound (1486-1516), filtered as for alpha = 1
-    const int nb = c.nbd[i];
+    const int nb = stage_at<int>(buf, o_nb, e);
     const S dk = (S)dr;
     if (nb != 0) {
       double cand = INFINITY;
@@ -561,13 +674,13 @@ __global__ void __launch_bounds__(kThreads) k_subsm_dir(Ctx<R, H, S> c, const R*
       }
       mn[0] = minpair(mn[0], MinPair{cand, i});
     }
-  }
+  });
   constexpr int W = 2;
   double sdum[1] = {0.0}, xdum[1] = {0.0}, ldum[1] = {0.0};
-  cta_reduce_to_row<0, 0, 1, 0>(sdum, xdum, mn, ldum, c.part, W);
+  cta_reduce_to_row<CONS + 32, 0, 0, 1, 0>(sdum, xdum, mn, ldum, c.part, W);
   if (!last_cta(c.ticket)) return;
   __shared__ double red[W];
-  fold_rows(c.part, gridDim.x, W, 0, 0, 1, red);
+  fold_rows<CONS + 32>(c.part, gridDim.x, W, 0, 0, 1, red);
   if (threadIdx.x != 0) return;
   const S cand = (S)red[0];
   if (cand < S(1)) {
@@ -583,8 +696,8 @@ __global__ void __launch_bounds__(kThreads) k_subsm_dir(Ctx<R, H, S> c, const R*
 
 // ------------------------------------------------------------------------------------
 // D: apply the subspace step, form z and d = z - x, and start the line search.
-template <typename R, typename H, typename S>
-__global__ void __launch_bounds__(kThreads) k_subsm_apply(Ctx<R, H, S> c, const R* __restrict__ x,
+template <typename R, typename H, typename S, int CONS>
+__global__ void __launch_bounds__(CONS + 32) k_subsm_apply(Ctx<R, H, S> c, const R* __restrict__ x,
                                                           const R* __restrict__ g, R* __restrict__ z) {
   DevState<S>* st = c.st;
   if (st->gcp_state == GCP_WALK || st->internal_fail != 0) return;
@@ -597,13 +710,34 @@ __global__ void __launch_bounds__(kThreads) k_subsm_apply(Ctx<R, H, S> c, const 
   const R big = (R)1.0e10;
   double s[2] = {0.0, 0.0};
   MinPair mn[1] = {MinPair{INFINITY, kNoIndex}};
-  for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < n;
-       i += (long long)gridDim.x * kThreads) {
-    const R xi = x[i], gi = g[i], li = c.l[i], ui = c.u[i];
-    const int code = c.code[i];
+
+  extern __shared__ __align__(128) unsigned char dyn[];
+  __shared__ StreamSet ss;
+  if (threadIdx.x == 0) {
+    ss.count = 0;
+    ss.stage_bytes = 0;
+    add_stream(ss, c.code, kTile);
+    add_stream(ss, x, kTile * (int)sizeof(R));
+    add_stream(ss, g, kTile * (int)sizeof(R));
+    add_stream(ss, c.l, kTile * (int)sizeof(R));
+    add_stream(ss, c.u, kTile * (int)sizeof(R));
+    add_stream(ss, c.dsub, kTile * (int)sizeof(R));
+    add_stream(ss, c.nbd, kTile * 4);
+  }
+  __syncthreads();
+  const int o_code = ss.off[0], o_x = ss.off[1], o_g = ss.off[2], o_l = ss.off[3];
+  const int o_u = ss.off[4], o_ds = ss.off[5], o_nb = ss.off[6];
+  const int cap = stage_capacity(StageBytes<R>::apply, 0, 0, (int)sizeof(H));
+  run_tiles<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
+            &st->device_error, [&](const unsigned char* buf, long long t, int valid, int e) {
+    if (e >= valid) return;
+    const long long i = t * kTile + e;
+    const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
+    const R li = stage_at<R>(buf, o_l, e), ui = stage_at<R>(buf, o_u, e);
+    const int code = stage_at<int8_t>(buf, o_code, e);
     R zi = uncon ? xi : gcp_point<R, S>(code, xi, gi, li, ui, tsum);
     if (sub && (uncon || iw_free(code))) {
-      S dk = (S)c.dsub[i];
+      S dk = (S)stage_at<R>(buf, o_ds, e);
       if (i == ibd) {
         if (dk > S(0)) {
           zi = ui;
@@ -620,7 +754,7 @@ __global__ void __launch_bounds__(kThreads) k_subsm_apply(Ctx<R, H, S> c, const 
     s[0] = fma((double)d, (double)d, s[0]);
     s[1] = fma((double)gi, (double)d, s[1]);
     if (want_stpmx) {
-      const int nb = c.nbd[i];
+      const int nb = stage_at<int>(buf, o_nb, e);
       if (nb != 0) {
         double cand = INFINITY;
         if (d < R(0) && nb <= 2) {
@@ -639,13 +773,13 @@ __global__ void __launch_bounds__(kThreads) k_subsm_apply(Ctx<R, H, S> c, const 
         mn[0] = minpair(mn[0], MinPair{cand, i});
       }
     }
-  }
+  });
   constexpr int W = 4;
   double xdum[1] = {0.0}, ldum[1] = {0.0};
-  cta_reduce_to_row<2, 0, 1, 0>(s, xdum, mn, ldum, c.part, W);
+  cta_reduce_to_row<CONS + 32, 2, 0, 1, 0>(s, xdum, mn, ldum, c.part, W);
   if (!last_cta(c.ticket)) return;
   __shared__ double red[W];
-  fold_rows(c.part, gridDim.x, W, 2, 0, 1, red);
+  fold_rows<CONS + 32>(c.part, gridDim.x, W, 2, 0, 1, red);
   if (threadIdx.x != 0) return;
 
   // lnsrlb with task != 1 (1263-1311), then its first dcsrch call (1312-1338)
@@ -703,8 +837,8 @@ __global__ void k_trial(int n, const R* __restrict__ t, const R* __restrict__ z,
 // ------------------------------------------------------------------------------------
 // E: after a function evaluation at xt (gradient gt; t and go are the point and the
 // gradient where the line search started).
-template <typename R, typename H, typename S>
-__global__ void __launch_bounds__(kThreads) k_post_eval(Ctx<R, H, S> c, const R* __restrict__ t,
+template <typename R, typename H, typename S, int CONS>
+__global__ void __launch_bounds__(CONS + 32) k_post_eval(Ctx<R, H, S> c, const R* __restrict__ t,
                                                         const R* __restrict__ z,
                                                         const R* __restrict__ xt,
                                                         const R* __restrict__ gt,
@@ -714,29 +848,54 @@ __global__ void __launch_bounds__(kThreads) k_post_eval(Ctx<R, H, S> c, const R*
   const int n = c.n, col = st->col;
   const R stp = (R)st->stp;
   const bool unit = st->stp == S(1);
-  const H *Y[kMaxM], *Sl[kMaxM];
-  ring_ptrs(st, c.wy, n, Y);
-  ring_ptrs(st, c.ws, n, Sl);
-  H* ysp = c.wy + (size_t)st->spare * n;
-  H* ssp = c.ws + (size_t)st->spare * n;
+  H* ysp = c.wy + (size_t)st->spare * (size_t)c.ld;
+  H* ssp = c.ws + (size_t)st->spare * (size_t)c.ld;
   // sums: [0] g'd, [1] |xold - x|^2, [2] y'y, [3..10] s'y_j, [11..18] s_j's; max: |proj g|
   constexpr int NS = 19, NX = 1;
   double s[NS], xm[NX] = {0.0};
 #pragma unroll
   for (int k = 0; k < NS; k++) s[k] = 0.0;
-  for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < n;
-       i += (long long)gridDim.x * kThreads) {
-    const R ti = t[i], zi = z[i], xi = xt[i], gi = gt[i], gold = go[i];
+
+  extern __shared__ __align__(128) unsigned char dyn[];
+  __shared__ StreamSet ss;
+  __shared__ int s_hy, s_hs;
+  const bool xt_is_z = xt == z;
+  if (threadIdx.x == 0) {
+    ss.count = 0;
+    ss.stage_bytes = 0;
+    add_stream(ss, t, kTile * (int)sizeof(R));
+    add_stream(ss, z, kTile * (int)sizeof(R));
+    add_stream(ss, gt, kTile * (int)sizeof(R));
+    add_stream(ss, go, kTile * (int)sizeof(R));
+    add_stream(ss, c.l, kTile * (int)sizeof(R));
+    add_stream(ss, c.u, kTile * (int)sizeof(R));
+    add_stream(ss, c.nbd, kTile * 4);
+    if (!xt_is_z) add_stream(ss, xt, kTile * (int)sizeof(R));
+    add_history(ss, c, st, s_hy, s_hs);
+  }
+  __syncthreads();
+  const int o_t = ss.off[0], o_z = ss.off[1], o_g = ss.off[2], o_go = ss.off[3];
+  const int o_l = ss.off[4], o_u = ss.off[5], o_nb = ss.off[6];
+  const int o_xt = xt_is_z ? o_z : ss.off[7];
+  const int hy = s_hy, hs = s_hs, hb = kTile * (int)sizeof(H);
+  const int cap = stage_capacity(StageBytes<R>::post, 0, st->m, (int)sizeof(H));
+  run_tiles<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
+            &st->device_error, [&](const unsigned char* buf, long long tt, int valid, int e) {
+    if (e >= valid) return;
+    const long long i = tt * kTile + e;
+    const R ti = stage_at<R>(buf, o_t, e), zi = stage_at<R>(buf, o_z, e);
+    const R xi = stage_at<R>(buf, o_xt, e), gi = stage_at<R>(buf, o_g, e);
+    const R gold = stage_at<R>(buf, o_go, e);
     const R d = rsub(zi, ti);
     s[0] = fma((double)gi, (double)d, s[0]);
     // projgr (1389-1414)
-    const int nb = c.nbd[i];
+    const int nb = stage_at<int>(buf, o_nb, e);
     R pg = gi;
     if (nb != 0) {
       if (gi < R(0)) {
-        if (nb >= 2) pg = smax<R>(rsub(xi, c.u[i]), gi);
+        if (nb >= 2) pg = smax<R>(rsub(xi, stage_at<R>(buf, o_u, e)), gi);
       } else {
-        if (nb <= 2) pg = smin<R>(rsub(xi, c.l[i]), gi);
+        if (nb <= 2) pg = smin<R>(rsub(xi, stage_at<R>(buf, o_l, e)), gi);
       }
     }
     const double apg = fabs((double)pg);
@@ -749,20 +908,20 @@ __global__ void __launch_bounds__(kThreads) k_post_eval(Ctx<R, H, S> c, const R*
 #pragma unroll
     for (int j = 0; j < kMaxM; j++) {
       if (j < col) {
-        s[3 + j] = fma((double)sv, (double)HistTraits<H>::load(Y[j] + i), s[3 + j]);
-        s[11 + j] = fma((double)HistTraits<H>::load(Sl[j] + i), (double)sv, s[11 + j]);
+        s[3 + j] = fma((double)sv, hist_at<H>(buf, hy + j * hb, e), s[3 + j]);
+        s[11 + j] = fma(hist_at<H>(buf, hs + j * hb, e), (double)sv, s[11 + j]);
       }
     }
     ssp[i] = HistTraits<H>::from((double)sv);
     ysp[i] = HistTraits<H>::from((double)y);
-  }
+  });
   constexpr int W = NS + NX;
   MinPair mdum[1] = {MinPair{0.0, 0}};
   double ldum[1] = {0.0};
-  cta_reduce_to_row<NS, NX, 0, 0>(s, xm, mdum, ldum, c.part, W);
+  cta_reduce_to_row<CONS + 32, NS, NX, 0, 0>(s, xm, mdum, ldum, c.part, W);
   if (!last_cta(c.ticket)) return;
   __shared__ double red[W];
-  fold_rows(c.part, gridDim.x, W, NS, NX, 0, red);
+  fold_rows<CONS + 32>(c.part, gridDim.x, W, NS, NX, 0, red);
   if (threadIdx.x != 0) return;
 
   st->f = f;
@@ -894,10 +1053,10 @@ __global__ void __launch_bounds__(kThreads) k_projgr(Ctx<R, H, S> c, const R* __
   }
   double sdum[1] = {0.0}, ldum[1] = {0.0};
   MinPair mdum[1] = {MinPair{0.0, 0}};
-  cta_reduce_to_row<0, 1, 0, 0>(sdum, xm, mdum, ldum, c.part, 1);
+  cta_reduce_to_row<kThreads, 0, 1, 0, 0>(sdum, xm, mdum, ldum, c.part, 1);
   if (!last_cta(c.ticket)) return;
   __shared__ double red[1];
-  fold_rows(c.part, gridDim.x, 1, 0, 1, 0, red);
+  fold_rows<kThreads>(c.part, gridDim.x, 1, 0, 1, 0, red);
   if (threadIdx.x != 0) return;
   c.st->sbgnrm = (S)red[0];
   c.st->f = f;

@@ -45,13 +45,13 @@ struct RowLayout {
 
 // CTA-level reduction of per-thread values into part[blockIdx.x * W + ...].  `lane_owned`
 // values (one distinct output per lane, NL per lane) are summed across warps only.
-template <int NS, int NX, int NM, int NL = 0>
+template <int NT, int NS, int NX, int NM, int NL = 0>
 __device__ __forceinline__ void cta_reduce_to_row(const double (&s)[NS > 0 ? NS : 1],
                                                   const double (&x)[NX > 0 ? NX : 1],
                                                   const MinPair (&mn)[NM > 0 ? NM : 1],
                                                   const double (&lo)[NL > 0 ? NL : 1],
                                                   double* part, int width) {
-  constexpr int kWarps = kThreads / 32;
+  constexpr int kWarps = NT / 32;
   constexpr int kVals = NS + NX + 2 * NM + 32 * NL;
   __shared__ double sm[kWarps][kVals > 0 ? kVals : 1];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -77,7 +77,7 @@ __device__ __forceinline__ void cta_reduce_to_row(const double (&s)[NS > 0 ? NS 
   for (int k = 0; k < NL; k++) sm[warp][NS + NX + 2 * NM + 32 * k + lane] = lo[k];
   __syncthreads();
   double* row = part + (size_t)blockIdx.x * width;
-  for (int k = threadIdx.x; k < kVals; k += kThreads) {
+  for (int k = threadIdx.x; k < kVals; k += NT) {
     if (k >= NS && k < NS + NX) {
       double a = sm[0][k];
       for (int w = 1; w < kWarps; w++) a = (sm[w][k] > a) ? sm[w][k] : a;
@@ -118,10 +118,11 @@ __device__ __forceinline__ bool last_cta(unsigned int* ticket) {
 // for k < ns and k >= ns + nx + 2*nm (lane-owned block), max for the next nx columns,
 // min pairs for the next 2*nm columns.  Warps take columns round robin; lanes stride over
 // rows; a fixed butterfly finishes each column.
+template <int NT>
 __device__ __forceinline__ void fold_rows(const double* part, int rows, int width, int ns,
                                           int nx, int nm, double* out) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int kWarps = kThreads / 32;
+  constexpr int kWarps = NT / 32;
   for (int k = warp; k < width; k += kWarps) {
     const bool is_max = (k >= ns && k < ns + nx);
     const bool is_min = (k >= ns + nx && k < ns + nx + 2 * nm);

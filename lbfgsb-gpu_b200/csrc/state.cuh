@@ -26,6 +26,7 @@ struct DevState {
   int gcp_state, nint, bnded, iword, subsm_active, wrk, uncon_branch;
   int internal_fail;   // 0, or the info code of a failed small-matrix step
   int input_error;     // errclb: bit 0 nbd out of range, bit 1 l > u on a boxed variable
+  int device_error;    // 1 if a bounded wait of a staged-tile pipeline gave up
   int ibkmin, ibd;
   int nbreak, nleft, nfree_mov, nfree, nenter, nleave;
   int pad0;

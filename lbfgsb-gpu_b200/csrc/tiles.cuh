@@ -1,0 +1,202 @@
+// tiles.cuh -- TMA-staged tile pipeline for the streaming passes.
+//
+// Each pass reads up to ~22 element streams (x, g, l, u, nbd, iwhere codes, and the 2*col
+// history columns).  Instead of relying on warps in flight to hide HBM latency (the pass
+// kernels carry many accumulators and run at 1-2 CTAs per SM), one thread per CTA issues
+// one bulk asynchronous copy (cp.async.bulk, completion counted on an mbarrier) per
+// stream per 256-element tile into a multi-stage shared-memory ring; the CTA's threads
+// compute on stage s while stages s+1.. are in flight.  No multicast is used.
+//
+// Every wait on an mbarrier is bounded: after kWaitPolls failed polls the CTA records
+// the failure in *err and stops issuing; the host turns the flag into an error status.
+#pragma once
+
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace lbfgsb_b200 {
+
+constexpr int kTile = 512;          // elements per tile
+constexpr int kMaxStreams = 24;
+constexpr long long kWaitPolls = 1LL << 24;
+
+// Bulk copies need 16-byte aligned addresses and sizes; the host pads the history slot
+// stride to a multiple of kTile elements and checks the user's arrays.
+struct StreamSet {
+  const unsigned char* src[kMaxStreams];  // base of element 0 of the stream
+  int tile_bytes[kMaxStreams];            // bytes of one tile of the stream
+  int off[kMaxStreams];                   // byte offset of the stream in a stage buffer
+  int count;
+  int stage_bytes;
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait; false after kWaitPolls polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (long long k = 0; k < kWaitPolls; k++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// Issue the copies of tile t into stage buffer `buf`, called by all lanes of warp 0:
+// lane 0 posts the byte count, then each lane issues the copies of its streams.
+__device__ __forceinline__ void issue_tile(const StreamSet& ss, long long t, unsigned char* buf,
+                                           uint64_t* bar) {
+  const int lane = threadIdx.x & 31;
+  if (lane == 0) mbar_arrive_expect_tx(bar, (uint32_t)ss.stage_bytes);
+  __syncwarp();
+  for (int j = lane; j < ss.count; j += 32)
+    bulk_g2s(buf + ss.off[j], ss.src[j] + (size_t)t * ss.tile_bytes[j], (uint32_t)ss.tile_bytes[j],
+             bar);
+}
+
+// Fill the partial last tile (elements [t*kTile, n)) with plain loads by the `nthr`
+// threads rank = 0..nthr-1; the rest of the stage is left as is (callers mask by index).
+__device__ __forceinline__ void fill_tail(const StreamSet& ss, long long t, long long n,
+                                          unsigned char* buf, int rank, int nthr) {
+  const long long first = t * kTile;
+  const long long valid = n - first;  // 0 < valid < kTile
+  for (int j = 0; j < ss.count; j++) {
+    const int tb = ss.tile_bytes[j];
+    // bytes of the valid prefix (bit streams round up to whole 32-bit words)
+    long long vb = (long long)tb * valid / kTile;
+    if ((long long)tb * valid % kTile) vb++;
+    if (tb < kTile) vb = ((vb + 3) / 4) * 4;
+    const unsigned char* src = ss.src[j] + (size_t)t * tb;
+    for (long long b = rank; b < vb; b += nthr) buf[ss.off[j] + b] = src[b];
+  }
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Warp-specialised pipeline.  The CTA has CONSUMERS + 32 threads: the last warp is the
+// producer, which issues the bulk copies of the CTA's tiles (grid-stride) into a ring of
+// `stages` buffers; consumer thread e handles elements e, e + CONSUMERS, ... of each tile.
+// full[s] completes when the bytes of the tile in stage s have landed; empty[s] completes
+// when every consumer warp has finished with it.  There is no CTA-wide barrier per tile.
+// The partial last tile is loaded by the producer warp with plain loads and published with
+// a plain arrive on full[s].  body(buf, t, valid,
+// e) must not contain block-level barriers nor write the stage buffer.  Every wait is
+// bounded; on a timeout the CTA sets *err and leaves the loop (returns false).
+template <int CONSUMERS, typename Body>
+__device__ __forceinline__ bool run_tiles(const StreamSet& ss, long long n, int stages,
+                                          unsigned char* ring, uint64_t* bars, int* err,
+                                          Body&& body) {
+  constexpr int kConsumerWarps = CONSUMERS / 32;
+  uint64_t* full = bars;
+  uint64_t* empty = bars + stages;
+  const long long nfull = n / kTile;
+  const long long ntiles = (n + kTile - 1) / kTile;
+  __shared__ int timed_out;
+  if (threadIdx.x == 0) {
+    timed_out = 0;
+    for (int s = 0; s < stages; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kConsumerWarps);
+    }
+    mbar_init_fence();
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp == kConsumerWarps) {
+    // producer
+    long long k = 0;
+    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, k++) {
+      const int s = (int)(k % stages);
+      unsigned char* buf = ring + (size_t)s * ss.stage_bytes;
+      if (k >= stages) {
+        const uint32_t parity = (uint32_t)(((k / stages) - 1) & 1);
+        bool ok = true;
+        if (lane == 0) ok = mbar_wait(&empty[s], parity);
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok || *(volatile int*)&timed_out) {
+          if (lane == 0) timed_out = 1;
+          break;
+        }
+      }
+      if (t < nfull) {
+        issue_tile(ss, t, buf, &full[s]);
+      } else {
+        fill_tail(ss, t, n, buf, lane, 32);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&full[s]);
+      }
+    }
+  } else {
+    // consumers
+    long long k = 0;
+    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, k++) {
+      const int s = (int)(k % stages);
+      unsigned char* buf = ring + (size_t)s * ss.stage_bytes;
+      if (!mbar_wait(&full[s], (uint32_t)((k / stages) & 1))) {
+        timed_out = 1;
+        break;
+      }
+      const int valid = t < nfull ? kTile : (int)(n - t * kTile);
+#pragma unroll
+      for (int h = 0; h < kTile / CONSUMERS; h++) body(buf, t, valid, (int)threadIdx.x + h * CONSUMERS);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+    }
+  }
+  __syncthreads();
+  if (timed_out) {
+    // let the copies still in flight land (bounded) before the CTA's shared memory goes
+    // away: wait on every stage's barrier at each of its two parities
+    if (threadIdx.x == 0) {
+      for (int s = 0; s < stages; s++) {
+        mbar_wait(&full[s], 0);
+        mbar_wait(&full[s], 1);
+      }
+      atomicExch(err, 1);
+    }
+    __syncthreads();
+    return false;
+  }
+  return true;
+}
+
+}  // namespace lbfgsb_b200

@@ -92,8 +92,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(Ctx<R, H, S> c, const R* 
   const long long L = *c.wl_n;
   const S theta = st->theta;
   const H *Y[kMaxM], *Sl[kMaxM];
-  ring_ptrs(st, c.wy, n, Y);
-  ring_ptrs(st, c.ws, n, Sl);
+  ring_ptrs(st, c.wy, c.ld, Y);
+  ring_ptrs(st, c.ws, c.ld, Sl);
 
   __shared__ unsigned long long k_hi[kChunk];
   __shared__ unsigned int k_lo[kChunk];
