@@ -170,14 +170,13 @@ struct PassCfg {
   int grid = 1, stages = 2, smem = 0, threads = 0;
 };
 constexpr int kConsWide = 512;    // consumer threads of the staged passes
-constexpr int kConsNarrow = 256;  // ... of the pass with the most accumulators
 constexpr int kRingBudget = 176 * 1024;
 
 template <typename K>
 static PassCfg pass_cfg(K kernel, int cap, long long n, int threads) {
   PassCfg p;
   p.threads = threads;
-  p.stages = std::max(2, std::min(8, kRingBudget / cap));
+  p.stages = std::max(2, std::min(kMaxStages, kRingBudget / cap));
   p.smem = ring_bytes(p.stages, cap);
   CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, p.smem));
   int per_sm = 0;
@@ -293,8 +292,8 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
     const PassCfg p_gcp = pass_cfg(k_gcp_scan<R, H, S, kConsWide>,
                                    stage_capacity(StageBytes<R>::gcp, 0, m, hsz), n, kConsWide + 32);
     const PassCfg p_freev =
-        pass_cfg(k_freev_formk<R, H, S, kConsNarrow>,
-                 stage_capacity(StageBytes<R>::freev, kTile / 8, m, hsz), n, kConsNarrow + 32);
+        pass_cfg(k_freev_formk<R, H, S, kConsWide>,
+                 stage_capacity(StageBytes<R>::freev, kTile / 8, m, hsz), n, kConsWide + 32);
     const PassCfg p_dir = pass_cfg(k_subsm_dir<R, H, S, kConsWide>,
                                    stage_capacity(StageBytes<R>::dir, 0, m, hsz), n, kConsWide + 32);
     const PassCfg p_apply = pass_cfg(k_subsm_apply<R, H, S, kConsWide>,
@@ -378,7 +377,7 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
         auto subspace = [&]() {
           L.run(KID_FREEV, [&] {
             c.stages = p_freev.stages;
-            k_freev_formk<R, H, S, kConsNarrow><<<p_freev.grid, p_freev.threads, p_freev.smem, stream>>>(c, xcur, gcur);
+            k_freev_formk<R, H, S, kConsWide><<<p_freev.grid, p_freev.threads, p_freev.smem, stream>>>(c, xcur, gcur);
           });
           L.run(KID_SUBDIR, [&] {
             c.stages = p_dir.stages;

@@ -373,24 +373,36 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const
     a2[j] = (j < col) ? theta * st->mc[col + 1 + j] : S(0);
     if (j == 0) a1[kMaxM] = theta;
   }
+  // Three warp roles over every tile (each role covers all kTile elements, so that the
+  // accumulator sets never live in the same thread):
+  //   role 0 (consumer warps 0..7, 2 elements per thread): acc[0..7] sum_F y_j r,
+  //     acc[8..15] sum_F s_j r, the counts (nfree, nenter, nleave, at lower, at upper),
+  //     the free-set bitmask and hash, and the entering / leaving corrections (lane-owned,
+  //     accumulated in shared memory: corr_sm[warp][q] belongs to lane q mod 32);
+  //   role 1 (warps 8..11, 4 elements per thread), when a pair was just added:
+  //     acc[0..7] sum_F y_col y_j, acc[8..15] sum_F s_j y_col;
+  //   role 2 (warps 12..15): acc[0..7] sum_A s_col s_j, acc[8..15] sum_A s_col y_j.
+  static_assert(CONS == 512, "the role split assumes 16 consumer warps");
+  constexpr int kRole0Warps = 8, kRole12Warps = 4;
+  constexpr int NA = 2 * kMaxM + 5, NB = 2 * kMaxM, NC = 2 * kMaxM;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int kWarps = CONS / 32;
-  // sums: [0..7] sum_F y_j r, [8..15] sum_F s_j r, [16..23] yy_new, [24..31] ss_new,
-  // [32..39] sy_row, [40..47] sy_col, [48] nfree, [49] nenter, [50] nleave,
-  // [51] at lower, [52] at upper
-  constexpr int NS = 53;
-  double s[NS];
+  const int role = warp < kRole0Warps ? 0
+                 : warp < kRole0Warps + kRole12Warps ? 1
+                 : warp < kRole0Warps + 2 * kRole12Warps ? 2 : 3;  // 3: the producer
+  const int rt = role == 0 ? (int)threadIdx.x
+               : (int)threadIdx.x - 32 * (kRole0Warps + (role - 1) * kRole12Warps);
+  double acc[2 * kMaxM];
 #pragma unroll
-  for (int k = 0; k < NS; k++) s[k] = 0.0;
-  double corr[kLaneOwned];
-#pragma unroll
-  for (int k = 0; k < kLaneOwned; k++) corr[k] = 0.0;
+  for (int k = 0; k < 2 * kMaxM; k++) acc[k] = 0.0;
+  int cnt[5] = {0, 0, 0, 0, 0};
   unsigned long long hash = 0;
-  __shared__ double bc[kWarps][2 * kMaxM];
-  const int newest = col - 1;
-  int ck[kLaneOwned], ca[kLaneOwned], cb[kLaneOwned];
+  __shared__ double corr_sm[kRole0Warps][32 * kLaneOwned];
+  __shared__ double bc[kRole0Warps][2 * kMaxM];
+  if (role == 0) {
 #pragma unroll
-  for (int k = 0; k < kLaneOwned; k++) corr_map(lane + 32 * k, ck[k], ca[k], cb[k]);
+    for (int k = 0; k < kLaneOwned; k++) corr_sm[warp][32 * k + lane] = 0.0;
+  }
+  const int newest = col - 1;
 
   extern __shared__ __align__(128) unsigned char dyn[];
   __shared__ StreamSet ss;
@@ -408,8 +420,8 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const
   const int o_code = ss.off[0], o_bits = ss.off[1], o_x = ss.off[2], o_g = ss.off[3];
   const int hy = s_hy, hs = s_hs, hb = kTile * (int)sizeof(H);
   const int cap = stage_capacity(StageBytes<R>::freev, kTile / 8, st->m, (int)sizeof(H));
-  run_tiles<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
-            &st->device_error, [&](const unsigned char* buf, long long t, int valid, int e) {
+
+  auto role0 = [&](const unsigned char* buf, long long t, int valid, int e) {
     // the whole warp runs every call (ballots); word e/32 of the tile's free-set bits
     const long long i = t * kTile + e;
     const bool ok = e < valid;
@@ -423,95 +435,92 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const
     const bool leave = track && ok && fprev && !fnow;
     const uint32_t newword = __ballot_sync(0xffffffffu, fnow);
     if (!uncon && lane == 0 && wi * 32 < valid) c.fbits[t * (kTile / 32) + wi] = newword;
-    S yv[kMaxM], sv[kMaxM];
-#pragma unroll
-    for (int j = 0; j < kMaxM; j++) {
-      yv[j] = (ok && j < col) ? (S)hist_at<H>(buf, hy + j * hb, e) : S(0);
-      sv[j] = (ok && j < col) ? (S)hist_at<H>(buf, hs + j * hb, e) : S(0);
-    }
     if (ok) {
       if (fnow) {
-        s[48] += 1.0;
+        cnt[0]++;
         hash += mix64((unsigned long long)i);
         const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
         const R zi = uncon ? xi : gcp_point<R, S>(code, xi, gi, R(0), R(0), tsum);
-        const S r = reduced_grad<R, S>(uncon, xi, zi, gi, col, yv, sv, a1, a2);
+        // the history rows stay in the stage buffer (re-read, not held in registers)
+        S r = -(S)gi;
+        if (!uncon) {
+          r = -a1[kMaxM] * ((S)zi - (S)xi) - (S)gi;
+#pragma unroll
+          for (int j = 0; j < kMaxM; j++)
+            if (j < col)
+              r = r + (S)hist_at<H>(buf, hy + j * hb, e) * a1[j] +
+                  (S)hist_at<H>(buf, hs + j * hb, e) * a2[j];
+        }
 #pragma unroll
         for (int j = 0; j < kMaxM; j++) {
           if (j < col) {
-            s[j] = fma((double)yv[j], (double)r, s[j]);
-            s[8 + j] = fma((double)sv[j], (double)r, s[8 + j]);
-          }
-        }
-        if (updatd) {
-          double ynew = 0;
-#pragma unroll
-          for (int j = 0; j < kMaxM; j++)
-            if (j == newest) ynew = (double)yv[j];
-#pragma unroll
-          for (int j = 0; j < kMaxM; j++) {
-            if (j < col) {
-              s[16 + j] = fma(ynew, (double)yv[j], s[16 + j]);
-              s[40 + j] = fma((double)sv[j], ynew, s[40 + j]);
-            }
+            acc[j] = fma(hist_at<H>(buf, hy + j * hb, e), (double)r, acc[j]);
+            acc[8 + j] = fma(hist_at<H>(buf, hs + j * hb, e), (double)r, acc[8 + j]);
           }
         }
       } else {
-        if (code == IW_LOW || code == IW_WALK_LOW) s[51] += 1.0;
-        if (code == IW_UPP || code == IW_WALK_UPP) s[52] += 1.0;
-        if (updatd) {
-          double snew = 0;
-#pragma unroll
-          for (int j = 0; j < kMaxM; j++)
-            if (j == newest) snew = (double)sv[j];
-#pragma unroll
-          for (int j = 0; j < kMaxM; j++) {
-            if (j < col) {
-              s[24 + j] = fma(snew, (double)sv[j], s[24 + j]);
-              s[32 + j] = fma(snew, (double)yv[j], s[32 + j]);
-            }
-          }
-        }
+        if (code == IW_LOW || code == IW_WALK_LOW) cnt[3]++;
+        if (code == IW_UPP || code == IW_WALK_UPP) cnt[4]++;
       }
-      if (enter) s[49] += 1.0;
-      if (leave) s[50] += 1.0;
+      if (enter) cnt[1]++;
+      if (leave) cnt[2]++;
     }
-    // entering (+) / leaving (-) corrections, one changed variable at a time per warp
-    uint32_t changed = __ballot_sync(0xffffffffu, enter || leave);
-    while (changed) {
-      const int src = __ffs(changed) - 1;
-      changed &= changed - 1;
+    // entering (+) / leaving (-) variables: the whole warp adds the products of the
+    // variable's rows, each lane its kLaneOwned outputs
+    uint32_t pick = __ballot_sync(0xffffffffu, enter || leave);
+    while (pick) {
+      const int src = __ffs(pick) - 1;
+      pick &= pick - 1;
       const double sign = __shfl_sync(0xffffffffu, enter ? 1.0 : -1.0, src);
-#pragma unroll
-      for (int j = 0; j < kMaxM; j++) {
-        const double yj = __shfl_sync(0xffffffffu, (double)yv[j], src);
-        const double sj = __shfl_sync(0xffffffffu, (double)sv[j], src);
-        if (lane == 0) {
-          bc[warp][j] = yj;
-          bc[warp][kMaxM + j] = sj;
-        }
-      }
+      // the source variable's y and s rows, read from the stage buffer by lanes 0..15
+      const int es = e - lane + src;
+      if (lane < kMaxM)
+        bc[warp][lane] = lane < col ? hist_at<H>(buf, hy + lane * hb, es) : 0.0;
+      else if (lane < 2 * kMaxM)
+        bc[warp][lane] = lane - kMaxM < col ? hist_at<H>(buf, hs + (lane - kMaxM) * hb, es) : 0.0;
       __syncwarp();
 #pragma unroll
       for (int k = 0; k < kLaneOwned; k++) {
-        const int kind = ck[k];
+        int kind, a, b;
+        corr_map(lane + 32 * k, kind, a, b);
         if (kind < 3) {
-          const int a = ca[k], b = cb[k];
-          double va, vb;
-          if (kind == 0) {
-            va = bc[warp][a];
-            vb = bc[warp][b];
-          } else if (kind == 1) {
-            va = bc[warp][kMaxM + a];
-            vb = bc[warp][kMaxM + b];
-          } else {
-            va = bc[warp][kMaxM + a];
-            vb = bc[warp][b];
-          }
-          corr[k] = fma(sign * va, vb, corr[k]);
+          const int oa = kind == 0 ? a : kMaxM + a;
+          const int ob = kind == 1 ? kMaxM + b : b;
+          double& cq = corr_sm[warp][32 * k + lane];
+          cq = fma(sign * bc[warp][oa], bc[warp][ob], cq);
         }
       }
       __syncwarp();
+    }
+  };
+  // roles 1 and 2: the new row's products over the free (role 1) or active (role 2) set
+  auto rowprod = [&](const unsigned char* buf, int valid, int e) {
+    if (e >= valid) return;
+    const int code = stage_at<int8_t>(buf, o_code, e);
+    const bool fnow = uncon || iw_free(code);
+    if (fnow != (role == 1)) return;
+    const double a = hist_at<H>(buf, (role == 1 ? hy : hs) + newest * hb, e);
+    const int o1 = role == 1 ? hy : hs;
+#pragma unroll
+    for (int j = 0; j < kMaxM; j++) {
+      if (j < col) {
+        acc[j] = fma(a, hist_at<H>(buf, o1 + j * hb, e), acc[j]);
+        acc[8 + j] = role == 1 ? fma(hist_at<H>(buf, hs + j * hb, e), a, acc[8 + j])
+                               : fma(a, hist_at<H>(buf, hy + j * hb, e), acc[8 + j]);
+      }
+    }
+  };
+  const bool need_row = updatd && col > 0;
+  run_stages<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
+                   &st->device_error, [&](const unsigned char* buf, long long t, int valid) {
+    if (role == 0) {
+#pragma unroll
+      for (int h = 0; h < kTile / (32 * kRole0Warps); h++)
+        role0(buf, t, valid, rt + h * 32 * kRole0Warps);
+    } else if (need_row) {
+#pragma unroll
+      for (int h = 0; h < kTile / (32 * kRole12Warps); h++)
+        rowprod(buf, valid, rt + h * 32 * kRole12Warps);
     }
   });
   // the free-set hash sums mod 2^64 (order free), one atomic per warp
@@ -519,10 +528,38 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const
   for (int o = 16; o > 0; o >>= 1) hash += __shfl_xor_sync(0xffffffffu, hash, o);
   if (lane == 0 && hash != 0) atomicAdd(&st->free_hash_acc, hash);
 
+  // CTA row: [ role 0: 16 sums + 5 counts | role 1: 16 | role 2: 16 | corrections ];
+  // every column is summed over the warps in warp order (fixed)
+  constexpr int NS = NA + NB + NC;
   constexpr int W = NS + 32 * kLaneOwned;
-  double xm[1] = {0.0};
-  MinPair mn[1] = {MinPair{0.0, 0}};
-  cta_reduce_to_row<CONS + 32, NS, 0, 0, kLaneOwned>(s, xm, mn, corr, c.part, W);
+  constexpr int kAllWarps = CONS / 32 + 1;
+  {
+    __shared__ double wsum[kAllWarps][NS];
+    for (int k = lane; k < NS; k += 32) wsum[warp][k] = 0.0;
+    __syncwarp();
+    const int off = role == 0 ? 0 : role == 1 ? NA : NA + NB;
+#pragma unroll
+    for (int k = 0; k < 2 * kMaxM; k++) {
+      const double v = warp_sum(acc[k]);
+      if (lane == 0 && role < 3) wsum[warp][off + k] = v;
+    }
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+      const double v = warp_sum((double)cnt[k]);
+      if (lane == 0 && role == 0) wsum[warp][2 * kMaxM + k] = v;
+    }
+    __syncthreads();
+    double* row = c.part + (size_t)blockIdx.x * W;
+    for (int k = threadIdx.x; k < W; k += CONS + 32) {
+      double a = 0.0;
+      if (k < NS) {
+        for (int w = 0; w < kAllWarps; w++) a += wsum[w][k];
+      } else {
+        for (int w = 0; w < kRole0Warps; w++) a += corr_sm[w][k - NS];
+      }
+      row[k] = a;
+    }
+  }
   if (!last_cta(c.ticket)) return;
   __shared__ double red[W];
   fold_rows<CONS + 32>(c.part, gridDim.x, W, W, 0, 0, red);
@@ -531,11 +568,11 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const
 
   // epilogue: freev's counts and wrk (1143-1161), formk (907-1103), subsm's K solves
   // (1459-1471)
-  const int nfree = (int)red[48];
+  const int nfree = (int)red[16];
   if (!uncon) {
     st->nfree = nfree;
-    st->nenter = (int)red[49];
-    st->nleave = (int)red[50];
+    st->nenter = (int)red[17];
+    st->nleave = (int)red[18];
     st->wrk = (st->nleave > 0 || st->nenter > 0 || updatd) ? 1 : 0;
   } else {
     st->wrk = updatd ? 1 : 0;
@@ -544,17 +581,17 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const
   }
   st->free_hash = st->free_hash_acc;
   st->free_hash_acc = 0;
-  st->at_lower = (unsigned long long)red[51];
-  st->at_upper = (unsigned long long)red[52];
+  st->at_lower = (unsigned long long)red[19];
+  st->at_upper = (unsigned long long)red[20];
   st->subsm_active = (st->nfree != 0 && col != 0) ? 1 : 0;
   if (!st->subsm_active) return;
   if (st->wrk) {
     FormkSums<S>& fs = sw.fs;
     for (int j = 0; j < kMaxM; j++) {
-      fs.yy_new[j] = (S)red[16 + j];
-      fs.ss_new[j] = (S)red[24 + j];
-      fs.sy_row[j] = (S)red[32 + j];
-      fs.sy_col[j] = (S)red[40 + j];
+      fs.yy_new[j] = (S)red[NA + j];
+      fs.sy_col[j] = (S)red[NA + kMaxM + j];
+      fs.ss_new[j] = (S)red[NA + NB + j];
+      fs.sy_row[j] = (S)red[NA + NB + kMaxM + j];
     }
     for (int q = 0; q < 32 * kLaneOwned; q++) {
       int kind, a, b;

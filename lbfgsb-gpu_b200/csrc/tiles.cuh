@@ -2,10 +2,10 @@
 //
 // Each pass reads up to ~22 element streams (x, g, l, u, nbd, iwhere codes, and the 2*col
 // history columns).  Instead of relying on warps in flight to hide HBM latency (the pass
-// kernels carry many accumulators and run at 1-2 CTAs per SM), one thread per CTA issues
-// one bulk asynchronous copy (cp.async.bulk, completion counted on an mbarrier) per
-// stream per 256-element tile into a multi-stage shared-memory ring; the CTA's threads
-// compute on stage s while stages s+1.. are in flight.  No multicast is used.
+// kernels carry many accumulators and run one CTA per SM), the lanes of one warp issue one
+// bulk asynchronous copy (cp.async.bulk, completion counted on an mbarrier) per stream per
+// kTile-element tile into a multi-stage shared-memory ring; the CTA's threads compute on
+// stage s while stages s+1.. are in flight.  No multicast is used.
 //
 // Every wait on an mbarrier is bounded: after kWaitPolls failed polls the CTA records
 // the failure in *err and stops issuing; the host turns the flag into an error status.
@@ -112,23 +112,39 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
-// Warp-specialised pipeline.  The CTA has CONSUMERS + 32 threads: the last warp is the
-// producer, which issues the bulk copies of the CTA's tiles (grid-stride) into a ring of
-// `stages` buffers; consumer thread e handles elements e, e + CONSUMERS, ... of each tile.
-// full[s] completes when the bytes of the tile in stage s have landed; empty[s] completes
-// when every consumer warp has finished with it.  There is no CTA-wide barrier per tile.
-// The partial last tile is loaded by the producer warp with plain loads and published with
-// a plain arrive on full[s].  body(buf, t, valid,
-// e) must not contain block-level barriers nor write the stage buffer.  Every wait is
-// bounded; on a timeout the CTA sets *err and leaves the loop (returns false).
+// Stage buffer of tile t: full tiles by bulk copies (lanes of the calling warp issue the
+// copies of their streams), the partial last tile by plain loads of the warp's lanes and a
+// plain arrive.  Called by a whole warp.
+__device__ __forceinline__ void load_tile(const StreamSet& ss, long long t, long long n,
+                                          unsigned char* buf, uint64_t* full) {
+  const int lane = threadIdx.x & 31;
+  if ((t + 1) * kTile <= n) {
+    issue_tile(ss, t, buf, full);
+  } else {
+    fill_tail(ss, t, n, buf, lane, 32);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(full);
+  }
+}
+
+constexpr int kMaxStages = 8;
+
+// Warp-specialised tile pipeline.  The CTA has CONSUMERS + 32 threads: the last warp is
+// the producer, which issues the copies of the CTA's tiles (grid-stride over the n
+// elements) into a ring of `stages` stage buffers; the consumer threads run
+// body(buf, t, valid) once per tile.  full[s] completes when the bytes of the tile in
+// stage s have landed; empty[s] completes when every consumer warp has finished with it.
+// There is no CTA-wide barrier per tile, and the producer issues a freed stage's next
+// tile while the consumers work on the other stages.  body must not contain block-level
+// barriers nor write the stage buffer.  Every wait is bounded; on a timeout the CTA sets
+// *err and leaves the loop (returns false).
 template <int CONSUMERS, typename Body>
-__device__ __forceinline__ bool run_tiles(const StreamSet& ss, long long n, int stages,
-                                          unsigned char* ring, uint64_t* bars, int* err,
-                                          Body&& body) {
+__device__ __forceinline__ bool run_stages(const StreamSet& ss, long long n, int stages,
+                                           unsigned char* ring, uint64_t* bars, int* err,
+                                           Body&& body) {
   constexpr int kConsumerWarps = CONSUMERS / 32;
   uint64_t* full = bars;
   uint64_t* empty = bars + stages;
-  const long long nfull = n / kTile;
   const long long ntiles = (n + kTile - 1) / kTile;
   __shared__ int timed_out;
   if (threadIdx.x == 0) {
@@ -146,7 +162,6 @@ __device__ __forceinline__ bool run_tiles(const StreamSet& ss, long long n, int 
     long long k = 0;
     for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, k++) {
       const int s = (int)(k % stages);
-      unsigned char* buf = ring + (size_t)s * ss.stage_bytes;
       if (k >= stages) {
         const uint32_t parity = (uint32_t)(((k / stages) - 1) & 1);
         bool ok = true;
@@ -157,27 +172,21 @@ __device__ __forceinline__ bool run_tiles(const StreamSet& ss, long long n, int 
           break;
         }
       }
-      if (t < nfull) {
-        issue_tile(ss, t, buf, &full[s]);
-      } else {
-        fill_tail(ss, t, n, buf, lane, 32);
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&full[s]);
-      }
+      load_tile(ss, t, n, ring + (size_t)s * ss.stage_bytes, &full[s]);
     }
   } else {
     // consumers
     long long k = 0;
     for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, k++) {
       const int s = (int)(k % stages);
-      unsigned char* buf = ring + (size_t)s * ss.stage_bytes;
-      if (!mbar_wait(&full[s], (uint32_t)((k / stages) & 1))) {
-        timed_out = 1;
+      const unsigned char* buf = ring + (size_t)s * ss.stage_bytes;
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(&full[s], (uint32_t)((k / stages) & 1)));
+      if (!ok) {
+        if (lane == 0) timed_out = 1;
         break;
       }
-      const int valid = t < nfull ? kTile : (int)(n - t * kTile);
-#pragma unroll
-      for (int h = 0; h < kTile / CONSUMERS; h++) body(buf, t, valid, (int)threadIdx.x + h * CONSUMERS);
+      const int valid = t * kTile + kTile <= n ? kTile : (int)(n - t * kTile);
+      body(buf, t, valid);
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
     }
@@ -197,6 +206,20 @@ __device__ __forceinline__ bool run_tiles(const StreamSet& ss, long long n, int 
     return false;
   }
   return true;
+}
+
+// run_stages with consumer thread e handling elements e, e + CONSUMERS, ... of each
+// tile: body(buf, t, valid, e).
+template <int CONSUMERS, typename Body>
+__device__ __forceinline__ bool run_tiles(const StreamSet& ss, long long n, int stages,
+                                          unsigned char* ring, uint64_t* bars, int* err,
+                                          Body&& body) {
+  return run_stages<CONSUMERS>(ss, n, stages, ring, bars, err,
+                               [&](const unsigned char* buf, long long t, int valid) {
+#pragma unroll
+    for (int h = 0; h < kTile / CONSUMERS; h++)
+      body(buf, t, valid, (int)threadIdx.x + h * CONSUMERS);
+  });
 }
 
 }  // namespace lbfgsb_b200

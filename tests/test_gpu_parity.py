@@ -13,7 +13,8 @@ decisions can only agree while the iterates agree):
         agree; for runs whose trace never diverges: same exit code and iteration count,
         final f within 1e-10 relative, final x within 1e-6 of max|x|; for a run that
         diverges after >= 100 identical iterations: f within 1e-10 for the first 50
-        iterations and 1e-8 up to the divergence, final f within 1e-5 relative.
+        iterations and 1e-6 up to the divergence (the oracle's own sensitivity to a 1e-16
+        perturbation of x0 reaches ~2e-7 there), final f within 1e-5 relative.
   FP32  (plain form, float scalars like the reference's float path) same exit code, the
         first 10 iterations' trace equal, final f within 1e-5 relative.
 """
@@ -97,17 +98,25 @@ def test_f64_trace_matches_oracle(LB, OB, golden, name):
 
 
 def test_f64_long_tight_run(LB, OB, golden):
-    """300 iterations against bounds of +-0.01: the traces agree for at least the first 100
-    iterations; afterwards the runs take different but equally valid paths, and the final
-    values agree to 1e-5 relative (the f-test stops at 1e-8 relative decrease per step)."""
+    """300 iterations against bounds of +-0.01.  This trajectory amplifies rounding: moving
+    x0 by 1e-16 relative (or 1e-19 absolute) moves the oracle's own f by up to ~2e-7
+    relative around iteration 100 while its discrete trace still agrees
+    (tests/test_oracle_pin.py::test_long_tight_run_sensitivity).  So: the traces agree for
+    at least the first 100 iterations, f within 1e-10 for the first 50 of them and within
+    1e-6 up to the divergence; afterwards the runs take different but equally valid paths,
+    and the final values agree to 1e-5 relative (the f-test stops at 1e-8 relative
+    decrease per step)."""
     prob, dt, a, b = run_pair(LB, OB, "synth_s64_f64_b001")
     k = first_divergence(a.trace, b.trace)
     assert k >= 100
     for i, (ra, rb) in enumerate(zip(a.trace[:k], b.trace[:k])):
-        assert relf(ra["f"], rb["f"]) <= (1e-10 if i < 50 else 1e-8)
+        assert relf(ra["f"], rb["f"]) <= (1e-10 if i < 50 else 1e-6)
     assert b.info == a.info
     assert relf(a.trace[-1]["f"], b.trace[-1]["f"]) <= 1e-5
-    assert np.all(b.x >= prob["l"] - 1e-15) and np.all(b.x <= prob["u"] + 1e-15)
+    nbd = prob["nbd"]
+    has_l = (nbd == 1) | (nbd == 2)
+    has_u = (nbd == 2) | (nbd == 3)
+    assert np.all(b.x[has_l] >= prob["l"][has_l]) and np.all(b.x[has_u] <= prob["u"][has_u])
 
 
 @pytest.mark.parametrize("name", F32_CASES)

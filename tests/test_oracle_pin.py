@@ -77,3 +77,28 @@ def test_oracle_matches_live_reference(s, seed, bound, dtype):
     assert a.iters == b.iters
     np.testing.assert_array_equal(a.x, b.x)
     assert a.info == b.info
+
+
+TRACE_KEYS = ["nint", "nbreak", "nfree", "nenter", "nleave", "col", "head", "iword",
+              "free_hash", "at_lower", "at_upper", "nfgv", "ifun"]
+
+
+def test_long_tight_run_sensitivity():
+    """The conditioning behind the GPU tolerance of synth_s64_f64_b001: moving the start
+    point (x0 = 0) by 1e-19 leaves the oracle's discrete trace unchanged for at least 90
+    iterations, yet moves its f by more than 1e-8 relative within that agreed prefix."""
+    prob, dtype, x0, over, stop = make_case("synth_s64_f64_b001")
+    opt = apply_options(B.default_option(dtype), over)
+    a = B.run_cpu("oracle", prob, dtype, option=opt, trace=True)
+    n = prob["nbd"].size
+    xp = 1e-19 * np.random.default_rng(1).standard_normal(n)
+    b = B.run_cpu("oracle", prob, dtype, x0=xp, option=opt, trace=True)
+    k = 0
+    worst = 0.0
+    for ra, rb in zip(a.trace, b.trace):
+        if any(ra[key] != rb[key] for key in TRACE_KEYS):
+            break
+        worst = max(worst, abs(ra["f"] - rb["f"]) / max(1.0, abs(ra["f"])))
+        k += 1
+    assert k >= 90
+    assert worst > 1e-8
