@@ -96,44 +96,6 @@ __device__ __forceinline__ void cta_reduce_to_row(const double (&s)[NS > 0 ? NS 
   }
 }
 
-// CTA reduction for a kernel whose warps take one of two roles: role-0 warps hold NA sums
-// and NL lane-owned values, role-1 warps NB sums, in the same accumulator array acc (a
-// warp that accumulated nothing passes zeros).  Row layout: [ role-0 sums (NA) | role-1 sums (NB) |
-// lane-owned (32*NL) ]; every column is summed over all warps in warp order (the other
-// role's warps add zeros), so the order is fixed.
-template <int NT, int NA, int NB, int NL>
-__device__ __forceinline__ void cta_reduce_roles(const double (&acc)[NA > NB ? NA : NB], int role,
-                                                 const double (&lo)[NL], double* part, int width) {
-  constexpr int kWarps = NT / 32;
-  constexpr int kVals = NA + NB + 32 * NL;
-  __shared__ double sm[kWarps][kVals];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int NMAX = NA > NB ? NA : NB;
-#pragma unroll
-  for (int k = 0; k < NMAX; k++) {
-    const double v = warp_sum(acc[k]);
-    if (lane == 0) {
-      if (role == 0 && k < NA) sm[warp][k] = v;
-      if (role == 1 && k < NB) sm[warp][NA + k] = v;
-    }
-  }
-  if (lane == 0) {
-    if (role == 0)
-      for (int k = NA; k < NA + NB; k++) sm[warp][k] = 0.0;
-    else
-      for (int k = 0; k < NA; k++) sm[warp][k] = 0.0;
-  }
-#pragma unroll
-  for (int k = 0; k < NL; k++) sm[warp][NA + NB + 32 * k + lane] = role == 0 ? lo[k] : 0.0;
-  __syncthreads();
-  double* row = part + (size_t)blockIdx.x * width;
-  for (int k = threadIdx.x; k < kVals; k += NT) {
-    double a = 0;
-    for (int w = 0; w < kWarps; w++) a += sm[w][k];
-    row[k] = a;
-  }
-}
-
 // Ticket: returns true in exactly one CTA (the last to arrive), after all rows are
 // visible.  Resets the ticket for the next launch.
 __device__ __forceinline__ bool last_cta(unsigned int* ticket) {
