@@ -193,6 +193,23 @@ int lbfgsb_b200_synth_funcgrad_f32(void* handle, float* x, float* f, float* g, v
  * device, 2 device to host, 3 device to device). */
 int lbfgsb_b200_copy(void* dst, const void* src, size_t bytes, int kind);
 
+/* ---- projected-gradient norm that allocates nothing (no counterpart in the reference) --
+ * *sbgnrm (device) = max_i |pg_i|, the reference's projgr (culbfgsb/lbfgsbcpu.cpp:1390)
+ * and the value the solver reports as summary.residual_g; x, g, nbd, l, u are device
+ * arrays of length n.  Enqueued on `stream`, nothing is synchronised.  It calls no
+ * allocator: its scratch is a static 64 KB device array, so n is limited to
+ * 0..33554432 (8192 per-CTA maxima of 4096 variables); a larger n returns
+ * LBFGSB_B200_ERR_ARGUMENT with a message in lbfgsb_b200_last_error().  Meant for callers
+ * that must not allocate, such as the solver's callbacks, which run in the middle of its
+ * stream work.  Every call on a device shares the scratch: calls that overlap on the GPU
+ * (streams not ordered with each other) race, so issue them in order.  The scratch's
+ * arrival ticket must be zero when a call starts; it is zero at load and each call leaves
+ * it zero.  The first call on a device looks up the scratch address
+ * (cudaGetSymbolAddress); make that first call outside any stream capture. */
+int lbfgsb_b200_projgr_noalloc_f64(int n, const double* x, const double* g, const int* nbd,
+                                   const double* l, const double* u, double* sbgnrm,
+                                   void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -86,7 +86,7 @@ EXPORTS = [
     "lbfgsb_b200_minimize_ext_f64", "lbfgsb_b200_minimize_ext_f32",
     "lbfgsb_b200_last_stats", "lbfgsb_b200_last_error", "lbfgsb_b200_synth_create",
     "lbfgsb_b200_synth_destroy", "lbfgsb_b200_synth_funcgrad_f64",
-    "lbfgsb_b200_synth_funcgrad_f32", "lbfgsb_b200_copy",
+    "lbfgsb_b200_synth_funcgrad_f32", "lbfgsb_b200_copy", "lbfgsb_b200_projgr_noalloc_f64",
 ]
 
 _lib = None
@@ -125,6 +125,8 @@ def load() -> C.CDLL:
     lib.lbfgsb_b200_synth_destroy.argtypes = [C.c_void_p]
     lib.lbfgsb_b200_copy.restype = C.c_int
     lib.lbfgsb_b200_copy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
+    lib.lbfgsb_b200_projgr_noalloc_f64.restype = C.c_int
+    lib.lbfgsb_b200_projgr_noalloc_f64.argtypes = [C.c_int] + [C.c_void_p] * 7
     _lib = lib
     return lib
 
