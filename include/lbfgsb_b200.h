@@ -97,8 +97,8 @@ void lbfgsb_b200_default_option_f32(lbfgsb_b200_option_f32* option);
  * breakpoint walk for the Cauchy point, subspace step truncated at the first bound).
  * x is updated in place with the final iterate.  after_iteration and
  * customized_stopping may be NULL.  The workspace (about 6 vectors of n reals, 18 of n
- * history elements, n bytes + n bits) is allocated on `stream` for the duration of the
- * call. */
+ * history elements, n bytes + n bits) is taken on `stream` from the library's per-device
+ * memory pool for the duration of the call (see lbfgsb_b200_trim_memory). */
 int lbfgsb_b200_minimize_f64(int n, double* x, const int* nbd, const double* l,
                              const double* u, const lbfgsb_b200_option_f64* option,
                              lbfgsb_b200_callback_f64 funcgrad,
@@ -173,6 +173,12 @@ int lbfgsb_b200_last_stats(lbfgsb_b200_stats* out);
 
 /* Message of the last LBFGSB_B200_ERR_CUDA on the calling thread ("" if none). */
 const char* lbfgsb_b200_last_error(void);
+
+/* The solver's workspace comes from a library-owned memory pool per device that keeps its
+ * memory between solves (no counterpart in the reference, which allocates and frees with
+ * cudaMalloc/cudaFree in every call).  This returns the unused memory of every pool to
+ * its device; call it when no solve is running. */
+int lbfgsb_b200_trim_memory(void);
 
 /* ---- synthetic objective (test and benchmark glue, no reference counterpart) ---------
  * f(x) = sum_k 0.5*kappa_k*((x_{i+1,j}-x_k)^2 + (x_{i,j+1}-x_k)^2)

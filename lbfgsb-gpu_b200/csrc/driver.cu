@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -125,6 +126,33 @@ class Launcher {
 };
 
 // Owns the device workspace of one solve.
+// Workspace memory comes from a library-owned stream-ordered pool per device that keeps
+// its memory between solves (release threshold: unlimited), so repeated solves do not map
+// and unmap gigabytes each time; lbfgsb_b200_trim_memory() returns it to the device.
+constexpr int kMaxDevices = 64;
+static std::mutex g_pool_mu;
+static cudaMemPool_t g_pools[kMaxDevices] = {};
+
+static cudaMemPool_t workspace_pool() {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) throw CudaFailure{cudaErrorInvalidDevice, "device ordinal", __LINE__};
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool;
+    CK(cudaMemPoolCreate(&pool, &props));
+    uint64_t keep = ~0ull;
+    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    g_pools[dev] = pool;
+  }
+  return g_pools[dev];
+}
+
 template <typename R, typename H, typename S>
 struct Workspace {
   cudaStream_t s = nullptr;
@@ -147,15 +175,34 @@ struct Workspace {
   template <typename T>
   T* alloc(size_t count) {
     void* p = nullptr;
-    CK(cudaMallocAsync(&p, std::max<size_t>(count, 1) * sizeof(T), s));
+    CK(cudaMallocFromPoolAsync(&p, std::max<size_t>(count, 1) * sizeof(T), workspace_pool(), s));
     blocks.push_back(p);
     return static_cast<T*>(p);
   }
   ~Workspace() {
     for (void* p : blocks) cudaFreeAsync(p, s);
-    if (hs) cudaFreeHost(hs);
   }
 };
+
+// Pinned host mirror of the state header, kept per thread (one page, allocated once).
+static void* pinned_mirror(size_t bytes) {
+  struct Mirror {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~Mirror() {
+      if (p) cudaFreeHost(p);
+    }
+  };
+  thread_local Mirror m;
+  if (m.bytes < bytes) {
+    if (m.p) CK(cudaFreeHost(m.p));
+    m.p = nullptr;
+    m.bytes = 0;
+    CK(cudaMallocHost(&m.p, bytes));
+    m.bytes = bytes;
+  }
+  return m.p;
+}
 
 static int device_sms() {
   int dev = 0, sms = 0;
@@ -243,7 +290,7 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
     w.fbits = w.template alloc<uint32_t>(words);
     w.st = w.template alloc<DevState<S>>(1);
     w.ticket = w.template alloc<unsigned int>(1);
-    CK(cudaMallocHost(&w.hs, sizeof(DevState<S>)));
+    w.hs = static_cast<DevState<S>*>(pinned_mirror(sizeof(DevState<S>)));
 
     // the staged passes copy l, u and nbd in 16-byte aligned tiles
     const R* la = l;
@@ -674,6 +721,19 @@ int lbfgsb_b200_last_stats(lbfgsb_b200_stats* out) {
 }
 
 const char* lbfgsb_b200_last_error(void) { return g_last_error.c_str(); }
+
+int lbfgsb_b200_trim_memory(void) {
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  for (int d = 0; d < kMaxDevices; d++) {
+    if (!g_pools[d]) continue;
+    cudaError_t e = cudaMemPoolTrimTo(g_pools[d], 0);
+    if (e != cudaSuccess) {
+      g_last_error = cudaGetErrorString(e);
+      return LBFGSB_B200_ERR_CUDA;
+    }
+  }
+  return LBFGSB_B200_OK;
+}
 
 int lbfgsb_b200_copy(void* dst, const void* src, size_t bytes, int kind) {
   cudaMemcpyKind k = kind == 1   ? cudaMemcpyHostToDevice

@@ -87,6 +87,7 @@ EXPORTS = [
     "lbfgsb_b200_last_stats", "lbfgsb_b200_last_error", "lbfgsb_b200_synth_create",
     "lbfgsb_b200_synth_destroy", "lbfgsb_b200_synth_funcgrad_f64",
     "lbfgsb_b200_synth_funcgrad_f32", "lbfgsb_b200_copy", "lbfgsb_b200_projgr_noalloc_f64",
+    "lbfgsb_b200_trim_memory",
 ]
 
 _lib = None
