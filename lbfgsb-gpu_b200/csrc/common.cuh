@@ -42,6 +42,64 @@ __device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b)
 __device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float rdiv(float a, float b) { return __fdiv_rn(a, b); }
 
+// Correctly rounded a / b for a divisor b that is the same over a whole pass (theta),
+// from y = RN(1/b) computed once.  Markstein's theorem (P. Markstein, "Computation of
+// elementary functions on the IBM RISC System/6000 processor", IBM J. Res. Develop. 34(1),
+// 1990; restated in Muller et al., Handbook of Floating-Point Arithmetic, ch. 4): if
+// y = RN(1/b) and q is a faithful approximation of a/b, then r = a - b*q is exactly
+// representable (one fma computes it) and RN(q + r*y) = RN(a/b).  q0 = RN(a*y) is within
+// about 2 ulp of a/b, so one correction q1 = RN(q0 + r0*y) first makes it faithful, and a
+// second one gives the correctly rounded quotient.  The theorem needs every intermediate
+// in the normal range: the caller passes fast = false unless |b| is in [2^-300, 2^300]
+// (double) / [2^-30, 2^30] (float), and |a| outside [2^-600, 2^600] / [2^-60, 2^60] (zero,
+// subnormal, infinite, NaN included) takes the full division.
+struct FixedDiv64 {
+  double b, y;
+  bool fast;
+  __device__ __forceinline__ explicit FixedDiv64(double b_) : b(b_) {
+    const double ab = fabs(b_);
+    fast = ab >= 0x1p-300 && ab <= 0x1p300;
+    y = __ddiv_rn(1.0, b_);
+  }
+  __device__ __forceinline__ double operator()(double a) const {
+    const double aa = fabs(a);
+    if (!(fast && aa >= 0x1p-600 && aa <= 0x1p600)) return __ddiv_rn(a, b);
+    double q = __dmul_rn(a, y);
+    double r = __fma_rn(-q, b, a);
+    q = __fma_rn(r, y, q);
+    r = __fma_rn(-q, b, a);
+    return __fma_rn(r, y, q);
+  }
+};
+struct FixedDiv32 {
+  float b, y;
+  bool fast;
+  __device__ __forceinline__ explicit FixedDiv32(float b_) : b(b_) {
+    const float ab = fabsf(b_);
+    fast = ab >= 0x1p-30f && ab <= 0x1p30f;
+    y = __fdiv_rn(1.0f, b_);
+  }
+  __device__ __forceinline__ float operator()(float a) const {
+    const float aa = fabsf(a);
+    if (!(fast && aa >= 0x1p-60f && aa <= 0x1p60f)) return __fdiv_rn(a, b);
+    float q = __fmul_rn(a, y);
+    float r = __fmaf_rn(-q, b, a);
+    q = __fmaf_rn(r, y, q);
+    r = __fmaf_rn(-q, b, a);
+    return __fmaf_rn(r, y, q);
+  }
+};
+template <typename S>
+struct FixedDiv;
+template <>
+struct FixedDiv<double> : FixedDiv64 {
+  using FixedDiv64::FixedDiv64;
+};
+template <>
+struct FixedDiv<float> : FixedDiv32 {
+  using FixedDiv32::FixedDiv32;
+};
+
 // Splitmix64 finaliser: the order-free hash of the free set used by the trace.
 __host__ __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
   z += 0x9E3779B97F4A7C15ULL;

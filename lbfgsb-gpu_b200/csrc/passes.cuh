@@ -124,6 +124,22 @@ __device__ __forceinline__ double hist_at(const unsigned char* buf, int off, int
   }
 }
 
+// The history loops run over the col live columns.  In the steady state col == kMaxM and
+// the pass body is compiled with that as a constant (the unrolled loops carry no
+// per-column tests); otherwise with the runtime col.  f(tag): decltype(tag)::value is
+// kMaxM or -1.
+template <int V>
+struct Cols {
+  static constexpr int value = V;
+};
+template <typename F>
+__device__ __forceinline__ void dispatch_cols(int col, F&& f) {
+  if (col == kMaxM)
+    f(Cols<kMaxM>{});
+  else
+    f(Cols<-1>{});
+}
+
 // cauchy's per-variable classification (lbfgsbcpu.cpp:635-663) and breakpoint
 // (675-699).  Returns the iwhere code; sets has_bp/t for a movable variable with a
 // breakpoint.  The static codes -1 (nbd 0) and 3 (l == u) come from nbd, l, u, which is
@@ -223,35 +239,38 @@ __global__ void __launch_bounds__(CONS + 32) k_gcp_scan(Ctx<R, H, S> c, const R*
   const int o_x = ss.off[0], o_g = ss.off[1], o_l = ss.off[2], o_u = ss.off[3], o_nb = ss.off[4];
   const int hy = s_hy, hs = s_hs, hb = kTile * (int)sizeof(H);
   const int cap = stage_capacity(StageBytes<R>::gcp, 0, st->m, (int)sizeof(H));
-  run_tiles<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
-            &st->device_error, [&](const unsigned char* buf, long long t, int valid, int e) {
-    if (e >= valid) return;
-    const long long i = t * kTile + e;
-    const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
-    const R li = stage_at<R>(buf, o_l, e), ui = stage_at<R>(buf, o_u, e);
-    const int nb = stage_at<int>(buf, o_nb, e);
-    bool has_bp;
-    R tb;
-    const int code = classify(xi, gi, li, ui, nb, has_bp, tb);
-    c.code[i] = (int8_t)code;
-    if (code == IW_FREE || code == IW_UNB) {
-      const double neggi = -(double)gi;
-      s[0] = fma(neggi, neggi, s[0]);
-#pragma unroll
-      for (int j = 0; j < kMaxM; j++) {
-        if (j < col) {
-          s[1 + j] = fma(hist_at<H>(buf, hy + j * hb, e), neggi, s[1 + j]);
-          s[9 + j] = fma(hist_at<H>(buf, hs + j * hb, e), neggi, s[9 + j]);
+  dispatch_cols(col, [&](auto cols_tag) {
+    constexpr bool kFull = decltype(cols_tag)::value == kMaxM;
+    run_tiles<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
+              &st->device_error, [&](const unsigned char* buf, long long t, int valid, int e) {
+      if (e >= valid) return;
+      const long long i = t * kTile + e;
+      const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
+      const R li = stage_at<R>(buf, o_l, e), ui = stage_at<R>(buf, o_u, e);
+      const int nb = stage_at<int>(buf, o_nb, e);
+      bool has_bp;
+      R tb;
+      const int code = classify(xi, gi, li, ui, nb, has_bp, tb);
+      c.code[i] = (int8_t)code;
+      if (code == IW_FREE || code == IW_UNB) {
+        const double neggi = -(double)gi;
+        s[0] = fma(neggi, neggi, s[0]);
+  #pragma unroll
+        for (int j = 0; j < kMaxM; j++) {
+          if (kFull || j < col) {
+            s[1 + j] = fma(hist_at<H>(buf, hy + j * hb, e), neggi, s[1 + j]);
+            s[9 + j] = fma(hist_at<H>(buf, hs + j * hb, e), neggi, s[9 + j]);
+          }
+        }
+        if (has_bp) {
+          s[17] += 1.0;
+          mn[0] = minpair(mn[0], MinPair{(double)tb, i});
+        } else {
+          s[18] += 1.0;
+          if (neggi != 0.0) xm[0] = 1.0;
         }
       }
-      if (has_bp) {
-        s[17] += 1.0;
-        mn[0] = minpair(mn[0], MinPair{(double)tb, i});
-      } else {
-        s[18] += 1.0;
-        if (neggi != 0.0) xm[0] = 1.0;
-      }
-    }
+    });
   });
   constexpr int W = NS + NX + 2 * NM;
   double lo[1] = {0.0};
@@ -421,107 +440,110 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const
   const int hy = s_hy, hs = s_hs, hb = kTile * (int)sizeof(H);
   const int cap = stage_capacity(StageBytes<R>::freev, kTile / 8, st->m, (int)sizeof(H));
 
-  auto role0 = [&](const unsigned char* buf, long long t, int valid, int e) {
-    // the whole warp runs every call (ballots); word e/32 of the tile's free-set bits
-    const long long i = t * kTile + e;
-    const bool ok = e < valid;
-    int code = IW_LOW;
-    if (ok) code = stage_at<int8_t>(buf, o_code, e);
-    const bool fnow = ok && (uncon || iw_free(code));
-    const int wi = e >> 5;
-    const uint32_t word = stage_at<uint32_t>(buf, o_bits, wi);
-    const bool fprev = (word >> lane) & 1u;
-    const bool enter = track && ok && !fprev && fnow;
-    const bool leave = track && ok && fprev && !fnow;
-    const uint32_t newword = __ballot_sync(0xffffffffu, fnow);
-    if (!uncon && lane == 0 && wi * 32 < valid) c.fbits[t * (kTile / 32) + wi] = newword;
-    if (ok) {
-      if (fnow) {
-        cnt[0]++;
-        hash += mix64((unsigned long long)i);
-        const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
-        const R zi = uncon ? xi : gcp_point<R, S>(code, xi, gi, R(0), R(0), tsum);
-        // the history rows stay in the stage buffer (re-read, not held in registers)
-        S r = -(S)gi;
-        if (!uncon) {
-          r = -a1[kMaxM] * ((S)zi - (S)xi) - (S)gi;
-#pragma unroll
-          for (int j = 0; j < kMaxM; j++)
-            if (j < col)
-              r = r + (S)hist_at<H>(buf, hy + j * hb, e) * a1[j] +
-                  (S)hist_at<H>(buf, hs + j * hb, e) * a2[j];
+  dispatch_cols(col, [&](auto cols_tag) {
+    constexpr bool kFull = decltype(cols_tag)::value == kMaxM;
+    auto role0 = [&](const unsigned char* buf, long long t, int valid, int e) {
+      // the whole warp runs every call (ballots); word e/32 of the tile's free-set bits
+      const long long i = t * kTile + e;
+      const bool ok = e < valid;
+      int code = IW_LOW;
+      if (ok) code = stage_at<int8_t>(buf, o_code, e);
+      const bool fnow = ok && (uncon || iw_free(code));
+      const int wi = e >> 5;
+      const uint32_t word = stage_at<uint32_t>(buf, o_bits, wi);
+      const bool fprev = (word >> lane) & 1u;
+      const bool enter = track && ok && !fprev && fnow;
+      const bool leave = track && ok && fprev && !fnow;
+      const uint32_t newword = __ballot_sync(0xffffffffu, fnow);
+      if (!uncon && lane == 0 && wi * 32 < valid) c.fbits[t * (kTile / 32) + wi] = newword;
+      if (ok) {
+        if (fnow) {
+          cnt[0]++;
+          hash += mix64((unsigned long long)i);
+          const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
+          const R zi = uncon ? xi : gcp_point<R, S>(code, xi, gi, R(0), R(0), tsum);
+          // the history rows stay in the stage buffer (re-read, not held in registers)
+          S r = -(S)gi;
+          if (!uncon) {
+            r = -a1[kMaxM] * ((S)zi - (S)xi) - (S)gi;
+  #pragma unroll
+            for (int j = 0; j < kMaxM; j++)
+              if (kFull || j < col)
+                r = r + (S)hist_at<H>(buf, hy + j * hb, e) * a1[j] +
+                    (S)hist_at<H>(buf, hs + j * hb, e) * a2[j];
+          }
+  #pragma unroll
+          for (int j = 0; j < kMaxM; j++) {
+            if (kFull || j < col) {
+              acc[j] = fma(hist_at<H>(buf, hy + j * hb, e), (double)r, acc[j]);
+              acc[8 + j] = fma(hist_at<H>(buf, hs + j * hb, e), (double)r, acc[8 + j]);
+            }
+          }
+        } else {
+          if (code == IW_LOW || code == IW_WALK_LOW) cnt[3]++;
+          if (code == IW_UPP || code == IW_WALK_UPP) cnt[4]++;
         }
-#pragma unroll
-        for (int j = 0; j < kMaxM; j++) {
-          if (j < col) {
-            acc[j] = fma(hist_at<H>(buf, hy + j * hb, e), (double)r, acc[j]);
-            acc[8 + j] = fma(hist_at<H>(buf, hs + j * hb, e), (double)r, acc[8 + j]);
+        if (enter) cnt[1]++;
+        if (leave) cnt[2]++;
+      }
+      // entering (+) / leaving (-) variables: the whole warp adds the products of the
+      // variable's rows, each lane its kLaneOwned outputs
+      uint32_t pick = __ballot_sync(0xffffffffu, enter || leave);
+      while (pick) {
+        const int src = __ffs(pick) - 1;
+        pick &= pick - 1;
+        const double sign = __shfl_sync(0xffffffffu, enter ? 1.0 : -1.0, src);
+        // the source variable's y and s rows, read from the stage buffer by lanes 0..15
+        const int es = e - lane + src;
+        if (lane < kMaxM)
+          bc[warp][lane] = lane < col ? hist_at<H>(buf, hy + lane * hb, es) : 0.0;
+        else if (lane < 2 * kMaxM)
+          bc[warp][lane] = lane - kMaxM < col ? hist_at<H>(buf, hs + (lane - kMaxM) * hb, es) : 0.0;
+        __syncwarp();
+  #pragma unroll
+        for (int k = 0; k < kLaneOwned; k++) {
+          int kind, a, b;
+          corr_map(lane + 32 * k, kind, a, b);
+          if (kind < 3) {
+            const int oa = kind == 0 ? a : kMaxM + a;
+            const int ob = kind == 1 ? kMaxM + b : b;
+            double& cq = corr_sm[warp][32 * k + lane];
+            cq = fma(sign * bc[warp][oa], bc[warp][ob], cq);
           }
         }
-      } else {
-        if (code == IW_LOW || code == IW_WALK_LOW) cnt[3]++;
-        if (code == IW_UPP || code == IW_WALK_UPP) cnt[4]++;
+        __syncwarp();
       }
-      if (enter) cnt[1]++;
-      if (leave) cnt[2]++;
-    }
-    // entering (+) / leaving (-) variables: the whole warp adds the products of the
-    // variable's rows, each lane its kLaneOwned outputs
-    uint32_t pick = __ballot_sync(0xffffffffu, enter || leave);
-    while (pick) {
-      const int src = __ffs(pick) - 1;
-      pick &= pick - 1;
-      const double sign = __shfl_sync(0xffffffffu, enter ? 1.0 : -1.0, src);
-      // the source variable's y and s rows, read from the stage buffer by lanes 0..15
-      const int es = e - lane + src;
-      if (lane < kMaxM)
-        bc[warp][lane] = lane < col ? hist_at<H>(buf, hy + lane * hb, es) : 0.0;
-      else if (lane < 2 * kMaxM)
-        bc[warp][lane] = lane - kMaxM < col ? hist_at<H>(buf, hs + (lane - kMaxM) * hb, es) : 0.0;
-      __syncwarp();
-#pragma unroll
-      for (int k = 0; k < kLaneOwned; k++) {
-        int kind, a, b;
-        corr_map(lane + 32 * k, kind, a, b);
-        if (kind < 3) {
-          const int oa = kind == 0 ? a : kMaxM + a;
-          const int ob = kind == 1 ? kMaxM + b : b;
-          double& cq = corr_sm[warp][32 * k + lane];
-          cq = fma(sign * bc[warp][oa], bc[warp][ob], cq);
+    };
+    // roles 1 and 2: the new row's products over the free (role 1) or active (role 2) set
+    auto rowprod = [&](const unsigned char* buf, int valid, int e) {
+      if (e >= valid) return;
+      const int code = stage_at<int8_t>(buf, o_code, e);
+      const bool fnow = uncon || iw_free(code);
+      if (fnow != (role == 1)) return;
+      const double a = hist_at<H>(buf, (role == 1 ? hy : hs) + newest * hb, e);
+      const int o1 = role == 1 ? hy : hs;
+  #pragma unroll
+      for (int j = 0; j < kMaxM; j++) {
+        if (kFull || j < col) {
+          acc[j] = fma(a, hist_at<H>(buf, o1 + j * hb, e), acc[j]);
+          acc[8 + j] = role == 1 ? fma(hist_at<H>(buf, hs + j * hb, e), a, acc[8 + j])
+                                 : fma(a, hist_at<H>(buf, hy + j * hb, e), acc[8 + j]);
         }
       }
-      __syncwarp();
-    }
-  };
-  // roles 1 and 2: the new row's products over the free (role 1) or active (role 2) set
-  auto rowprod = [&](const unsigned char* buf, int valid, int e) {
-    if (e >= valid) return;
-    const int code = stage_at<int8_t>(buf, o_code, e);
-    const bool fnow = uncon || iw_free(code);
-    if (fnow != (role == 1)) return;
-    const double a = hist_at<H>(buf, (role == 1 ? hy : hs) + newest * hb, e);
-    const int o1 = role == 1 ? hy : hs;
-#pragma unroll
-    for (int j = 0; j < kMaxM; j++) {
-      if (j < col) {
-        acc[j] = fma(a, hist_at<H>(buf, o1 + j * hb, e), acc[j]);
-        acc[8 + j] = role == 1 ? fma(hist_at<H>(buf, hs + j * hb, e), a, acc[8 + j])
-                               : fma(a, hist_at<H>(buf, hy + j * hb, e), acc[8 + j]);
+    };
+    const bool need_row = updatd && col > 0;
+    run_stages<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
+                     &st->device_error, [&](const unsigned char* buf, long long t, int valid) {
+      if (role == 0) {
+  #pragma unroll
+        for (int h = 0; h < kTile / (32 * kRole0Warps); h++)
+          role0(buf, t, valid, rt + h * 32 * kRole0Warps);
+      } else if (need_row) {
+  #pragma unroll
+        for (int h = 0; h < kTile / (32 * kRole12Warps); h++)
+          rowprod(buf, valid, rt + h * 32 * kRole12Warps);
       }
-    }
-  };
-  const bool need_row = updatd && col > 0;
-  run_stages<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
-                   &st->device_error, [&](const unsigned char* buf, long long t, int valid) {
-    if (role == 0) {
-#pragma unroll
-      for (int h = 0; h < kTile / (32 * kRole0Warps); h++)
-        role0(buf, t, valid, rt + h * 32 * kRole0Warps);
-    } else if (need_row) {
-#pragma unroll
-      for (int h = 0; h < kTile / (32 * kRole12Warps); h++)
-        rowprod(buf, valid, rt + h * 32 * kRole12Warps);
-    }
+    });
   });
   // the free-set hash sums mod 2^64 (order free), one atomic per warp
 #pragma unroll
@@ -649,6 +671,7 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c, const R
     if (j == 0) a1[kMaxM] = theta;
   }
   MinPair mn[1] = {MinPair{INFINITY, kNoIndex}};
+  const FixedDiv<S> divt(theta);
 
   extern __shared__ __align__(128) unsigned char dyn[];
   __shared__ StreamSet ss;
@@ -669,48 +692,54 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c, const R
   const int o_u = ss.off[4], o_nb = ss.off[5];
   const int hy = s_hy, hs = s_hs, hb = kTile * (int)sizeof(H);
   const int cap = stage_capacity(StageBytes<R>::dir, 0, st->m, (int)sizeof(H));
-  run_tiles<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
-            &st->device_error, [&](const unsigned char* buf, long long t, int valid, int e) {
-    if (e >= valid) return;
-    const long long i = t * kTile + e;
-    const int code = stage_at<int8_t>(buf, o_code, e);
-    if (!(uncon || iw_free(code))) return;
-    S yv[kMaxM], sv[kMaxM];
-#pragma unroll
-    for (int j = 0; j < kMaxM; j++) {
-      yv[j] = (j < col) ? (S)hist_at<H>(buf, hy + j * hb, e) : S(0);
-      sv[j] = (j < col) ? (S)hist_at<H>(buf, hs + j * hb, e) : S(0);
-    }
-    const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
-    const R li = stage_at<R>(buf, o_l, e), ui = stage_at<R>(buf, o_u, e);
-    const R zi = uncon ? xi : gcp_point<R, S>(code, xi, gi, li, ui, tsum);
-    S d = reduced_grad<R, S>(uncon, xi, zi, gi, col, yv, sv, a1, a2);
-#pragma unroll
-    for (int j = 0; j < kMaxM; j++)
-      if (j < col) d = d + yv[j] * w1[j] / theta + sv[j] * w2[j];
-    d = d / theta;
-    const R dr = (R)d;
-    c.dsub[i] = dr;
-    // candidate step to the bound (1486-1516), filtered as for alpha = 1
-    const int nb = stage_at<int>(buf, o_nb, e);
-    const S dk = (S)dr;
-    if (nb != 0) {
-      double cand = INFINITY;
-      if (dk < S(0) && nb <= 2) {
-        const S temp2 = (S)li - (S)zi;
-        if (temp2 >= S(0))
-          cand = 0.0;
-        else if (dk * S(1) < temp2)
-          cand = (double)(temp2 / dk);
-      } else if (dk > S(0) && nb >= 2) {
-        const S temp2 = (S)ui - (S)zi;
-        if (temp2 <= S(0))
-          cand = 0.0;
-        else if (dk * S(1) > temp2)
-          cand = (double)(temp2 / dk);
+  dispatch_cols(col, [&](auto cols_tag) {
+    constexpr bool kFull = decltype(cols_tag)::value == kMaxM;
+    run_tiles<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
+              &st->device_error, [&](const unsigned char* buf, long long t, int valid, int e) {
+      if (e >= valid) return;
+      const long long i = t * kTile + e;
+      const int code = stage_at<int8_t>(buf, o_code, e);
+      if (!(uncon || iw_free(code))) return;
+      S yv[kMaxM], sv[kMaxM];
+  #pragma unroll
+      for (int j = 0; j < kMaxM; j++) {
+        yv[j] = (kFull || j < col) ? (S)hist_at<H>(buf, hy + j * hb, e) : S(0);
+        sv[j] = (kFull || j < col) ? (S)hist_at<H>(buf, hs + j * hb, e) : S(0);
       }
-      mn[0] = minpair(mn[0], MinPair{cand, i});
-    }
+      const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
+      const R li = stage_at<R>(buf, o_l, e), ui = stage_at<R>(buf, o_u, e);
+      const R zi = uncon ? xi : gcp_point<R, S>(code, xi, gi, li, ui, tsum);
+      S d = reduced_grad<R, S>(uncon, xi, zi, gi, kFull ? kMaxM : col, yv, sv, a1, a2);
+      // ... + wy*wv(jy)/theta + ws*wv(js), then d/theta (1472-1483): the divisions by the
+      // pass-constant theta use its reciprocal with Markstein's correction (FixedDiv), which
+      // rounds exactly like the division
+  #pragma unroll
+      for (int j = 0; j < kMaxM; j++)
+        if (kFull || j < col) d = d + divt(yv[j] * w1[j]) + sv[j] * w2[j];
+      d = divt(d);
+      const R dr = (R)d;
+      c.dsub[i] = dr;
+      // candidate step to the bound (1486-1516), filtered as for alpha = 1
+      const int nb = stage_at<int>(buf, o_nb, e);
+      const S dk = (S)dr;
+      if (nb != 0) {
+        double cand = INFINITY;
+        if (dk < S(0) && nb <= 2) {
+          const S temp2 = (S)li - (S)zi;
+          if (temp2 >= S(0))
+            cand = 0.0;
+          else if (dk * S(1) < temp2)
+            cand = (double)(temp2 / dk);
+        } else if (dk > S(0) && nb >= 2) {
+          const S temp2 = (S)ui - (S)zi;
+          if (temp2 <= S(0))
+            cand = 0.0;
+          else if (dk * S(1) > temp2)
+            cand = (double)(temp2 / dk);
+        }
+        mn[0] = minpair(mn[0], MinPair{cand, i});
+      }
+    });
   });
   constexpr int W = 2;
   double sdum[1] = {0.0}, xdum[1] = {0.0}, ldum[1] = {0.0};
@@ -916,41 +945,44 @@ __global__ void __launch_bounds__(CONS + 32) k_post_eval(Ctx<R, H, S> c, const R
   const int o_xt = xt_is_z ? o_z : ss.off[7];
   const int hy = s_hy, hs = s_hs, hb = kTile * (int)sizeof(H);
   const int cap = stage_capacity(StageBytes<R>::post, 0, st->m, (int)sizeof(H));
-  run_tiles<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
-            &st->device_error, [&](const unsigned char* buf, long long tt, int valid, int e) {
-    if (e >= valid) return;
-    const long long i = tt * kTile + e;
-    const R ti = stage_at<R>(buf, o_t, e), zi = stage_at<R>(buf, o_z, e);
-    const R xi = stage_at<R>(buf, o_xt, e), gi = stage_at<R>(buf, o_g, e);
-    const R gold = stage_at<R>(buf, o_go, e);
-    const R d = rsub(zi, ti);
-    s[0] = fma((double)gi, (double)d, s[0]);
-    // projgr (1389-1414)
-    const int nb = stage_at<int>(buf, o_nb, e);
-    R pg = gi;
-    if (nb != 0) {
-      if (gi < R(0)) {
-        if (nb >= 2) pg = smax<R>(rsub(xi, stage_at<R>(buf, o_u, e)), gi);
-      } else {
-        if (nb <= 2) pg = smin<R>(rsub(xi, stage_at<R>(buf, o_l, e)), gi);
+  dispatch_cols(col, [&](auto cols_tag) {
+    constexpr bool kFull = decltype(cols_tag)::value == kMaxM;
+    run_tiles<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
+              &st->device_error, [&](const unsigned char* buf, long long tt, int valid, int e) {
+      if (e >= valid) return;
+      const long long i = tt * kTile + e;
+      const R ti = stage_at<R>(buf, o_t, e), zi = stage_at<R>(buf, o_z, e);
+      const R xi = stage_at<R>(buf, o_xt, e), gi = stage_at<R>(buf, o_g, e);
+      const R gold = stage_at<R>(buf, o_go, e);
+      const R d = rsub(zi, ti);
+      s[0] = fma((double)gi, (double)d, s[0]);
+      // projgr (1389-1414)
+      const int nb = stage_at<int>(buf, o_nb, e);
+      R pg = gi;
+      if (nb != 0) {
+        if (gi < R(0)) {
+          if (nb >= 2) pg = smax<R>(rsub(xi, stage_at<R>(buf, o_u, e)), gi);
+        } else {
+          if (nb <= 2) pg = smin<R>(rsub(xi, stage_at<R>(buf, o_l, e)), gi);
+        }
       }
-    }
-    const double apg = fabs((double)pg);
-    xm[0] = (apg > xm[0]) ? apg : xm[0];
-    const R xd = rsub(ti, xi);
-    s[1] = fma((double)xd, (double)xd, s[1]);
-    const R y = rsub(gi, gold);
-    s[2] = fma((double)y, (double)y, s[2]);
-    const R sv = unit ? d : rmul(d, stp);
-#pragma unroll
-    for (int j = 0; j < kMaxM; j++) {
-      if (j < col) {
-        s[3 + j] = fma((double)sv, hist_at<H>(buf, hy + j * hb, e), s[3 + j]);
-        s[11 + j] = fma(hist_at<H>(buf, hs + j * hb, e), (double)sv, s[11 + j]);
+      const double apg = fabs((double)pg);
+      xm[0] = (apg > xm[0]) ? apg : xm[0];
+      const R xd = rsub(ti, xi);
+      s[1] = fma((double)xd, (double)xd, s[1]);
+      const R y = rsub(gi, gold);
+      s[2] = fma((double)y, (double)y, s[2]);
+      const R sv = unit ? d : rmul(d, stp);
+  #pragma unroll
+      for (int j = 0; j < kMaxM; j++) {
+        if (kFull || j < col) {
+          s[3 + j] = fma((double)sv, hist_at<H>(buf, hy + j * hb, e), s[3 + j]);
+          s[11 + j] = fma(hist_at<H>(buf, hs + j * hb, e), (double)sv, s[11 + j]);
+        }
       }
-    }
-    ssp[i] = HistTraits<H>::from((double)sv);
-    ysp[i] = HistTraits<H>::from((double)y);
+      ssp[i] = HistTraits<H>::from((double)sv);
+      ysp[i] = HistTraits<H>::from((double)y);
+    });
   });
   constexpr int W = NS + NX;
   MinPair mdum[1] = {MinPair{0.0, 0}};
