@@ -26,37 +26,16 @@ struct SynthCtx {
   double* fdev;
   double* fhost;        // pinned
   unsigned int* ticket;
-  int grid;
+  int grid[2];          // launch grid of the double / float kernel: one wave of CTAs
 };
 
-template <typename R>
-__device__ __forceinline__ R softplus_r(R z);
-template <>
-__device__ __forceinline__ double softplus_r(double z) {
-  return (z > 0 ? z : 0.0) + log1p(exp(-fabs(z)));
-}
-template <>
-__device__ __forceinline__ float softplus_r(float z) {
-  return (z > 0 ? z : 0.0f) + log1pf(expf(-fabsf(z)));
-}
-template <typename R>
-__device__ __forceinline__ R sigmoid_r(R z);
-template <>
-__device__ __forceinline__ double sigmoid_r(double z) {
-  if (z >= 0) return 1.0 / (1.0 + exp(-z));
-  const double e = exp(z);
-  return e / (1.0 + e);
-}
-template <>
-__device__ __forceinline__ float sigmoid_r(float z) {
-  if (z >= 0) return 1.0f / (1.0f + expf(-z));
-  const float e = expf(z);
-  return e / (1.0f + e);
-}
-__device__ __forceinline__ double rcos(double v) { return cos(v); }
-__device__ __forceinline__ float rcos(float v) { return cosf(v); }
-__device__ __forceinline__ double rsin(double v) { return sin(v); }
-__device__ __forceinline__ float rsin(float v) { return sinf(v); }
+// exp, log1p and sincos in the kernel's precision.
+__device__ __forceinline__ double rexp(double v) { return exp(v); }
+__device__ __forceinline__ float rexp(float v) { return expf(v); }
+__device__ __forceinline__ double rlog1p(double v) { return log1p(v); }
+__device__ __forceinline__ float rlog1p(float v) { return log1pf(v); }
+__device__ __forceinline__ void rsincos(double v, double* s, double* c) { sincos(v, s, c); }
+__device__ __forceinline__ void rsincos(float v, float* s, float* c) { sincosf(v, s, c); }
 
 template <typename R, typename F>
 __global__ void __launch_bounds__(kThreads) k_synth(int s, const R* __restrict__ x,
@@ -78,13 +57,19 @@ __global__ void __launch_bounds__(kThreads) k_synth(int s, const R* __restrict__
     const R de = xe - xk, dn = xn - xk;
     const R kk = (R)kap[k], wk = (R)w[k], bk = (R)b[k];
     const R z = xk - (R)tt[k];
-    const R term = R(0.5) * kk * (de * de + dn * dn) +
-                   h2 * (wk * softplus_r(z) - bk * xk + R(0.05) * rcos(R(3) * xk));
+    // softplus(z) = max(z, 0) + log1p(exp(-|z|)) and sigmoid(z) = (z >= 0 ? 1 : e) / (1 + e)
+    // share e = exp(-|z|); cos(3x) and sin(3x) share one sincos
+    const R e = rexp(-fabs(z));
+    const R softplus = (z > R(0) ? z : R(0)) + rlog1p(e);
+    const R sigmoid = (z >= R(0) ? R(1) : e) / (R(1) + e);
+    R s3, c3;
+    rsincos(R(3) * xk, &s3, &c3);
+    const R term = R(0.5) * kk * (de * de + dn * dn) + h2 * (wk * softplus - bk * xk + R(0.05) * c3);
     acc += (double)term;
     R gk = -kk * (de + dn);
     if (i > 0) gk += (R)kap[k - 1] * (xk - x[k - 1]);
     if (j > 0) gk += (R)kap[k - s] * (xk - x[k - s]);
-    gk += h2 * (wk * sigmoid_r(z) - bk - R(0.15) * rsin(R(3) * xk));
+    gk += h2 * (wk * sigmoid - bk - R(0.15) * s3);
     g[k] = gk;
   }
   double sarr[1] = {acc}, xd[1] = {0.0}, ld[1] = {0.0};
@@ -101,11 +86,11 @@ static int synth_eval(void* handle, R* x, R* f, R* g, void* stream) {
   SynthCtx* c = static_cast<SynthCtx*>(handle);
   cudaStream_t s = (cudaStream_t)stream;
   if (c->single) {
-    k_synth<R, float><<<c->grid, kThreads, 0, s>>>(
+    k_synth<R, float><<<c->grid[sizeof(R) == 8 ? 0 : 1], kThreads, 0, s>>>(
         c->s, x, (const float*)c->field[0], (const float*)c->field[1],
         (const float*)c->field[2], (const float*)c->field[3], g, c->part, c->ticket, c->fdev);
   } else {
-    k_synth<R, double><<<c->grid, kThreads, 0, s>>>(
+    k_synth<R, double><<<c->grid[sizeof(R) == 8 ? 0 : 1], kThreads, 0, s>>>(
         c->s, x, (const double*)c->field[0], (const double*)c->field[1],
         (const double*)c->field[2], (const double*)c->field[3], g, c->part, c->ticket,
         c->fdev);
@@ -147,9 +132,23 @@ void* lbfgsb_b200_synth_create(int s, const double* kappa, const double* w, cons
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  long long want = ((long long)n + kThreads - 1) / kThreads;
-  c->grid = (int)(want < (long long)sms * 4 ? want : (long long)sms * 4);
-  ok = ok && cudaMalloc(&c->part, (size_t)c->grid * sizeof(double)) == cudaSuccess;
+  const long long want = ((long long)n + kThreads - 1) / kThreads;
+  for (int r = 0; r < 2; r++) {
+    // one wave of resident CTAs; the grid-stride loop covers the rest
+    int per_sm = 1;
+    if (c->single)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &per_sm, r == 0 ? (const void*)k_synth<double, float> : (const void*)k_synth<float, float>,
+          kThreads, 0);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &per_sm, r == 0 ? (const void*)k_synth<double, double> : (const void*)k_synth<float, double>,
+          kThreads, 0);
+    if (per_sm < 1) per_sm = 1;
+    c->grid[r] = (int)(want < (long long)sms * per_sm ? want : (long long)sms * per_sm);
+  }
+  const int rows = c->grid[0] > c->grid[1] ? c->grid[0] : c->grid[1];
+  ok = ok && cudaMalloc(&c->part, (size_t)rows * sizeof(double)) == cudaSuccess;
   ok = ok && cudaMalloc(&c->fdev, sizeof(double)) == cudaSuccess;
   ok = ok && cudaMalloc(&c->ticket, sizeof(unsigned int)) == cudaSuccess;
   ok = ok && cudaMemset(c->ticket, 0, sizeof(unsigned int)) == cudaSuccess;
