@@ -78,8 +78,14 @@ class ClockSampler:
                  "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=self.fh, stderr=subprocess.DEVNULL)
+            # the timed work starts once the sampler has produced its first sample
+            t0 = time.time()
+            while time.time() - t0 < 5.0:
+                if os.path.getsize(self.path) > 0:
+                    break
+                time.sleep(0.02)
         except Exception:
             self.proc = None
         return self
@@ -294,7 +300,7 @@ def cpu_reference(side: int, dtype: str, warm: int, timed: int, budget_s: float 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--side", type=int, default=4096)
