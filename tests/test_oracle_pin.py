@@ -102,3 +102,44 @@ def test_long_tight_run_sensitivity():
         k += 1
     assert k >= 90
     assert worst > 1e-8
+
+
+def _config0(opt_over=None):
+    import synth
+    prob = synth.synth_problem(256, seed=0)
+    prob["kind"] = "synth"
+    opt = B.default_option(np.float64)
+    opt.eps_f = opt.eps_g = opt.eps_x = 1e-8
+    opt.max_iteration = 1000
+    return prob, opt
+
+
+@pytest.mark.skipif(not B.ref_available(), reason="reference build not present")
+def test_oracle_matches_live_reference_config0():
+    """The full config-0 solve (s = 256, FP64, eps 1e-8), oracle against the reference
+    build: every evaluation, every summary and the final x bit for bit."""
+    prob, opt = _config0()
+    a = B.run_cpu("ref", prob, np.float64, option=opt)
+    b = B.run_cpu("oracle", prob, np.float64, option=opt)
+    assert a.evals == b.evals
+    assert a.iters == b.iters
+    np.testing.assert_array_equal(a.x, b.x)
+    assert a.info == b.info
+
+
+def test_config0_sensitivity():
+    """The conditioning behind the GPU tolerance of the config-0 solve: moving x0 = 0 by
+    1e-19 keeps the oracle's discrete trace for at least 100 iterations, and the run then
+    stops on the f-test at a final f more than 1e-6 (relative) away."""
+    prob, opt = _config0()
+    a = B.run_cpu("oracle", prob, np.float64, option=opt, trace=True)
+    xp = 1e-19 * np.random.default_rng(1).standard_normal(prob["nbd"].size)
+    b = B.run_cpu("oracle", prob, np.float64, x0=xp, option=opt, trace=True)
+    k = 0
+    for ra, rb in zip(a.trace, b.trace):
+        if any(ra[key] != rb[key] for key in TRACE_KEYS):
+            break
+        k += 1
+    assert k >= 100
+    fa, fb = a.trace[-1]["f"], b.trace[-1]["f"]
+    assert abs(fa - fb) / abs(fa) > 1e-6
