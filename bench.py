@@ -238,14 +238,25 @@ def run_ours(args, rank: int, world: int, dist):
     so.close()
 
     # ---- gather over ranks (max time) ----
-    t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms, e2e_ms = float(t[0]), float(t[1])
+    ms, e2e_ms = max_over_ranks([ms, e2e_ms], dist, dev)
     return {"ms": ms, "kern": kern, "launches_k": launches_k, "evals_k": evals_k,
             "clocks": sampler.summary(), "e2e_ms": e2e_ms, "e2e_iters": summ2.num_iteration,
             "h2d": h2d, "d2h": d2h, "n": n,
             "model_bytes_iter": st_wk["bytes_per_iteration_model"]}
+
+
+def max_over_ranks(values, dist, device):
+    """Each value's maximum over the ranks (the job's time is its slowest rank's)."""
+    import torch
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t]
+
+
+def job_throughput(world: int, steps: int, ms: float) -> float:
+    """Whole-job iterations/s: every rank runs `steps` iterations of its own replica."""
+    return world * steps / (ms / 1000.0)
 
 
 def cpu_reference(side: int, dtype: str, warm: int, timed: int, budget_s: float = 60.0):
@@ -347,7 +358,7 @@ def main():
         import torch
         import torch.distributed as td
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = td
     try:
         r = run_ours(args, rank, world, dist)
@@ -358,7 +369,7 @@ def main():
     if rank != 0:
         return
     K = args.steps
-    value = world * K / (r["ms"] / 1000.0)
+    value = job_throughput(world, K, r["ms"])
     hbm, hbm_kind = peaks()
     kern = r["kern"]
     top = max(kern.items(), key=lambda kv: kv[1]["ms"]) if kern else None
@@ -393,7 +404,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": r["ms"] / K, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
         "config": config,
-        "e2e": {"value": world * e2e_iters / (r["e2e_ms"] / 1000.0), "unit": UNIT,
+        "e2e": {"value": job_throughput(world, e2e_iters, r["e2e_ms"]), "unit": UNIT,
                 "h2d_bytes_per_step": r["h2d"] / e2e_iters,
                 "d2h_bytes_per_step": r["d2h"] / e2e_iters},
         "gpu_launches": r["launches_k"],
