@@ -145,16 +145,30 @@ def _digest(a: np.ndarray) -> str:
     return hashlib.sha1(np.ascontiguousarray(a).tobytes()).hexdigest()[:16]
 
 
-def host_objective(prob: dict, dtype):
+def host_objective(prob: dict, dtype, source: str = "oracle"):
     """Host objective callback body for a problem dict: (xp, fp, gp) pointers -> fills f, g.
 
     prob["kind"] == "synth" (default): the grid objective of objective.c with fields
-    kappa, w, t, b; "quad": the separable quadratic with vectors a, c."""
-    lib = _load(ORACLE_SO)
+    kappa, w, t, b; "quad": the separable quadratic with vectors a, c; "dsscfg": the
+    steady-state combustion objective on an nx x ny grid with parameter lam, from
+    objective.c (source "oracle") or from the reference's own example code (source
+    "ref", the reference build)."""
     is64 = np.dtype(dtype) == np.float64
     real = C.c_double if is64 else C.c_float
     sfx = "f64" if is64 else "f32"
     kind = prob.get("kind", "synth")
+    if kind == "dsscfg":
+        lib = _load(ORACLE_SO if source == "oracle" else REF_SO)
+        fn = getattr(lib, f"{'orc' if source == 'oracle' else 'ref'}_dsscfg_eval_{sfx}")
+        fn.restype = None
+        fn.argtypes = [C.c_int, C.c_int, real] + [C.POINTER(real)] * 3
+        nx, ny, lam = int(prob["nx"]), int(prob["ny"]), float(prob["lam"])
+
+        def evaluate_dsscfg(xp, fp, gp):
+            fn(nx, ny, lam, xp, fp, gp)
+
+        return evaluate_dsscfg
+    lib = _load(ORACLE_SO)
     names = ("kappa", "w", "t", "b") if kind == "synth" else ("a", "c")
     arrs = [np.ascontiguousarray(prob[k], dtype=np.float64) for k in names]
     ptrs = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in arrs]
@@ -170,8 +184,35 @@ def host_objective(prob: dict, dtype):
     return evaluate_ptr
 
 
+def dsscfg_problem(nx: int, ny: int, lam: float = 1.0, bounds=None) -> dict:
+    """The reference example's problem: unbounded (nbd = 0, as dsscfg_main.cpp:66-80) or,
+    with bounds=(lo, hi), nbd = 2 everywhere."""
+    n = nx * ny
+    p = {"kind": "dsscfg", "nx": nx, "ny": ny, "lam": lam, "s": 0}
+    if bounds is None:
+        p.update(l=np.zeros(n), u=np.zeros(n), nbd=np.zeros(n, np.int32))
+    else:
+        p.update(l=np.full(n, float(bounds[0])), u=np.full(n, float(bounds[1])),
+                 nbd=np.full(n, 2, np.int32))
+    return p
+
+
+def dsscfg_start(prob: dict, dtype, source: str = "oracle") -> np.ndarray:
+    """The standard start point ('XS') of the dsscfg problem."""
+    is64 = np.dtype(dtype) == np.float64
+    real = C.c_double if is64 else C.c_float
+    lib = _load(ORACLE_SO if source == "oracle" else REF_SO)
+    fn = getattr(lib, f"{'orc' if source == 'oracle' else 'ref'}_dsscfg_start_{'f64' if is64 else 'f32'}")
+    fn.restype = None
+    fn.argtypes = [C.c_int, C.c_int, real, C.POINTER(real)]
+    x = np.zeros(int(prob["nx"]) * int(prob["ny"]), dtype=dtype)
+    fn(int(prob["nx"]), int(prob["ny"]), float(prob["lam"]), x.ctypes.data_as(C.POINTER(real)))
+    return x
+
+
 def run_cpu(which: str, prob: dict, dtype=np.float64, x0=None, option=None, record=True,
-            trace=False, custom_stop_at: int | None = None) -> RunResult:
+            trace=False, custom_stop_at: int | None = None,
+            objective_source: str = "oracle") -> RunResult:
     """Run the oracle ('oracle') or the reference build ('ref') on a synthetic problem."""
     dtype = np.dtype(dtype)
     is64 = dtype == np.float64
@@ -184,7 +225,7 @@ def run_cpu(which: str, prob: dict, dtype=np.float64, x0=None, option=None, reco
     u = np.ascontiguousarray(prob["u"], dtype=dtype)
     nbd = np.ascontiguousarray(prob["nbd"], dtype=np.int32)
     opt = option if option is not None else default_option(dtype)
-    ev = host_objective(prob, dtype)
+    ev = host_objective(prob, dtype, objective_source)
     res = RunResult(x=x, info=0, num_iteration=0, residual_g=0, residual_f=0, residual_x=0)
 
     def fg(user, xp, fp, gp, sp):

@@ -111,3 +111,117 @@ void orc_quad_eval_f32(int n, const double* a, const double* c, const float* x, 
   }
   *f = (float)acc;
 }
+
+/* ---- dsscfg: MINPACK-2 steady-state combustion (Averick, Carter, More, Xue, "The
+ * MINPACK-2 test problem collection", 1992), in the variant of the reference's example
+ * (examples/dsscfg/dsscfg_cpu.cpp:16-147): nx x ny nodes, k = nx*j + i, h = 1/(n+1),
+ * zero values outside the grid, two triangles per node (lower: the node, its right and
+ * top neighbours; upper: the node, its left and bottom neighbours),
+ *
+ *   f = area * (0.5 * sum dv^2 terms + fexp),  fexp = -lambda/3 * sum over triangles of
+ *   the exponentials of their three corners (trapezoidal rule), area = hx*hy/2.
+ *
+ * f sums the triangles in the reference's order (j, then i, lower then upper).  The
+ * gradient is gathered per node from the (up to) six triangles that touch it, added in
+ * the reference's order: own lower + own upper, then the triangles of the nodes above,
+ * right, left and below.  The f32 variant repeats the reference's float expressions
+ * including their promotions to double (the literals 3.0 and 0.5 are doubles there, and
+ * its unqualified exp of a float is the C library's double exp, rounded to float). */
+
+static float expd_f(float v) { return (float)exp((double)v); }
+
+void orc_dsscfg_start_f64(int nx, int ny, double lam, double* x) {
+  const double hx = 1.0 / (double)(nx + 1), hy = 1.0 / (double)(ny + 1);
+  const double c = lam / (lam + 1.0);
+  int i, j;
+  for (j = 0; j < ny; j++) {
+    const double ty = (double)(j < ny - j ? j : ny - j) * hy;
+    for (i = 0; i < nx; i++) {
+      const double tx = (double)(i < nx - i ? i : nx - i) * hx;
+      x[(long)nx * j + i] = c * sqrt(ty < tx ? ty : tx);
+    }
+  }
+}
+
+void orc_dsscfg_start_f32(int nx, int ny, float lam, float* x) {
+  const float hx = (float)(1.0 / (double)(float)(nx + 1));
+  const float hy = (float)(1.0 / (double)(float)(ny + 1));
+  const float c = (float)((double)lam / ((double)lam + 1.0));
+  int i, j;
+  for (j = 0; j < ny; j++) {
+    const float ty = (float)(j < ny - j ? j : ny - j) * hy;
+    for (i = 0; i < nx; i++) {
+      const float tx = (float)(i < nx - i ? i : nx - i) * hx;
+      x[(long)nx * j + i] = c * sqrtf(ty < tx ? ty : tx);
+    }
+  }
+}
+
+void orc_dsscfg_eval_f64(int nx, int ny, double lam, const double* x, double* f, double* g) {
+  const double hx = 1.0 / (double)(nx + 1), hy = 1.0 / (double)(ny + 1);
+  const double area = 0.5 * hx * hy;
+  double fquad = 0.0, fexp = 0.0;
+  int i, j;
+  for (j = 0; j < ny; j++) {
+    for (i = 0; i < nx; i++) {
+      const long k = (long)nx * j + i;
+      const double v = x[k];
+      const double vr = i < nx - 1 ? x[k + 1] : 0.0, vt = j < ny - 1 ? x[k + nx] : 0.0;
+      const double vl = i > 0 ? x[k - 1] : 0.0, vb = j > 0 ? x[k - nx] : 0.0;
+      double dx = (vr - v) / hx, dy = (vt - v) / hy;
+      fquad += dx * dx + dy * dy;
+      fexp = fexp - lam * (exp(v) + exp(vr) + exp(vt)) / 3.0;
+      dx = (v - vl) / hx;
+      dy = (v - vb) / hy;
+      fquad += dx * dx + dy * dy;
+      fexp = fexp - lam * (exp(vb) + exp(vl) + exp(v)) / 3.0;
+      if (g) {
+        const double e3 = lam * exp(v) / 3.0;
+        double gk = 0.0 + (-((vr - v) / hx) / hx - ((vt - v) / hy) / hy - e3);
+        gk = gk + (((v - vl) / hx) / hx + ((v - vb) / hy) / hy - e3);
+        const double above = j < ny - 1 ? -((vt - v) / hy) / hy - e3 : 0.0;
+        const double right = i < nx - 1 ? -((vr - v) / hx) / hx - e3 : 0.0;
+        const double left = i > 0 ? ((v - vl) / hx) / hx - e3 : 0.0;
+        const double below = j > 0 ? ((v - vb) / hy) / hy - e3 : 0.0;
+        g[k] = ((((gk + above) + right) + left) + below) * area;
+      }
+    }
+  }
+  *f = area * (0.5 * fquad + fexp);
+}
+
+void orc_dsscfg_eval_f32(int nx, int ny, float lam, const float* x, float* f, float* g) {
+  const float hx = (float)(1.0 / (double)(float)(nx + 1));
+  const float hy = (float)(1.0 / (double)(float)(ny + 1));
+  const float area = (float)(0.5 * (double)hx * (double)hy);
+  float fquad = 0.0f, fexp = 0.0f;
+  int i, j;
+  for (j = 0; j < ny; j++) {
+    for (i = 0; i < nx; i++) {
+      const long k = (long)nx * j + i;
+      const float v = x[k];
+      const float vr = i < nx - 1 ? x[k + 1] : 0.0f, vt = j < ny - 1 ? x[k + nx] : 0.0f;
+      const float vl = i > 0 ? x[k - 1] : 0.0f, vb = j > 0 ? x[k - nx] : 0.0f;
+      float dx = (vr - v) / hx, dy = (vt - v) / hy;
+      fquad += dx * dx + dy * dy;
+      fexp = (float)((double)fexp - (double)(lam * (expd_f(v) + expd_f(vr) + expd_f(vt))) / 3.0);
+      dx = (v - vl) / hx;
+      dy = (v - vb) / hy;
+      fquad += dx * dx + dy * dy;
+      fexp = (float)((double)fexp - (double)(lam * (expd_f(vb) + expd_f(vl) + expd_f(v))) / 3.0);
+      if (g) {
+        const double e3 = (double)(lam * expd_f(v)) / 3.0;
+        const float dxl = (vr - v) / hx, dyl = (vt - v) / hy;   /* own lower triangle */
+        const float dxu = (v - vl) / hx, dyu = (v - vb) / hy;   /* own upper triangle */
+        float gk = (float)(0.0 + ((double)(-dxl / hx - dyl / hy) - e3));
+        gk = (float)((double)gk + ((double)(dxu / hx + dyu / hy) - e3));
+        const float above = j < ny - 1 ? (float)((double)(-dyl / hy) - e3) : 0.0f;
+        const float right = i < nx - 1 ? (float)((double)(-dxl / hx) - e3) : 0.0f;
+        const float left = i > 0 ? (float)((double)(dxu / hx) - e3) : 0.0f;
+        const float below = j > 0 ? (float)((double)(dyu / hy) - e3) : 0.0f;
+        g[k] = ((((gk + above) + right) + left) + below) * area;
+      }
+    }
+  }
+  *f = (float)((double)area * (0.5 * (double)fquad + (double)fexp));
+}

@@ -96,6 +96,18 @@ void orc_synth_eval_f64(int s, const double* kappa, const double* w, const doubl
 void orc_synth_eval_f32(int s, const double* kappa, const double* w, const double* t,
                         const double* b, const float* x, float* f, float* g);
 
+/* dsscfg, the reference example's steady-state combustion objective (objective.c): start
+ * point and f, g on an nx x ny grid; g may be NULL.  The ref_ variants run the
+ * reference's own examples/dsscfg/dsscfg_cpu.cpp (in _ref/libref_lbfgsb.so only). */
+void orc_dsscfg_start_f64(int nx, int ny, double lam, double* x);
+void orc_dsscfg_start_f32(int nx, int ny, float lam, float* x);
+void orc_dsscfg_eval_f64(int nx, int ny, double lam, const double* x, double* f, double* g);
+void orc_dsscfg_eval_f32(int nx, int ny, float lam, const float* x, float* f, float* g);
+void ref_dsscfg_start_f64(int nx, int ny, double lam, double* x);
+void ref_dsscfg_start_f32(int nx, int ny, float lam, float* x);
+void ref_dsscfg_eval_f64(int nx, int ny, double lam, double* x, double* f, double* g);
+void ref_dsscfg_eval_f32(int nx, int ny, float lam, float* x, float* f, float* g);
+
 /* Separable quadratic sum_k 0.5*a_k*(x_k - c_k)^2 (objective.c), for ties and zero
  * gradients. */
 void orc_quad_eval_f64(int n, const double* a, const double* c, const double* x, double* f,

@@ -7,6 +7,7 @@
 #include <functional>
 
 #include "culbfgsb/lbfgsbcpu.h"
+#include "examples/dsscfg/dsscfg_cpu.h"
 #include "oracle_api.h"
 
 namespace {
@@ -85,4 +86,33 @@ extern "C" void ref_lbfgsb_minimize_f32(int n, float* x, const int* nbd, const f
                                         orc_cb_f32 custom_stop, void* user,
                                         orc_summary_f32* summary) {
   run<float>(n, x, nbd, l, u, opt, funcgrad, after_iter, custom_stop, user, summary);
+}
+
+// The reference's own dsscfg objective (examples/dsscfg/dsscfg_cpu.cpp), compiled from the
+// reference tree: task 'XS' writes the standard start point (and allocates work buffers,
+// freed here); 'FG' evaluates f and g with four n-vectors of work space.
+extern "C" void ref_dsscfg_start_f64(int nx, int ny, double lam, double* x) {
+  double* work = nullptr;
+  double fdum = 0;
+  dsscfg_cpu<double>(nx, ny, x, fdum, nullptr, &work, 'XS', lam);
+  delete[] work;
+}
+
+extern "C" void ref_dsscfg_start_f32(int nx, int ny, float lam, float* x) {
+  float* work = nullptr;
+  float fdum = 0;
+  dsscfg_cpu<float>(nx, ny, x, fdum, nullptr, &work, 'XS', lam);
+  delete[] work;
+}
+
+extern "C" void ref_dsscfg_eval_f64(int nx, int ny, double lam, double* x, double* f, double* g) {
+  double* work = new double[4 * (size_t)nx * ny];
+  dsscfg_cpu<double>(nx, ny, x, *f, g, &work, 'FG', lam);
+  delete[] work;
+}
+
+extern "C" void ref_dsscfg_eval_f32(int nx, int ny, float lam, float* x, float* f, float* g) {
+  float* work = new float[4 * (size_t)nx * ny];
+  dsscfg_cpu<float>(nx, ny, x, *f, g, &work, 'FG', lam);
+  delete[] work;
 }

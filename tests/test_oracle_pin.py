@@ -143,3 +143,69 @@ def test_config0_sensitivity():
     assert k >= 100
     fa, fb = a.trace[-1]["f"], b.trace[-1]["f"]
     assert abs(fa - fb) / abs(fa) > 1e-6
+
+
+# ---- dsscfg, the reference's own example objective ----------------------------------
+
+def _dsscfg_eval(prob, dtype, source, x):
+    import ctypes as C
+    real = C.c_double if dtype == np.float64 else C.c_float
+    f = real()
+    g = np.zeros(x.size, dtype)
+    xx = x.copy()
+    B.host_objective(prob, dtype, source)(xx.ctypes.data_as(C.POINTER(real)), C.byref(f),
+                                          g.ctypes.data_as(C.POINTER(real)))
+    return f.value, g
+
+
+@pytest.mark.skipif(not B.ref_available(), reason="reference build not present")
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_dsscfg_objective_matches_reference(dtype):
+    """oracle/objective.c's dsscfg against examples/dsscfg/dsscfg_cpu.cpp compiled from the
+    reference: the start point, f and every gradient entry bit for bit, on 60 random
+    points per grid (three grid shapes, values over four scales)."""
+    for nx, ny in ((7, 5), (31, 47), (64, 64)):
+        prob = B.dsscfg_problem(nx, ny, 1.0)
+        np.testing.assert_array_equal(B.dsscfg_start(prob, dtype, "oracle"),
+                                      B.dsscfg_start(prob, dtype, "ref"))
+        for trial in range(20):
+            rng = np.random.default_rng(100 + trial)
+            x = (rng.random(nx * ny) * [0.01, 0.3, 1.0, 3.0][trial % 4]).astype(dtype)
+            fa, ga = _dsscfg_eval(prob, dtype, "oracle", x)
+            fb, gb = _dsscfg_eval(prob, dtype, "ref", x)
+            assert fa == fb
+            np.testing.assert_array_equal(ga, gb)
+
+
+@pytest.mark.parametrize("nx,dtype,iters,evals,fmin", [
+    (64, np.float64, 163, 169, -0.990070631538),
+    (256, np.float64, 531, 550, -1.01129586297),
+    (256, np.float32, 333, 354, -1.01110565662)])
+def test_dsscfg_known_answers(nx, dtype, iters, evals, fmin):
+    """The reference's own runs of its dsscfg example (lambda = 1, unbounded, standard
+    start, eps 1e-8, 1000 iterations at most): iterations, evaluations and the smallest f
+    seen (printed to 12 digits), reproduced by the oracle."""
+    prob = B.dsscfg_problem(nx, nx, 1.0)
+    opt = B.default_option(dtype)
+    opt.eps_f = opt.eps_g = opt.eps_x = 1e-8
+    opt.max_iteration = 1000
+    r = B.run_cpu("oracle", prob, dtype, x0=B.dsscfg_start(prob, dtype), option=opt)
+    assert r.info == 1 and r.num_iteration == iters and len(r.evals) == evals
+    assert f"{min(e[0] for e in r.evals):.12g}" == f"{fmin:.12g}"
+
+
+@pytest.mark.skipif(not B.ref_available(), reason="reference build not present")
+@pytest.mark.parametrize("dtype,bounds", [(np.float64, None), (np.float32, None),
+                                          (np.float64, (0.0, 0.25)), (np.float32, (0.0, 0.25))])
+def test_dsscfg_solve_matches_reference(dtype, bounds):
+    """64 x 64 dsscfg solves, unbounded and with 0 <= x <= 0.25: the reference build with
+    its own objective against the oracle with objective.c, every evaluation bit for bit."""
+    prob = B.dsscfg_problem(64, 64, 1.0, bounds)
+    opt = B.default_option(dtype)
+    opt.eps_f = opt.eps_g = opt.eps_x = 1e-8
+    opt.max_iteration = 1000
+    x0 = B.dsscfg_start(prob, dtype, "ref")
+    a = B.run_cpu("ref", prob, dtype, x0=x0, option=opt, objective_source="ref")
+    b = B.run_cpu("oracle", prob, dtype, x0=x0, option=opt)
+    assert a.evals == b.evals and a.iters == b.iters and a.info == b.info
+    np.testing.assert_array_equal(a.x, b.x)
