@@ -195,6 +195,20 @@ int lbfgsb_b200_synth_funcgrad_f64(void* handle, double* x, double* f, double* g
 int lbfgsb_b200_synth_funcgrad_f32(void* handle, float* x, float* f, float* g, void* stream,
                                    const lbfgsb_b200_summary_f32* summary);
 
+/* ---- dsscfg objective (the reference example's objective, examples/dsscfg/dsscfg_cuda.cu)
+ * The MINPACK-2 steady-state combustion problem on an nx x ny grid with parameter lambda,
+ * as a device funcgrad callback: the handle is its `user` pointer; g is computed on the
+ * device, f in double (deterministic order) and returned after a stream synchronisation.
+ * _start writes the example's standard start point into the device vector x. */
+void* lbfgsb_b200_dsscfg_create(int nx, int ny, double lambda);
+void lbfgsb_b200_dsscfg_destroy(void* handle);
+int lbfgsb_b200_dsscfg_funcgrad_f64(void* handle, double* x, double* f, double* g, void* stream,
+                                    const lbfgsb_b200_summary_f64* summary);
+int lbfgsb_b200_dsscfg_funcgrad_f32(void* handle, float* x, float* f, float* g, void* stream,
+                                    const lbfgsb_b200_summary_f32* summary);
+int lbfgsb_b200_dsscfg_start_f64(void* handle, double* x, void* stream);
+int lbfgsb_b200_dsscfg_start_f32(void* handle, float* x, void* stream);
+
 /* Plain blocking copies for bindings without their own CUDA runtime (kind: 1 host to
  * device, 2 device to host, 3 device to device). */
 int lbfgsb_b200_copy(void* dst, const void* src, size_t bytes, int kind);

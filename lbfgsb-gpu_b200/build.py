@@ -17,7 +17,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "liblbfgsb_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", f) for f in ("driver.cu", "objective.cu", "noalloc.cu")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("driver.cu", "objective.cu", "dsscfg.cu", "noalloc.cu")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in
            ("common.cuh", "small.cuh", "state.cuh", "reduce.cuh", "tiles.cuh", "passes.cuh", "walk.cuh")]
 HEADERS.append(os.path.join(REPO, "include", "lbfgsb_b200.h"))

@@ -462,15 +462,20 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const
           hash += mix64((unsigned long long)i);
           const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
           const R zi = uncon ? xi : gcp_point<R, S>(code, xi, gi, R(0), R(0), tsum);
-          // the history rows stay in the stage buffer (re-read, not held in registers)
+          // cmprlb's r (842-867).  Here it only feeds the W'r reductions (the subspace
+          // pass recomputes r in the reference's operation order for the stored
+          // direction), so it is accumulated with fma in two independent chains.  The
+          // history rows stay in the stage buffer (re-read, not held in registers).
           S r = -(S)gi;
           if (!uncon) {
-            r = -a1[kMaxM] * ((S)zi - (S)xi) - (S)gi;
+            S ry = -a1[kMaxM] * ((S)zi - (S)xi) - (S)gi, rs = S(0);
   #pragma unroll
             for (int j = 0; j < kMaxM; j++)
-              if (kFull || j < col)
-                r = r + (S)hist_at<H>(buf, hy + j * hb, e) * a1[j] +
-                    (S)hist_at<H>(buf, hs + j * hb, e) * a2[j];
+              if (kFull || j < col) {
+                ry = fma((S)hist_at<H>(buf, hy + j * hb, e), a1[j], ry);
+                rs = fma((S)hist_at<H>(buf, hs + j * hb, e), a2[j], rs);
+              }
+            r = ry + rs;
           }
   #pragma unroll
           for (int j = 0; j < kMaxM; j++) {

@@ -87,7 +87,9 @@ EXPORTS = [
     "lbfgsb_b200_last_stats", "lbfgsb_b200_last_error", "lbfgsb_b200_synth_create",
     "lbfgsb_b200_synth_destroy", "lbfgsb_b200_synth_funcgrad_f64",
     "lbfgsb_b200_synth_funcgrad_f32", "lbfgsb_b200_copy", "lbfgsb_b200_projgr_noalloc_f64",
-    "lbfgsb_b200_trim_memory",
+    "lbfgsb_b200_trim_memory", "lbfgsb_b200_dsscfg_create", "lbfgsb_b200_dsscfg_destroy",
+    "lbfgsb_b200_dsscfg_funcgrad_f64", "lbfgsb_b200_dsscfg_funcgrad_f32",
+    "lbfgsb_b200_dsscfg_start_f64", "lbfgsb_b200_dsscfg_start_f32",
 ]
 
 _lib = None
@@ -126,6 +128,14 @@ def load() -> C.CDLL:
     lib.lbfgsb_b200_synth_destroy.argtypes = [C.c_void_p]
     lib.lbfgsb_b200_copy.restype = C.c_int
     lib.lbfgsb_b200_copy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
+    lib.lbfgsb_b200_dsscfg_create.restype = C.c_void_p
+    lib.lbfgsb_b200_dsscfg_create.argtypes = [C.c_int, C.c_int, C.c_double]
+    lib.lbfgsb_b200_dsscfg_destroy.restype = None
+    lib.lbfgsb_b200_dsscfg_destroy.argtypes = [C.c_void_p]
+    for sfx in ("f64", "f32"):
+        fn = getattr(lib, f"lbfgsb_b200_dsscfg_start_{sfx}")
+        fn.restype = C.c_int
+        fn.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     lib.lbfgsb_b200_projgr_noalloc_f64.restype = C.c_int
     lib.lbfgsb_b200_projgr_noalloc_f64.argtypes = [C.c_int] + [C.c_void_p] * 7
     _lib = lib
@@ -154,6 +164,31 @@ def last_stats() -> dict:
         out["kernels"][name] = {"launches": st.launches[k], "ms": st.ms[k],
                                 "bytes": st.bytes[k]}
     return out
+
+
+class DsscfgObjective:
+    """The device dsscfg objective of csrc/dsscfg.cu (the reference example's problem)."""
+
+    def __init__(self, nx: int, ny: int, lam: float = 1.0):
+        lib = load()
+        self.nx, self.ny = nx, ny
+        self.handle = lib.lbfgsb_b200_dsscfg_create(nx, ny, lam)
+        if not self.handle:
+            raise RuntimeError("lbfgsb_b200_dsscfg_create failed")
+        self.f64 = C.cast(lib.lbfgsb_b200_dsscfg_funcgrad_f64, C.c_void_p).value
+        self.f32 = C.cast(lib.lbfgsb_b200_dsscfg_funcgrad_f32, C.c_void_p).value
+
+    def start(self, x_dev_ptr: int, dtype=np.float64, stream=None) -> None:
+        lib = load()
+        fn = lib.lbfgsb_b200_dsscfg_start_f64 if np.dtype(dtype) == np.float64 else \
+            lib.lbfgsb_b200_dsscfg_start_f32
+        if fn(self.handle, x_dev_ptr, stream) != 0:
+            raise RuntimeError("lbfgsb_b200_dsscfg_start failed")
+
+    def close(self) -> None:
+        if self.handle:
+            load().lbfgsb_b200_dsscfg_destroy(self.handle)
+            self.handle = None
 
 
 class SynthObjective:

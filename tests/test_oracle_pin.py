@@ -209,3 +209,20 @@ def test_dsscfg_solve_matches_reference(dtype, bounds):
     b = B.run_cpu("oracle", prob, dtype, x0=x0, option=opt)
     assert a.evals == b.evals and a.iters == b.iters and a.info == b.info
     np.testing.assert_array_equal(a.x, b.x)
+
+
+def test_dsscfg_256_sensitivity():
+    """The conditioning behind the GPU bound on the 256 x 256 dsscfg solve: starting from
+    the standard x0 moved by 1e-15 relative, the oracle's smallest f differs from the
+    unperturbed run's by more than 5e-8 relative."""
+    prob = B.dsscfg_problem(256, 256)
+    x0 = B.dsscfg_start(prob, np.float64)
+    opt = B.default_option(np.float64)
+    opt.eps_f = opt.eps_g = opt.eps_x = 1e-8
+    opt.max_iteration = 1000
+    a = B.run_cpu("oracle", prob, np.float64, x0=x0, option=opt)
+    xp = x0 * (1 + 1e-15 * np.random.default_rng(1).standard_normal(x0.size))
+    b = B.run_cpu("oracle", prob, np.float64, x0=xp, option=opt)
+    fa = min(e[0] for e in a.evals)
+    fb = min(e[0] for e in b.evals)
+    assert abs(fa - fb) / abs(fa) > 5e-8
