@@ -19,6 +19,9 @@ ours:      W untimed iterations, then exactly K iterations timed with CUDA event
            the host-to-device copies of x0, l, u, nbd, the whole call (workspace, start
            point, K iterations) and the device-to-host copy of x inside the timed region.
            The objective's fields are the user's problem data and are uploaded before.
+dsscfg:    the reference's only published workload (its dsscfg example): our GPU path with
+           the device dsscfg objective against the reference's CPU path with its own
+           objective, at 256^2 FP64 and 2048^2 FP32, beside the published speedups.
 reference: the reference's own CPU L-BFGS-B (culbfgsb/lbfgsbcpu.cpp built into
            oracle/_ref/) on the same problem on the host, single thread (the reference has
            no threading), a bounded number of iterations.
@@ -245,6 +248,68 @@ def run_ours(args, rank: int, world: int, dist):
             "model_bytes_iter": st_wk["bytes_per_iteration_model"]}
 
 
+def dsscfg_compare():
+    """The reference's own published workload (its dsscfg example, README.md:23: GPU/CPU
+    speedup 10.15x at 256^2 FP64 and 36.86x at 2048^2 FP32, RTX 2080 Ti vs i9-9900K): our
+    GPU path with the device dsscfg objective (csrc/dsscfg.cu), whole solves from the
+    standard start (lambda = 1, unbounded, eps 1e-8, at most 1000 iterations), timed with
+    CUDA events around the call; against the reference's CPU path with its own dsscfg
+    objective (oracle/_ref), a bounded sample of iterations on one host core."""
+    import torch
+    import lbfgsb_b200 as LB
+    from oracle import binding as OB
+    lib = LB.load()
+    out = {"published_gpu_cpu_speedup": {"fp64_256": 10.15, "fp32_2048": 36.86,
+                                         "hardware": "RTX 2080 Ti vs i9-9900K",
+                                         "source": "README.md:23"}}
+    for key, nx, dt, cpu_iters in (("fp64_256", 256, np.float64, 60), ("fp32_2048", 2048, np.float32, 3)):
+        n = nx * nx
+        tdt = torch.float64 if dt == np.float64 else torch.float32
+        d = LB.DsscfgObjective(nx, nx)
+        x = torch.zeros(n, dtype=tdt, device="cuda")
+        zeros = torch.zeros(n, dtype=tdt, device="cuda")
+        nbd = torch.zeros(n, dtype=torch.int32, device="cuda")
+        fn = lib.lbfgsb_b200_minimize_f64 if dt == np.float64 else lib.lbfgsb_b200_minimize_f32
+        summ = LB.SummaryF64() if dt == np.float64 else LB.SummaryF32()
+
+        def solve(iters):
+            d.start(x.data_ptr(), dt)
+            o = LB.default_option(dt)
+            o.eps_f = o.eps_g = o.eps_x = 1e-8
+            o.max_iteration = iters
+            st = fn(n, x.data_ptr(), nbd.data_ptr(), zeros.data_ptr(), zeros.data_ptr(), C.byref(o),
+                    d.f64 if dt == np.float64 else d.f32, None, None, d.handle, None, C.byref(summ))
+            if st != 0:
+                raise RuntimeError(lib.lbfgsb_b200_last_error())
+
+        solve(5)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        solve(1000)
+        e1.record()
+        e1.synchronize()
+        gpu_s = e0.elapsed_time(e1) / 1000.0
+        gpu = {"iterations": summ.num_iteration, "info": summ.info,
+               "iters_per_s": summ.num_iteration / gpu_s, "seconds": gpu_s}
+        d.close()
+        cpu = None
+        if OB.ref_available():
+            prob = OB.dsscfg_problem(nx, nx)
+            x0 = OB.dsscfg_start(prob, dt, "ref")
+            o = OB.default_option(dt)
+            o.eps_f = o.eps_g = o.eps_x = 1e-8
+            o.max_iteration = cpu_iters
+            t0 = time.perf_counter()
+            r = OB.run_cpu("ref", prob, dt, x0=x0, option=o, objective_source="ref", record=False)
+            secs = time.perf_counter() - t0
+            cpu = {"iterations": r.num_iteration, "iters_per_s": r.num_iteration / secs,
+                   "sample": f"first {r.num_iteration} iterations of the same solve, 1 thread"}
+        out[key] = {"gpu": gpu, "cpu_reference": cpu,
+                    "speedup": (gpu["iters_per_s"] / cpu["iters_per_s"]) if cpu else None}
+    return out
+
+
 def max_over_ranks(values, dist, device):
     """Each value's maximum over the ranks (the job's time is its slowest rank's)."""
     import torch
@@ -398,6 +463,9 @@ def main():
             cpu = {"value": c["value"], "unit": UNIT, "cores": 1, "kind": "reference",
                    "sample": f"{c['iters']} iterations (after 1) of the same n={c['n']} problem, "
                              "reference lbfgsbcpu.cpp built from source, 1 thread"}
+    dss = None
+    if not args.no_cpu_baseline and world == 1:
+        dss = dsscfg_compare()
     e2e_iters = max(1, r["e2e_iters"])
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
@@ -415,6 +483,7 @@ def main():
         "evaluations_per_step": r["evals_k"] / K,
         "hbm_GBps_model": r["model_bytes_iter"] / (solver_ms / K / 1000.0) / 1e9 if solver_ms else None,
         "kernels": per_kernel,
+        "dsscfg": dss,
     }
     print(json.dumps(line))
 
