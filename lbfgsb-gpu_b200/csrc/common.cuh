@@ -89,6 +89,35 @@ struct FixedDiv32 {
     return __fmaf_rn(r, y, q);
   }
 };
+// Filter for arg-min reductions of quotients num/den (breakpoints, steps to a bound):
+// true when num/den certainly exceeds `best`, so that the correctly rounded quotient need
+// not be formed.  The estimate is num * y with y the hardware reciprocal refined by one
+// Newton step (relative error about 2^-44 in double, one float ulp in float), and the
+// test keeps a margin of 2^-20, far above it: a quotient within that margin of `best`,
+// or any operand outside [2^-100, 2^100] (where the flushed reciprocal could mislead), is
+// never filtered, and NaN estimates compare false.  A filtered candidate is strictly
+// larger than `best`, so it can change neither the minimum nor its (lowest) index.
+__device__ __forceinline__ double rcp_estimate(double b) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+  return y;
+}
+__device__ __forceinline__ float rcp_estimate(float b) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(b));
+  return y;
+}
+template <typename T>
+__device__ __forceinline__ bool quotient_exceeds(T num, T den, double best) {
+  const T ad = den < T(0) ? -den : den;
+  if (!(ad >= T(0x1p-100) && ad <= T(0x1p100))) return false;
+  T y = rcp_estimate(den);
+  const T e = fma(-den, y, T(1));
+  y = fma(y, e, y);
+  const double q = (double)(num * y);
+  return q > best + fabs(best) * 0x1p-20;
+}
+
 template <typename S>
 struct FixedDiv;
 template <>

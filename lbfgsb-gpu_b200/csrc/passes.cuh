@@ -141,14 +141,17 @@ __device__ __forceinline__ void dispatch_cols(int col, F&& f) {
 }
 
 // cauchy's per-variable classification (lbfgsbcpu.cpp:635-663) and breakpoint
-// (675-699).  Returns the iwhere code; sets has_bp/t for a movable variable with a
-// breakpoint.  The static codes -1 (nbd 0) and 3 (l == u) come from nbd, l, u, which is
-// what lbfgsbactive stored (467-515).
+// (675-699).  Returns the iwhere code; for a movable variable with a breakpoint sets
+// has_bp and the breakpoint as the quotient num/den (the reference's tl/(-g) or tu/g).
+// The static codes -1 (nbd 0) and 3 (l == u) come from nbd, l, u, which is what
+// lbfgsbactive stored (467-515).
 template <typename R>
-__device__ __forceinline__ int classify(R x, R g, R l, R u, int nb, bool& has_bp, R& t) {
+__device__ __forceinline__ int classify_q(R x, R g, R l, R u, int nb, bool& has_bp, R& num,
+                                          R& den) {
   const R neggi = -g;
   has_bp = false;
-  t = R(0);
+  num = R(0);
+  den = R(1);
   if (nb == 0) return IW_UNB;
   if (nb == 2 && rsub(u, l) <= R(0)) return IW_FIX;
   R tl = 0, tu = 0;
@@ -167,12 +170,22 @@ __device__ __forceinline__ int classify(R x, R g, R l, R u, int nb, bool& has_bp
   if (code == IW_FREE) {
     if (nb <= 2 && neggi < R(0)) {
       has_bp = true;
-      t = rdiv(tl, -neggi);
+      num = tl;
+      den = -neggi;
     } else if (nb >= 2 && neggi > R(0)) {
       has_bp = true;
-      t = rdiv(tu, neggi);
+      num = tu;
+      den = neggi;
     }
   }
+  return code;
+}
+// classify_q with the breakpoint t = num/den correctly rounded.
+template <typename R>
+__device__ __forceinline__ int classify(R x, R g, R l, R u, int nb, bool& has_bp, R& t) {
+  R num, den;
+  const int code = classify_q(x, g, l, u, nb, has_bp, num, den);
+  t = has_bp ? rdiv(num, den) : R(0);
   return code;
 }
 
@@ -249,8 +262,8 @@ __global__ void __launch_bounds__(CONS + 32) k_gcp_scan(Ctx<R, H, S> c, const R*
       const R li = stage_at<R>(buf, o_l, e), ui = stage_at<R>(buf, o_u, e);
       const int nb = stage_at<int>(buf, o_nb, e);
       bool has_bp;
-      R tb;
-      const int code = classify(xi, gi, li, ui, nb, has_bp, tb);
+      R tnum, tden;
+      const int code = classify_q(xi, gi, li, ui, nb, has_bp, tnum, tden);
       c.code[i] = (int8_t)code;
       if (code == IW_FREE || code == IW_UNB) {
         const double neggi = -(double)gi;
@@ -264,7 +277,9 @@ __global__ void __launch_bounds__(CONS + 32) k_gcp_scan(Ctx<R, H, S> c, const R*
         }
         if (has_bp) {
           s[17] += 1.0;
-          mn[0] = minpair(mn[0], MinPair{(double)tb, i});
+          // the smallest breakpoint: only candidates that can reach it are divided exactly
+          if (!quotient_exceeds(tnum, tden, mn[0].v))
+            mn[0] = minpair(mn[0], MinPair{(double)rdiv(tnum, tden), i});
         } else {
           s[18] += 1.0;
           if (neggi != 0.0) xm[0] = 1.0;
@@ -729,20 +744,25 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c, const R
       const S dk = (S)dr;
       if (nb != 0) {
         double cand = INFINITY;
+        bool skip = false;  // a candidate that cannot reach the running minimum
         if (dk < S(0) && nb <= 2) {
           const S temp2 = (S)li - (S)zi;
           if (temp2 >= S(0))
             cand = 0.0;
-          else if (dk * S(1) < temp2)
-            cand = (double)(temp2 / dk);
+          else if (dk * S(1) < temp2) {
+            skip = quotient_exceeds(temp2, dk, mn[0].v);
+            if (!skip) cand = (double)(temp2 / dk);
+          }
         } else if (dk > S(0) && nb >= 2) {
           const S temp2 = (S)ui - (S)zi;
           if (temp2 <= S(0))
             cand = 0.0;
-          else if (dk * S(1) > temp2)
-            cand = (double)(temp2 / dk);
+          else if (dk * S(1) > temp2) {
+            skip = quotient_exceeds(temp2, dk, mn[0].v);
+            if (!skip) cand = (double)(temp2 / dk);
+          }
         }
-        mn[0] = minpair(mn[0], MinPair{cand, i});
+        if (!skip) mn[0] = minpair(mn[0], MinPair{cand, i});
       }
     });
   });
@@ -828,20 +848,25 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_apply(Ctx<R, H, S> c, const
       const int nb = stage_at<int>(buf, o_nb, e);
       if (nb != 0) {
         double cand = INFINITY;
+        bool skip = false;  // a candidate that cannot reach the running minimum
         if (d < R(0) && nb <= 2) {
           const R a2 = rsub(li, xi);
           if (a2 >= R(0))
             cand = 0.0;
-          else if (rmul(d, big) < a2)
-            cand = (double)rdiv(a2, d);
+          else if (rmul(d, big) < a2) {
+            skip = quotient_exceeds(a2, d, mn[0].v);
+            if (!skip) cand = (double)rdiv(a2, d);
+          }
         } else if (d > R(0) && nb >= 2) {
           const R a2 = rsub(ui, xi);
           if (a2 <= R(0))
             cand = 0.0;
-          else if (rmul(d, big) > a2)
-            cand = (double)rdiv(a2, d);
+          else if (rmul(d, big) > a2) {
+            skip = quotient_exceeds(a2, d, mn[0].v);
+            if (!skip) cand = (double)rdiv(a2, d);
+          }
         }
-        mn[0] = minpair(mn[0], MinPair{cand, i});
+        if (!skip) mn[0] = minpair(mn[0], MinPair{cand, i});
       }
     }
   });

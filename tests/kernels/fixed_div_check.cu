@@ -1,6 +1,9 @@
 // Compares the fixed-divisor quotient of csrc/common.cuh (FixedDiv64 / FixedDiv32) with
 // CUDA's correctly rounded division (__ddiv_rn / __fdiv_rn) bit for bit on random and
-// constructed inputs.  Prints the number of mismatches per family and exits 1 if any.
+// constructed inputs, and checks that the arg-min filter quotient_exceeds(num, den, best)
+// never reports a quotient that is <= best (with best at, just below and just above the
+// correctly rounded quotient, and far from it).  Prints the number of mismatches /
+// violations per family and exits 1 if any.
 //   argv[1] = millions of random pairs per family (default 64)
 #include <cuda_runtime.h>
 
@@ -107,6 +110,38 @@ __global__ void k_check32(long long count, unsigned long long seed, unsigned lon
   }
 }
 
+template <typename T>
+__device__ T rand_real(unsigned long long& s, int elo, int ehi);
+template <>
+__device__ double rand_real<double>(unsigned long long& s, int elo, int ehi) { return rand_double(s, elo, ehi); }
+template <>
+__device__ float rand_real<float>(unsigned long long& s, int elo, int ehi) { return rand_float(s, elo, ehi); }
+
+// bad[0]: filtered although q <= best; bad[1]: number filtered (for information)
+template <typename T>
+__global__ void k_check_filter(long long count, unsigned long long seed, unsigned long long* bad) {
+  unsigned long long s = seed + 0x2468aceULL * (blockIdx.x * blockDim.x + threadIdx.x);
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < count;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int wide = (sizeof(T) == 8) ? 120 : 25;
+    const T num = rand_real<T>(s, -wide, wide);
+    const T den = rand_real<T>(s, -wide, wide);
+    const T q = num / den;  // correctly rounded
+    double best;
+    const int mode = (int)(k % 6);
+    if (mode == 0) best = (double)q;
+    else if (mode == 1) best = (double)q * (1.0 - 1e-12);
+    else if (mode == 2) best = (double)q * (1.0 + 1e-12);
+    else if (mode == 3) best = (double)q * 0.5;
+    else if (mode == 4) best = (double)q * 2.0;
+    else best = (double)q * (1.0 - 1e-6);
+    if (quotient_exceeds(num, den, best)) {
+      atomicAdd(&bad[1], 1ULL);
+      if (!((double)q > best)) atomicAdd(&bad[0], 1ULL);
+    }
+  }
+}
+
 int main(int argc, char** argv) {
   const long long count = (argc > 1 ? atoll(argv[1]) : 64) * 1000000LL;
   unsigned long long* bad = nullptr;
@@ -116,11 +151,19 @@ int main(int argc, char** argv) {
   k_check32<<<148 * 8, 256>>>(count, 2, bad + 5);
   unsigned long long h[10];
   if (cudaMemcpy(h, bad, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) return 2;
+  cudaMemset(bad, 0, 4 * sizeof(unsigned long long));
+  k_check_filter<double><<<148 * 8, 256>>>(count, 3, bad);
+  k_check_filter<float><<<148 * 8, 256>>>(count, 4, bad + 2);
+  unsigned long long hf[4];
+  if (cudaMemcpy(hf, bad, sizeof(hf), cudaMemcpyDeviceToHost) != cudaSuccess) return 2;
   cudaFree(bad);
+  printf("filter f64: %llu violations, %llu of %lld filtered\n", hf[0], hf[1], count);
+  printf("filter f32: %llu violations, %llu of %lld filtered\n", hf[2], hf[3], count);
   unsigned long long total = 0;
   for (int k = 0; k < 10; k++) {
     printf("%s family %d: %llu mismatches of %lld\n", k < 5 ? "f64" : "f32", k % 5, h[k], count / 5);
     total += h[k];
   }
+  total += hf[0] + hf[2];
   return total == 0 ? 0 : 1;
 }

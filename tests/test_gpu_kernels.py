@@ -4,7 +4,10 @@ FixedDiv (csrc/common.cuh) replaces a division by the pass-constant theta in the
 pass; it must round exactly like CUDA's correctly rounded division.  The check program
 (tests/kernels/fixed_div_check.cu) compares both bit for bit on 64 million random and
 constructed pairs per precision (quotients near representable values and near midpoints,
-divisors with all-ones mantissas, zeros, subnormals, infinities, NaNs).
+divisors with all-ones mantissas, zeros, subnormals, infinities, NaNs).  The same program
+checks the arg-min filter quotient_exceeds on 64 million random quotients per precision
+with the running minimum at, just below, just above and far from the quotient: it must
+never skip a quotient that could still be the minimum.
 """
 import os
 import subprocess
@@ -33,3 +36,4 @@ def test_fixed_divisor_quotient_rounds_like_division(tmp_path):
     run = subprocess.run([str(exe), "64"], capture_output=True, text=True, timeout=300)
     assert run.returncode == 0, run.stdout + run.stderr
     assert run.stdout.count("0 mismatches") == 10, run.stdout
+    assert run.stdout.count(": 0 violations") == 2, run.stdout
