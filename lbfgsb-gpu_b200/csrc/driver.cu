@@ -48,12 +48,13 @@ enum KernelId {
   KID_SUBAPPLY,
   KID_TRIAL,
   KID_POST,
+  KID_POSTGCP,
   KID_COUNT
 };
 static const char* kKernelNames[KID_COUNT] = {
     "k_init",      "k_projgr",    "k_begin_iteration", "k_gcp_scan",
     "k_walk_gather", "k_walk",    "k_freev_formk",     "k_subsm_dir",
-    "k_subsm_apply", "k_trial",   "k_post_eval"};
+    "k_subsm_apply", "k_trial",   "k_post_eval",       "k_post_gcp"};
 
 template <typename R>
 struct Api;
@@ -276,6 +277,7 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
   Workspace<R, H, S> w;
   w.s = stream;
   Launcher L(stream, profile);
+  bool fused = false;  // the post-evaluation pass runs the next Cauchy scan (k_post_gcp)
   long long syncs = 0, evals = 0;
   try {
     const size_t N = (size_t)n;
@@ -347,8 +349,11 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
                                      stage_capacity(StageBytes<R>::apply, 0, 0, hsz), n, kConsWide + 32);
     const PassCfg p_post = pass_cfg(k_post_eval<R, H, S, kConsWide>,
                                     stage_capacity(StageBytes<R>::post, 0, m, hsz), n, kConsWide + 32);
+    const PassCfg p_pgcp = pass_cfg(k_post_gcp<R, H, S, kConsWide>,
+                                    stage_capacity(StageBytes<R>::post, 0, m, hsz), n, kConsWide + 32);
     const int g_proj = grid_for(k_projgr<R, H, S>, n, kThreads);
-    const int g_max = std::max({p_gcp.grid, p_freev.grid, p_dir.grid, p_apply.grid, p_post.grid, g_proj});
+    const int g_max = std::max({p_gcp.grid, p_freev.grid, p_dir.grid, p_apply.grid, p_post.grid,
+                                p_pgcp.grid, g_proj});
     w.part = w.template alloc<double>((size_t)g_max * 256);
     c.part = w.part;
     const int g_elem = (int)std::min<long long>(((long long)n + 255) / 256, (long long)device_sms() * 8);
@@ -414,9 +419,16 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
       if (hs.sbgnrm <= (S)opt->eps_g) finish(4);
 
       int reset = 0;
+      // with bounds, the post-evaluation pass also runs the next iteration's Cauchy scan
+      // (k_post_gcp); spec: the last accepted step left that scan's result in the state
+      fused = cnstnd;
+      bool spec = false;
       DevState<S> snap;
       while (!finished) {
-        L.run(KID_BEGIN, [&] { k_begin_iteration<S><<<1, 1, 0, stream>>>(w.st, reset); });
+        const bool start_here = reset || !spec;
+        if (start_here)
+          L.run(KID_BEGIN, [&] { k_begin_iteration<S><<<1, 1, 0, stream>>>(w.st, reset); });
+        spec = false;
         const int reset_before = reset;
         reset = 0;
         const int col_now = reset_before ? 0 : hs.col;
@@ -435,7 +447,7 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
             k_subsm_apply<R, H, S, kConsWide><<<p_apply.grid, p_apply.threads, p_apply.smem, stream>>>(c, xcur, gcur, zb);
           });
         };
-        if (!uncon) {
+        if (!uncon && start_here) {
           L.run(KID_GCP, [&] {
             c.stages = p_gcp.stages;
             k_gcp_scan<R, H, S, kConsWide><<<p_gcp.grid, p_gcp.threads, p_gcp.smem, stream>>>(c, xcur, gcur);
@@ -478,6 +490,21 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
           reset = 1;
           continue;
         }
+        auto post = [&](R* xt_, R fval, int force) {
+          if (fused) {
+            L.run(KID_POSTGCP, [&] {
+              c.stages = p_pgcp.stages;
+              k_post_gcp<R, H, S, kConsWide><<<p_pgcp.grid, p_pgcp.threads, p_pgcp.smem, stream>>>(
+                  c, xcur, zb, xt_, gnew, gcur, (S)fval, force);
+            });
+          } else {
+            L.run(KID_POST, [&] {
+              c.stages = p_post.stages;
+              k_post_eval<R, H, S, kConsWide><<<p_post.grid, p_post.threads, p_post.smem, stream>>>(
+                  c, xcur, zb, xt_, gnew, gcur, (S)fval, force);
+            });
+          }
+        };
         // line search (347-358)
         R* xt = zb;
         bool quirk = false;
@@ -492,11 +519,7 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
           }
           funcgrad(user, xt, &f, gnew, (void*)stream, summary);
           evals++;
-          L.run(KID_POST, [&] {
-            c.stages = p_post.stages;
-            k_post_eval<R, H, S, kConsWide><<<p_post.grid, p_post.threads, p_post.smem, stream>>>(c, xcur, zb, xt, gnew,
-                                                                              gcur, (S)f, 0);
-          });
+          post(xt, f, 0);
           pull();
           if (hs.ls_task != 1) break;
           if (hs.iback >= 20) {
@@ -515,11 +538,7 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
             });
             xt = tb;
           }
-          L.run(KID_POST, [&] {
-            c.stages = p_post.stages;
-            k_post_eval<R, H, S, kConsWide><<<p_post.grid, p_post.threads, p_post.smem, stream>>>(c, xcur, zb, xt, gnew,
-                                                                              gcur, (S)f, 1);
-          });
+          post(xt, f, 1);
           pull();
         }
         if (xt == zb)
@@ -527,6 +546,7 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
         else
           std::swap(xcur, tb);
         std::swap(gcur, gnew);
+        spec = fused && hs.spec_gcp != 0;
         summary->num_iteration = hs.iter;
         if (trace) {
           lbfgsb_b200_trace_record rec;
@@ -621,13 +641,14 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
     st.bytes[KID_SUBDIR] = nn * (5 * Rb + hist + 5);
     st.bytes[KID_SUBAPPLY] = nn * (6 * Rb + 5);
     st.bytes[KID_POST] = nn * (6 * Rb + 4 + hist + 2 * Hb);
+    st.bytes[KID_POSTGCP] = nn * (6 * Rb + 4 + hist + 2 * Hb + 1);
     st.bytes[KID_TRIAL] = nn * 3 * Rb;
     st.bytes[KID_WALK_GATHER] = nn * (4 * Rb + 4);
     st.bytes[KID_PROJGR] = nn * (4 * Rb + 4);
     st.bytes[KID_INIT] = nn * (4 * Rb + 4);
-    st.bytes_per_iteration_model = st.bytes[KID_GCP] + st.bytes[KID_FREEV] +
-                                   st.bytes[KID_SUBDIR] + st.bytes[KID_SUBAPPLY] +
-                                   st.bytes[KID_POST];
+    st.bytes_per_iteration_model =
+        (fused ? st.bytes[KID_POSTGCP] : st.bytes[KID_POST] + st.bytes[KID_GCP]) +
+        st.bytes[KID_FREEV] + st.bytes[KID_SUBDIR] + st.bytes[KID_SUBAPPLY];
   } catch (const CudaFailure& e) {
     char buf[256];
     std::snprintf(buf, sizeof(buf), "%s failed at driver.cu:%d: %s", e.call, e.line,

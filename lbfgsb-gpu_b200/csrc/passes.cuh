@@ -217,6 +217,82 @@ __device__ __forceinline__ S reduced_grad(bool uncon, R x, R z, R g, int col,
   return r;
 }
 
+// cauchy's epilogue (lbfgsbcpu.cpp:702-733) and the first breakpoint test of the walk
+// (745-747), from the sums of the scan over the movable variables: red[0] sum g^2,
+// red[1..8] / red[9..16] the y / s parts of p = W'd by ring position, red[17] nbreak,
+// red[18] movable variables without a breakpoint, red[19] > 0 if one of them has g != 0,
+// red[20] / red[21] the smallest breakpoint and its index.
+template <typename S>
+__device__ void gcp_epilogue(DevState<S>* st, const double* red, int col, SmallWork<S>& sw) {
+  const S theta = st->theta;
+  const S f1 = -(S)red[0];
+  const int col2 = 2 * col;
+  for (int j = 1; j <= col; j++) {
+    st->p[j] = (S)red[j];
+    st->p[col + j] = (S)red[8 + j];
+  }
+  if (theta != S(1))
+    for (int j = col + 1; j <= col2; j++) st->p[j] *= theta;
+  st->nbreak = (int)red[17];
+  st->nfree_mov = (int)red[18];
+  st->bnded = red[19] > 0.0 ? 0 : 1;
+  st->internal_fail = 0;
+  if (st->nbreak == 0 && st->nfree_mov == 0) {
+    // xcp = x; c is left as it was (lbfgsbcpu.cpp:706-708), and cmprlb still applies the
+    // current middle matrix to it
+    st->gcp_state = GCP_EARLY;
+    st->tsum = 0;
+    if (col > 0) {
+      int info = 0;
+      sbmv(st->sy, st->wt, col, st->c, st->mc, &info, sw.work);
+      if (info != 0) st->internal_fail = -8;
+    }
+    return;
+  }
+  for (int j = 1; j <= col2; j++) st->c[j] = 0;
+  S f2 = -theta * f1;
+  const S f2org = f2;
+  if (col > 0) {
+    S* v = sw.v;
+    int info = 0;
+    sbmv(st->sy, st->wt, col, st->p, v, &info, sw.work);
+    if (info != 0) {
+      st->internal_fail = info;
+      return;
+    }
+    f2 = f2 - sdot(&v[1], 1, &st->p[1], 1, col2);
+  }
+  S dtm = -f1 / f2;
+  st->f1 = f1;
+  st->f2 = f2;
+  st->f1_0 = f1;
+  st->f2_0 = f2;
+  st->f2org = f2org;
+  st->tsum = 0;
+  st->tj = 0;
+  st->nint = 1;
+  st->nleft = st->nbreak;
+  if (st->nbreak != 0) {
+    st->bkmin = (S)red[20];
+    st->ibkmin = (int)red[21];
+    if (!(dtm < st->bkmin - S(0))) {
+      st->dtm = dtm;
+      st->gcp_state = GCP_WALK;  // at least one breakpoint is passed
+      return;
+    }
+  }
+  if (dtm <= S(0)) dtm = 0;
+  st->dtm = dtm;
+  st->tsum = st->tsum + dtm;
+  for (int j = 1; j <= col2; j++) st->c[j] += dtm * st->p[j];
+  if (col > 0) {
+    int info = 0;
+    sbmv(st->sy, st->wt, col, st->c, st->mc, &info, sw.work);  // cmprlb's M c (852)
+    if (info != 0) st->internal_fail = -8;
+  }
+  st->gcp_state = GCP_DONE;
+}
+
 // ------------------------------------------------------------------------------------
 // A: the Cauchy-point scan.
 template <typename R, typename H, typename S, int CONS>
@@ -296,74 +372,7 @@ __global__ void __launch_bounds__(CONS + 32) k_gcp_scan(Ctx<R, H, S> c, const R*
   __shared__ SmallWork<S> sw;
   if (threadIdx.x != 0) return;
 
-  // epilogue: lbfgsbcpu.cpp:702-733 and the first breakpoint test of the walk (745-747)
-  const S theta = st->theta;
-  const S f1 = -(S)red[0];
-  const int col2 = 2 * col;
-  for (int j = 1; j <= col; j++) {
-    st->p[j] = (S)red[j];
-    st->p[col + j] = (S)red[8 + j];
-  }
-  if (theta != S(1))
-    for (int j = col + 1; j <= col2; j++) st->p[j] *= theta;
-  st->nbreak = (int)red[17];
-  st->nfree_mov = (int)red[18];
-  st->bnded = red[19] > 0.0 ? 0 : 1;
-  st->internal_fail = 0;
-  if (st->nbreak == 0 && st->nfree_mov == 0) {
-    // xcp = x; c is left as it was (lbfgsbcpu.cpp:706-708), and cmprlb still applies the
-    // current middle matrix to it
-    st->gcp_state = GCP_EARLY;
-    st->tsum = 0;
-    if (col > 0) {
-      int info = 0;
-      sbmv(st->sy, st->wt, col, st->c, st->mc, &info, sw.work);
-      if (info != 0) st->internal_fail = -8;
-    }
-    return;
-  }
-  for (int j = 1; j <= col2; j++) st->c[j] = 0;
-  S f2 = -theta * f1;
-  const S f2org = f2;
-  if (col > 0) {
-    S* v = sw.v;
-    int info = 0;
-    sbmv(st->sy, st->wt, col, st->p, v, &info, sw.work);
-    if (info != 0) {
-      st->internal_fail = info;
-      return;
-    }
-    f2 = f2 - sdot(&v[1], 1, &st->p[1], 1, col2);
-  }
-  S dtm = -f1 / f2;
-  st->f1 = f1;
-  st->f2 = f2;
-  st->f1_0 = f1;
-  st->f2_0 = f2;
-  st->f2org = f2org;
-  st->tsum = 0;
-  st->tj = 0;
-  st->nint = 1;
-  st->nleft = st->nbreak;
-  if (st->nbreak != 0) {
-    st->bkmin = (S)red[NS + NX];
-    st->ibkmin = (int)red[NS + NX + 1];
-    if (!(dtm < st->bkmin - S(0))) {
-      st->dtm = dtm;
-      st->gcp_state = GCP_WALK;  // at least one breakpoint is passed
-      return;
-    }
-  }
-  if (dtm <= S(0)) dtm = 0;
-  st->dtm = dtm;
-  st->tsum = st->tsum + dtm;
-  for (int j = 1; j <= col2; j++) st->c[j] += dtm * st->p[j];
-  if (col > 0) {
-    int info = 0;
-    sbmv(st->sy, st->wt, col, st->c, st->mc, &info, sw.work);  // cmprlb's M c (852)
-    if (info != 0) st->internal_fail = -8;
-  }
-  st->gcp_state = GCP_DONE;
+  gcp_epilogue<S>(st, red, col, sw);
 }
 
 // ------------------------------------------------------------------------------------
@@ -930,6 +939,87 @@ __global__ void k_trial(int n, const R* __restrict__ t, const R* __restrict__ z,
   }
 }
 
+// The epilogue after a function evaluation: g'd and dcsrch (lbfgsbcpu.cpp:1312-1338); on
+// acceptance the stopping-test quantities (394-417) and matupd/formt (431-461, 1105-1133),
+// committing the spare slot that holds (s, y) to the ring.  red[0] g'd, red[1] |xold-x|^2,
+// red[2] y'y, red[3..10] s'y_j and red[11..18] s_j's by old ring position, red[19] the
+// projected-gradient norm.  Returns false while the line search goes on.
+template <typename S>
+__device__ bool post_epilogue(DevState<S>* st, const double* red, S f, int force_accept) {
+  st->f = f;
+  st->gd = (S)red[0];
+  if (!force_accept) {
+    // lnsrlb with task == 1 (1312-1338)
+    sdcsrch<S>(f, st->gd, st->stp, (S)1.0e-3, (S)0.9, (S)0.1, (S)0, st->stpmx, st->csave,
+               st->ls);
+    st->xstep = st->stp * st->dnrm;
+    if (st->csave != 4 && st->csave != 3) {
+      st->ls_task = 1;
+      st->ifun = st->ifun + 1;
+      st->nfgv = st->nfgv + 1;
+      st->iback = st->ifun - 1;
+      return false;
+    }
+    st->ls_task = 5;
+  }
+  // accepted: quantities of the stopping tests (394-417)
+  st->iter = st->iter + 1;
+  st->sbgnrm = (S)red[19];
+  st->tf = ssqrt((S)red[1]);
+  st->rr = (S)red[2];
+  // the update (431-461), carried out ahead of the host-side tests; if a test stops the
+  // solve the updated memory is simply discarded
+  S dr, ddum;
+  const S sstp = st->stp;
+  if (sstp == S(1)) {
+    dr = st->gd - st->gdold;
+    ddum = -st->gdold;
+  } else {
+    dr = (st->gd - st->gdold) * sstp;
+    ddum = -st->gdold * sstp;
+  }
+  st->dr = dr;
+  st->ddum_dr = ddum;
+  st->internal_fail = 0;
+  if ((double)dr <= 5e-16 * (double)ddum) {
+    st->updatd = 0;
+    return true;
+  }
+  st->updatd = 1;
+  st->iupdat = st->iupdat + 1;
+  const int m = st->m;
+  int shifted = 0;
+  if (st->iupdat <= m) {
+    st->col = st->iupdat;
+    st->itail = (st->head + st->iupdat - 2) % m + 1;
+  } else {
+    st->itail = st->itail % m + 1;
+    st->head = st->head % m + 1;
+    shifted = 1;
+  }
+  const int old = st->phys[st->itail];
+  st->phys[st->itail] = st->spare;
+  st->spare = old;
+  st->theta = st->rr / dr;
+  const int ncol = st->col;
+  constexpr int ld = kMaxM;
+  if (st->iupdat > m) {
+    for (int j = 1; j <= ncol - 1; j++) {
+      for (int i = 1; i <= j; i++) LB_AT(st->ss, ld, i, j) = LB_AT(st->ss, ld, i + 1, j + 1);
+      for (int i = j; i <= ncol - 1; i++) LB_AT(st->sy, ld, i, j) = LB_AT(st->sy, ld, i + 1, j + 1);
+    }
+  }
+  for (int j = 1; j <= ncol - 1; j++) {
+    LB_AT(st->sy, ld, ncol, j) = (S)red[3 + j - 1 + shifted];
+    LB_AT(st->ss, ld, j, ncol) = (S)red[11 + j - 1 + shifted];
+  }
+  LB_AT(st->ss, ld, ncol, ncol) = (sstp == S(1)) ? st->dtd : sstp * sstp * st->dtd;
+  LB_AT(st->sy, ld, ncol, ncol) = dr;
+  const int info = sformt<S>(st->wt, st->sy, st->ss, ncol, st->theta);
+  if (info != 0) st->internal_fail = info;
+  return true;
+}
+
 // ------------------------------------------------------------------------------------
 // E: after a function evaluation at xt (gradient gt; t and go are the point and the
 // gradient where the line search started).
@@ -1023,77 +1113,7 @@ __global__ void __launch_bounds__(CONS + 32) k_post_eval(Ctx<R, H, S> c, const R
   fold_rows<CONS + 32>(c.part, gridDim.x, W, NS, NX, 0, red);
   if (threadIdx.x != 0) return;
 
-  st->f = f;
-  st->gd = (S)red[0];
-  if (!force_accept) {
-    // lnsrlb with task == 1 (1312-1338)
-    sdcsrch<S>(f, st->gd, st->stp, (S)1.0e-3, (S)0.9, (S)0.1, (S)0, st->stpmx, st->csave,
-               st->ls);
-    st->xstep = st->stp * st->dnrm;
-    if (st->csave != 4 && st->csave != 3) {
-      st->ls_task = 1;
-      st->ifun = st->ifun + 1;
-      st->nfgv = st->nfgv + 1;
-      st->iback = st->ifun - 1;
-      return;
-    }
-    st->ls_task = 5;
-  }
-  // accepted: quantities of the stopping tests (394-417)
-  st->iter = st->iter + 1;
-  st->sbgnrm = (S)red[NS];
-  st->tf = ssqrt((S)red[1]);
-  st->rr = (S)red[2];
-  // the update (431-461), carried out ahead of the host-side tests; if a test stops the
-  // solve the updated memory is simply discarded
-  S dr, ddum;
-  const S sstp = st->stp;
-  if (sstp == S(1)) {
-    dr = st->gd - st->gdold;
-    ddum = -st->gdold;
-  } else {
-    dr = (st->gd - st->gdold) * sstp;
-    ddum = -st->gdold * sstp;
-  }
-  st->dr = dr;
-  st->ddum_dr = ddum;
-  st->internal_fail = 0;
-  if ((double)dr <= 5e-16 * (double)ddum) {
-    st->updatd = 0;
-    return;
-  }
-  st->updatd = 1;
-  st->iupdat = st->iupdat + 1;
-  const int m = st->m;
-  int shifted = 0;
-  if (st->iupdat <= m) {
-    st->col = st->iupdat;
-    st->itail = (st->head + st->iupdat - 2) % m + 1;
-  } else {
-    st->itail = st->itail % m + 1;
-    st->head = st->head % m + 1;
-    shifted = 1;
-  }
-  const int old = st->phys[st->itail];
-  st->phys[st->itail] = st->spare;
-  st->spare = old;
-  st->theta = st->rr / dr;
-  const int ncol = st->col;
-  constexpr int ld = kMaxM;
-  if (st->iupdat > m) {
-    for (int j = 1; j <= ncol - 1; j++) {
-      for (int i = 1; i <= j; i++) LB_AT(st->ss, ld, i, j) = LB_AT(st->ss, ld, i + 1, j + 1);
-      for (int i = j; i <= ncol - 1; i++) LB_AT(st->sy, ld, i, j) = LB_AT(st->sy, ld, i + 1, j + 1);
-    }
-  }
-  for (int j = 1; j <= ncol - 1; j++) {
-    LB_AT(st->sy, ld, ncol, j) = (S)red[3 + j - 1 + shifted];
-    LB_AT(st->ss, ld, j, ncol) = (S)red[11 + j - 1 + shifted];
-  }
-  LB_AT(st->ss, ld, ncol, ncol) = (sstp == S(1)) ? st->dtd : sstp * sstp * st->dtd;
-  LB_AT(st->sy, ld, ncol, ncol) = dr;
-  const int info = sformt<S>(st->wt, st->sy, st->ss, ncol, st->theta);
-  if (info != 0) st->internal_fail = info;
+  post_epilogue<S>(st, red, f, force_accept);
 }
 
 // ------------------------------------------------------------------------------------
@@ -1164,7 +1184,7 @@ __global__ void __launch_bounds__(kThreads) k_projgr(Ctx<R, H, S> c, const R* __
 // The memory reset of the reference driver (col = 0, head = 1, theta = 1, iupdat = 0,
 // updatd = false), and the branch flags of the next iteration.
 template <typename S>
-__global__ void k_begin_iteration(DevState<S>* st, int reset) {
+__device__ __forceinline__ void begin_state(DevState<S>* st, int reset) {
   if (reset) {
     st->col = 0;
     st->head = 1;
@@ -1184,6 +1204,265 @@ __global__ void k_begin_iteration(DevState<S>* st, int reset) {
     st->tsum = 0;
     st->nint = 0;
   }
+}
+
+template <typename S>
+__global__ void k_begin_iteration(DevState<S>* st, int reset) {
+  begin_state(st, reset);
+}
+
+
+// The value a history element holds once stored (the history precision H), as a double.
+template <typename H>
+__device__ __forceinline__ double stored_value(double v) {
+  const H h = HistTraits<H>::from(v);
+  if constexpr (sizeof(H) == 2) {
+    return (double)__bfloat162float(h);
+  } else {
+    return (double)h;
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// E+A: the post-evaluation pass fused with the next iteration's Cauchy-point scan, for
+// problems with bounds.  Two warp roles cover every tile:
+//   role P (consumer warps 0..7): k_post_eval's per-variable work (g'd, projgr, |dx|, y,
+//     the S'y / S's sums, the (s, y) write);
+//   role G (warps 8..15): cauchy's scan at the trial point xt with its gradient gt, as the
+//     next iteration will need it if the line search accepts xt: iwhere codes, breakpoints,
+//     and p = W'd summed over the old ring positions and over the new pair (s, y) in its
+//     stored precision, so that the epilogue can form p for whichever ring the update
+//     produces.
+// The epilogue runs the post-evaluation epilogue; when the step is accepted and the memory
+// update succeeded it starts the next iteration (the reference's loop top, 279-284) and
+// runs cauchy's epilogue on the reordered sums, and marks spec_gcp so that the host skips
+// the separate scan.  A rejected trial leaves codes that the next trial overwrites.
+template <typename R, typename H, typename S, int CONS>
+__global__ void __launch_bounds__(CONS + 32) k_post_gcp(Ctx<R, H, S> c, const R* __restrict__ t,
+                                                       const R* __restrict__ z,
+                                                       const R* __restrict__ xt,
+                                                       const R* __restrict__ gt,
+                                                       const R* __restrict__ go, S f,
+                                                       int force_accept) {
+  static_assert(CONS == 512, "the role split assumes 16 consumer warps");
+  DevState<S>* st = c.st;
+  const int n = c.n, col = st->col;
+  const R stp = (R)st->stp;
+  const bool unit = st->stp == S(1);
+  H* ysp = c.wy + (size_t)st->spare * (size_t)c.ld;
+  H* ssp = c.ws + (size_t)st->spare * (size_t)c.ld;
+  constexpr int kRoleWarps = 8, kRoleThreads = 32 * kRoleWarps;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int role = warp < kRoleWarps ? 0 : warp < 2 * kRoleWarps ? 1 : 2;  // 2: producer
+  const int rt = (int)threadIdx.x - (role == 1 ? kRoleThreads : 0);
+  // role P: acc[0] g'd, [1] |xold - x|^2, [2] y'y, [3..10] s'y_j, [11..18] s_j's;
+  //   xmx |proj g|.
+  // role G: acc[0] sum g^2 (movable), [1..8] / [9..16] y_j'(-g) / s_j'(-g) by old ring
+  //   position, [17] / [18] y'(-g) / s'(-g) of the new pair, [19] nbreak, [20] movable
+  //   without breakpoint; xmx: any of those with g != 0; mn: smallest breakpoint.
+  constexpr int NP = 19, NG = 21;
+  double acc[NG];
+#pragma unroll
+  for (int k = 0; k < NG; k++) acc[k] = 0.0;
+  double xmx = 0.0;
+  MinPair mn = MinPair{INFINITY, kNoIndex};
+
+  extern __shared__ __align__(128) unsigned char dyn[];
+  __shared__ StreamSet ss;
+  __shared__ int s_hy, s_hs;
+  const bool xt_is_z = xt == z;
+  if (threadIdx.x == 0) {
+    ss.count = 0;
+    ss.stage_bytes = 0;
+    add_stream(ss, t, kTile * (int)sizeof(R));
+    add_stream(ss, z, kTile * (int)sizeof(R));
+    add_stream(ss, gt, kTile * (int)sizeof(R));
+    add_stream(ss, go, kTile * (int)sizeof(R));
+    add_stream(ss, c.l, kTile * (int)sizeof(R));
+    add_stream(ss, c.u, kTile * (int)sizeof(R));
+    add_stream(ss, c.nbd, kTile * 4);
+    if (!xt_is_z) add_stream(ss, xt, kTile * (int)sizeof(R));
+    add_history(ss, c, st, s_hy, s_hs);
+  }
+  __syncthreads();
+  const int o_t = ss.off[0], o_z = ss.off[1], o_g = ss.off[2], o_go = ss.off[3];
+  const int o_l = ss.off[4], o_u = ss.off[5], o_nb = ss.off[6];
+  const int o_xt = xt_is_z ? o_z : ss.off[7];
+  const int hy = s_hy, hs = s_hs, hb = kTile * (int)sizeof(H);
+  const int cap = stage_capacity(StageBytes<R>::post, 0, st->m, (int)sizeof(H));
+  dispatch_cols(col, [&](auto cols_tag) {
+    constexpr bool kFull = decltype(cols_tag)::value == kMaxM;
+    auto post_elem = [&](const unsigned char* buf, long long tt, int valid, int e) {
+      if (e >= valid) return;
+      const long long i = tt * kTile + e;
+      const R ti = stage_at<R>(buf, o_t, e), zi = stage_at<R>(buf, o_z, e);
+      const R xi = stage_at<R>(buf, o_xt, e), gi = stage_at<R>(buf, o_g, e);
+      const R gold = stage_at<R>(buf, o_go, e);
+      const R d = rsub(zi, ti);
+      acc[0] = fma((double)gi, (double)d, acc[0]);
+      // projgr (1389-1414)
+      const int nb = stage_at<int>(buf, o_nb, e);
+      R pg = gi;
+      if (nb != 0) {
+        if (gi < R(0)) {
+          if (nb >= 2) pg = smax<R>(rsub(xi, stage_at<R>(buf, o_u, e)), gi);
+        } else {
+          if (nb <= 2) pg = smin<R>(rsub(xi, stage_at<R>(buf, o_l, e)), gi);
+        }
+      }
+      const double apg = fabs((double)pg);
+      xmx = (apg > xmx) ? apg : xmx;
+      const R xd = rsub(ti, xi);
+      acc[1] = fma((double)xd, (double)xd, acc[1]);
+      const R y = rsub(gi, gold);
+      acc[2] = fma((double)y, (double)y, acc[2]);
+      const R sv = unit ? d : rmul(d, stp);
+#pragma unroll
+      for (int j = 0; j < kMaxM; j++) {
+        if (kFull || j < col) {
+          acc[3 + j] = fma((double)sv, hist_at<H>(buf, hy + j * hb, e), acc[3 + j]);
+          acc[11 + j] = fma(hist_at<H>(buf, hs + j * hb, e), (double)sv, acc[11 + j]);
+        }
+      }
+      ssp[i] = HistTraits<H>::from((double)sv);
+      ysp[i] = HistTraits<H>::from((double)y);
+    };
+    auto gcp_elem = [&](const unsigned char* buf, long long tt, int valid, int e) {
+      if (e >= valid) return;
+      const long long i = tt * kTile + e;
+      const R xi = stage_at<R>(buf, o_xt, e), gi = stage_at<R>(buf, o_g, e);
+      const R li = stage_at<R>(buf, o_l, e), ui = stage_at<R>(buf, o_u, e);
+      const int nb = stage_at<int>(buf, o_nb, e);
+      bool has_bp;
+      R tnum, tden;
+      const int code = classify_q(xi, gi, li, ui, nb, has_bp, tnum, tden);
+      c.code[i] = (int8_t)code;
+      if (code == IW_FREE || code == IW_UNB) {
+        const double neggi = -(double)gi;
+        acc[0] = fma(neggi, neggi, acc[0]);
+#pragma unroll
+        for (int j = 0; j < kMaxM; j++) {
+          if (kFull || j < col) {
+            acc[1 + j] = fma(hist_at<H>(buf, hy + j * hb, e), neggi, acc[1 + j]);
+            acc[9 + j] = fma(hist_at<H>(buf, hs + j * hb, e), neggi, acc[9 + j]);
+          }
+        }
+        // the new pair as the ring will hold it
+        const R ti = stage_at<R>(buf, o_t, e), zi = stage_at<R>(buf, o_z, e);
+        const R d = rsub(zi, ti);
+        const R sv = unit ? d : rmul(d, stp);
+        const R y = rsub(gi, stage_at<R>(buf, o_go, e));
+        acc[17] = fma(stored_value<H>((double)y), neggi, acc[17]);
+        acc[18] = fma(stored_value<H>((double)sv), neggi, acc[18]);
+        if (has_bp) {
+          acc[19] += 1.0;
+          if (!quotient_exceeds(tnum, tden, mn.v))
+            mn = minpair(mn, MinPair{(double)rdiv(tnum, tden), i});
+        } else {
+          acc[20] += 1.0;
+          if (neggi != 0.0) xmx = 1.0;
+        }
+      }
+    };
+    run_stages<CONS>(ss, n, c.stages, dyn,
+                     reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap), &st->device_error,
+                     [&](const unsigned char* buf, long long tt, int valid) {
+      if (role == 0) {
+#pragma unroll
+        for (int h = 0; h < kTile / kRoleThreads; h++) post_elem(buf, tt, valid, rt + h * kRoleThreads);
+      } else {
+#pragma unroll
+        for (int h = 0; h < kTile / kRoleThreads; h++) gcp_elem(buf, tt, valid, rt + h * kRoleThreads);
+      }
+    });
+  });
+  // CTA row: [ role P sums (19) | role G sums (21) | role P max | role G max | min pair ]
+  constexpr int NS = NP + NG, W = NS + 2 + 2;
+  constexpr int kAllWarps = CONS / 32 + 1;
+  {
+    __shared__ double wsum[kAllWarps][W];
+    for (int k = lane; k < W; k += 32) wsum[warp][k] = 0.0;
+    __syncwarp();
+    const int off = role == 0 ? 0 : NP;
+    const int cnt = role == 0 ? NP : role == 1 ? NG : 0;
+#pragma unroll
+    for (int k = 0; k < NG; k++) {
+      const double v = warp_sum(acc[k]);
+      if (lane == 0 && k < cnt) wsum[warp][off + k] = v;
+    }
+    const double xv = warp_max(xmx);
+    const MinPair mv = warp_min(mn);
+    if (lane == 0) {
+      if (role < 2) wsum[warp][NS + role] = xv;
+      wsum[warp][NS + 2] = role == 1 ? mv.v : INFINITY;
+      wsum[warp][NS + 3] = role == 1 ? (double)mv.i : (double)kNoIndex;
+    }
+    __syncthreads();
+    double* row = c.part + (size_t)blockIdx.x * W;
+    for (int k = threadIdx.x; k < W; k += CONS + 32) {
+      if (k < NS) {
+        double a = 0.0;
+        for (int w = 0; w < kAllWarps; w++) a += wsum[w][k];
+        row[k] = a;
+      } else if (k < NS + 2) {
+        double a = 0.0;
+        for (int w = 0; w < kAllWarps; w++) a = wsum[w][k] > a ? wsum[w][k] : a;
+        row[k] = a;
+      } else if (k == NS + 2) {
+        MinPair a = MinPair{INFINITY, kNoIndex};
+        for (int w = 0; w < kAllWarps; w++)
+          a = minpair(a, MinPair{wsum[w][k], (long long)wsum[w][k + 1]});
+        row[k] = a.v;
+        row[k + 1] = (double)a.i;
+      }
+    }
+  }
+  if (!last_cta(c.ticket)) return;
+  __shared__ double red[W];
+  fold_rows<CONS + 32>(c.part, gridDim.x, W, NS, 2, 1, red);
+  __shared__ SmallWork<S> sw;
+  __shared__ double rp[NP + 1], rg[22];  // epilogue temporaries (shared, as all of them)
+  if (threadIdx.x != 0) return;
+
+  for (int k = 0; k < NP; k++) rp[k] = red[k];
+  rp[NP] = red[NS];
+  st->spec_gcp = 0;
+  const int col_old = col;
+  if (!post_epilogue<S>(st, rp, f, force_accept) || st->internal_fail != 0) return;
+  // the next iteration's loop top and cauchy epilogue (279-284, 702-747) at the accepted x
+  begin_state(st, 0);
+  if (st->uncon_branch) {
+    st->spec_gcp = 1;
+    return;
+  }
+  const double* g = red + NP;
+  const int ncol = st->col;
+  const int shifted = (st->updatd && st->iupdat > st->m) ? 1 : 0;
+  rg[0] = g[0];
+  for (int j = 1; j <= kMaxM; j++) {
+    rg[j] = 0.0;
+    rg[8 + j] = 0.0;
+  }
+  if (!st->updatd) {
+    for (int j = 1; j <= col_old; j++) {
+      rg[j] = g[j];
+      rg[8 + j] = g[8 + j];
+    }
+  } else {
+    for (int j = 1; j <= ncol - 1; j++) {
+      rg[j] = g[j + shifted];
+      rg[8 + j] = g[8 + j + shifted];
+    }
+    rg[ncol] = g[17];
+    rg[8 + ncol] = g[18];
+  }
+  rg[17] = g[19];
+  rg[18] = g[20];
+  rg[19] = red[NS + 1];
+  rg[20] = red[NS + 2];
+  rg[21] = red[NS + 3];
+  gcp_epilogue<S>(st, rg, ncol, sw);
+  st->spec_gcp = 1;
 }
 
 }  // namespace lbfgsb_b200

@@ -29,7 +29,7 @@ struct DevState {
   int device_error;    // 1 if a bounded wait of a staged-tile pipeline gave up
   int ibkmin, ibd;
   int nbreak, nleft, nfree_mov, nfree, nenter, nleave;
-  int pad0;
+  int spec_gcp;       // 1: the post-evaluation pass also ran the next Cauchy scan
   unsigned long long free_hash, free_hash_acc, at_lower, at_upper;
   S theta, f, fold, gd, gdold, stp, dnrm, dtd, xstep, stpmx;
   S sbgnrm, tf, rr, dr, ddum_dr;
