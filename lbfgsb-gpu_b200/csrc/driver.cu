@@ -440,7 +440,7 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
           });
           L.run(KID_SUBDIR, [&] {
             c.stages = p_dir.stages;
-            k_subsm_dir<R, H, S, kConsWide><<<p_dir.grid, p_dir.threads, p_dir.smem, stream>>>(c, xcur, gcur);
+            k_subsm_dir<R, H, S, kConsWide><<<p_dir.grid, p_dir.threads, p_dir.smem, stream>>>(c, xcur, gcur, zb);
           });
           L.run(KID_SUBAPPLY, [&] {
             c.stages = p_apply.stages;

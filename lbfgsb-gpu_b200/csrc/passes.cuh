@@ -632,6 +632,7 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const
   }
   st->free_hash = st->free_hash_acc;
   st->free_hash_acc = 0;
+  st->spec_apply = 0;  // set by the direction pass when it applies an untruncated step
   st->at_lower = (unsigned long long)red[19];
   st->at_upper = (unsigned long long)red[20];
   st->subsm_active = (st->nfree != 0 && col != 0) ? 1 : 0;
@@ -680,11 +681,86 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const
   for (int j = 1; j <= 2 * col; j++) st->wv[j] = wv[j];
 }
 
+// lnsrlb's per-variable start at the subspace point z (lbfgsbcpu.cpp:1263-1299): d = z - x,
+// d'd, g'd, and the step along d to the first bound (stpmx), filtered as for stpmx = 1e10;
+// candidates that cannot reach the running minimum skip the exact division.
+template <typename R>
+__device__ __forceinline__ void lnsrlb_elem(R zi, R xi, R gi, R li, R ui, int nb, bool want_stpmx,
+                                            long long i, double& dtd, double& gd, MinPair& mn) {
+  const R big = (R)1.0e10;
+  const R d = rsub(zi, xi);
+  dtd = fma((double)d, (double)d, dtd);
+  gd = fma((double)gi, (double)d, gd);
+  if (!want_stpmx || nb == 0) return;
+  double cand = INFINITY;
+  bool skip = false;  // a candidate that cannot reach the running minimum
+  if (d < R(0) && nb <= 2) {
+    const R a2 = rsub(li, xi);
+    if (a2 >= R(0))
+      cand = 0.0;
+    else if (rmul(d, big) < a2) {
+      skip = quotient_exceeds(a2, d, mn.v);
+      if (!skip) cand = (double)rdiv(a2, d);
+    }
+  } else if (d > R(0) && nb >= 2) {
+    const R a2 = rsub(ui, xi);
+    if (a2 <= R(0))
+      cand = 0.0;
+    else if (rmul(d, big) > a2) {
+      skip = quotient_exceeds(a2, d, mn.v);
+      if (!skip) cand = (double)rdiv(a2, d);
+    }
+  }
+  if (!skip) mn = minpair(mn, MinPair{cand, i});
+}
+
+// lnsrlb with task != 1 (1263-1311), then its first dcsrch call (1312-1338), from
+// red[0] d'd, red[1] g'd and red[2] the smallest step to a bound.
+template <typename S>
+__device__ void lnsrlb_start(DevState<S>* st, const double* red) {
+  const S sbig = (S)1.0e10;
+  st->dtd = (S)red[0];
+  st->dnrm = ssqrt(st->dtd);
+  st->stpmx = sbig;
+  if (st->cnstnd) {
+    if (st->iter == 0)
+      st->stpmx = 1;
+    else if ((S)red[2] < st->stpmx)
+      st->stpmx = (S)red[2];
+  }
+  if (st->iter == 0 && !st->boxed)
+    st->stp = smin((S)1 / st->dnrm, st->stpmx);
+  else
+    st->stp = 1;
+  st->fold = st->f;
+  st->ifun = 0;
+  st->iback = 0;
+  st->csave = 0;
+  st->gd = (S)red[1];
+  st->gdold = st->gd;
+  st->ls_info = 0;
+  if (st->gd >= S(0)) {
+    st->ls_info = -4;
+    return;
+  }
+  sdcsrch<S>(st->f, st->gd, st->stp, (S)1.0e-3, (S)0.9, (S)0.1, (S)0, st->stpmx, st->csave,
+             st->ls);
+  st->xstep = st->stp * st->dnrm;
+  if (st->csave != 4 && st->csave != 3) {
+    st->ls_task = 1;
+    st->ifun = st->ifun + 1;
+    st->nfgv = st->nfgv + 1;
+    st->iback = st->ifun - 1;
+  } else {
+    st->ls_task = 5;
+  }
+}
+
 // ------------------------------------------------------------------------------------
 // C: subspace direction on the free set and the step to the first bound it meets.
 template <typename R, typename H, typename S, int CONS>
 __global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c, const R* __restrict__ x,
-                                                        const R* __restrict__ g) {
+                                                        const R* __restrict__ g, R* __restrict__ z) {
   DevState<S>* st = c.st;
   if (st->gcp_state == GCP_WALK || st->internal_fail != 0 || !st->subsm_active) return;
   const int n = c.n, col = st->col;
@@ -699,7 +775,13 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c, const R
     w2[j] = (j < col) ? st->wv[col + 1 + j] : S(0);
     if (j == 0) a1[kMaxM] = theta;
   }
-  MinPair mn[1] = {MinPair{INFINITY, kNoIndex}};
+  // mn[0]: the step to the first bound (alpha); the speculative lnsrlb start at the
+  // untruncated step (alpha = 1): sums d'd, g'd and mn[1] the smallest step to a bound
+  MinPair mn[2] = {MinPair{INFINITY, kNoIndex}, MinPair{INFINITY, kNoIndex}};
+  double sl[2] = {0.0, 0.0};
+  const bool want_stpmx = st->cnstnd && st->iter > 0;
+  // speculate unless the last step was truncated (then this one likely is too)
+  const bool spec = st->dir_no_spec == 0;
   const FixedDiv<S> divt(theta);
 
   extern __shared__ __align__(128) unsigned char dyn[];
@@ -728,7 +810,17 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c, const R
       if (e >= valid) return;
       const long long i = t * kTile + e;
       const int code = stage_at<int8_t>(buf, o_code, e);
-      if (!(uncon || iw_free(code))) return;
+      if (!(uncon || iw_free(code))) {
+        if (!spec) return;
+        // an active variable: z is its Cauchy point
+        const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
+        const R li = stage_at<R>(buf, o_l, e), ui = stage_at<R>(buf, o_u, e);
+        const R zi = gcp_point<R, S>(code, xi, gi, li, ui, tsum);
+        z[i] = zi;
+        lnsrlb_elem<R>(zi, xi, gi, li, ui, stage_at<int>(buf, o_nb, e), want_stpmx, i, sl[0],
+                       sl[1], mn[1]);
+        return;
+      }
       S yv[kMaxM], sv[kMaxM];
   #pragma unroll
       for (int j = 0; j < kMaxM; j++) {
@@ -773,25 +865,42 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c, const R
         }
         if (!skip) mn[0] = minpair(mn[0], MinPair{cand, i});
       }
+      // the subspace step with alpha = 1 (1517-1533): z = xcp + d
+      if (spec) {
+        const R zs = (R)((S)zi + dk);
+        z[i] = zs;
+        lnsrlb_elem<R>(zs, xi, gi, li, ui, nb, want_stpmx, i, sl[0], sl[1], mn[1]);
+      }
     });
   });
-  constexpr int W = 2;
-  double sdum[1] = {0.0}, xdum[1] = {0.0}, ldum[1] = {0.0};
-  cta_reduce_to_row<CONS + 32, 0, 0, 1, 0>(sdum, xdum, mn, ldum, c.part, W);
+  // row: [ d'd, g'd | alpha candidate (value, index) | stpmx candidate (value, index) ]
+  constexpr int W = 6;
+  double xdum[1] = {0.0}, ldum[1] = {0.0};
+  cta_reduce_to_row<CONS + 32, 2, 0, 2, 0>(sl, xdum, mn, ldum, c.part, W);
   if (!last_cta(c.ticket)) return;
   __shared__ double red[W];
-  fold_rows<CONS + 32>(c.part, gridDim.x, W, 0, 0, 1, red);
+  __shared__ double rl[3];
+  fold_rows<CONS + 32>(c.part, gridDim.x, W, 2, 0, 2, red);
   if (threadIdx.x != 0) return;
-  const S cand = (S)red[0];
+  const S cand = (S)red[2];
   if (cand < S(1)) {
     st->alpha = cand;
-    st->ibd = (int)red[1];
+    st->ibd = (int)red[3];
     st->iword = 1;
-  } else {
-    st->alpha = 1;
-    st->ibd = -1;
-    st->iword = 0;
+    st->dir_no_spec = 1;
+    return;  // truncated: k_subsm_apply applies the step
   }
+  st->alpha = 1;
+  st->ibd = -1;
+  st->iword = 0;
+  st->dir_no_spec = 0;
+  if (!spec) return;  // k_subsm_apply applies the step
+  // not truncated: the step written above is the subspace point; start the line search
+  rl[0] = red[0];
+  rl[1] = red[1];
+  rl[2] = red[4];
+  lnsrlb_start<S>(st, rl);
+  st->spec_apply = 1;
 }
 
 // ------------------------------------------------------------------------------------
@@ -800,14 +909,13 @@ template <typename R, typename H, typename S, int CONS>
 __global__ void __launch_bounds__(CONS + 32) k_subsm_apply(Ctx<R, H, S> c, const R* __restrict__ x,
                                                           const R* __restrict__ g, R* __restrict__ z) {
   DevState<S>* st = c.st;
-  if (st->gcp_state == GCP_WALK || st->internal_fail != 0) return;
+  if (st->gcp_state == GCP_WALK || st->internal_fail != 0 || st->spec_apply) return;
   const int n = c.n;
   const bool uncon = st->uncon_branch != 0;
   const bool sub = st->subsm_active != 0;
   const S alpha = sub ? st->alpha : S(1), tsum = st->tsum;
   const long long ibd = sub ? st->ibd : -1;
   const bool want_stpmx = st->cnstnd && st->iter > 0;
-  const R big = (R)1.0e10;
   double s[2] = {0.0, 0.0};
   MinPair mn[1] = {MinPair{INFINITY, kNoIndex}};
 
@@ -850,34 +958,8 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_apply(Ctx<R, H, S> c, const
       zi = (R)((S)zi + alpha * dk);
     }
     z[i] = zi;
-    const R d = rsub(zi, xi);
-    s[0] = fma((double)d, (double)d, s[0]);
-    s[1] = fma((double)gi, (double)d, s[1]);
-    if (want_stpmx) {
-      const int nb = stage_at<int>(buf, o_nb, e);
-      if (nb != 0) {
-        double cand = INFINITY;
-        bool skip = false;  // a candidate that cannot reach the running minimum
-        if (d < R(0) && nb <= 2) {
-          const R a2 = rsub(li, xi);
-          if (a2 >= R(0))
-            cand = 0.0;
-          else if (rmul(d, big) < a2) {
-            skip = quotient_exceeds(a2, d, mn[0].v);
-            if (!skip) cand = (double)rdiv(a2, d);
-          }
-        } else if (d > R(0) && nb >= 2) {
-          const R a2 = rsub(ui, xi);
-          if (a2 <= R(0))
-            cand = 0.0;
-          else if (rmul(d, big) > a2) {
-            skip = quotient_exceeds(a2, d, mn[0].v);
-            if (!skip) cand = (double)rdiv(a2, d);
-          }
-        }
-        if (!skip) mn[0] = minpair(mn[0], MinPair{cand, i});
-      }
-    }
+    lnsrlb_elem<R>(zi, xi, gi, li, ui, want_stpmx ? stage_at<int>(buf, o_nb, e) : 0, want_stpmx, i,
+                   s[0], s[1], mn[0]);
   });
   constexpr int W = 4;
   double xdum[1] = {0.0}, ldum[1] = {0.0};
@@ -887,43 +969,7 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_apply(Ctx<R, H, S> c, const
   fold_rows<CONS + 32>(c.part, gridDim.x, W, 2, 0, 1, red);
   if (threadIdx.x != 0) return;
 
-  // lnsrlb with task != 1 (1263-1311), then its first dcsrch call (1312-1338)
-  const S sbig = (S)1.0e10;
-  st->dtd = (S)red[0];
-  st->dnrm = ssqrt(st->dtd);
-  st->stpmx = sbig;
-  if (st->cnstnd) {
-    if (st->iter == 0)
-      st->stpmx = 1;
-    else if ((S)red[2] < st->stpmx)
-      st->stpmx = (S)red[2];
-  }
-  if (st->iter == 0 && !st->boxed)
-    st->stp = smin((S)1 / st->dnrm, st->stpmx);
-  else
-    st->stp = 1;
-  st->fold = st->f;
-  st->ifun = 0;
-  st->iback = 0;
-  st->csave = 0;
-  st->gd = (S)red[1];
-  st->gdold = st->gd;
-  st->ls_info = 0;
-  if (st->gd >= S(0)) {
-    st->ls_info = -4;
-    return;
-  }
-  sdcsrch<S>(st->f, st->gd, st->stp, (S)1.0e-3, (S)0.9, (S)0.1, (S)0, st->stpmx, st->csave,
-             st->ls);
-  st->xstep = st->stp * st->dnrm;
-  if (st->csave != 4 && st->csave != 3) {
-    st->ls_task = 1;
-    st->ifun = st->ifun + 1;
-    st->nfgv = st->nfgv + 1;
-    st->iback = st->ifun - 1;
-  } else {
-    st->ls_task = 5;
-  }
+  lnsrlb_start<S>(st, red);
 }
 
 // Trial point x = stp*d + t with d = z - t (lbfgsbcpu.cpp:1332-1334).

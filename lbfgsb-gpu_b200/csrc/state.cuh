@@ -30,6 +30,8 @@ struct DevState {
   int ibkmin, ibd;
   int nbreak, nleft, nfree_mov, nfree, nenter, nleave;
   int spec_gcp;       // 1: the post-evaluation pass also ran the next Cauchy scan
+  int spec_apply;     // 1: the direction pass also applied the (untruncated) step
+  int dir_no_spec;    // 1 after a truncated step: the next direction pass does not try
   unsigned long long free_hash, free_hash_acc, at_lower, at_upper;
   S theta, f, fold, gd, gdold, stp, dnrm, dtd, xstep, stpmx;
   S sbgnrm, tf, rr, dr, ddum_dr;
