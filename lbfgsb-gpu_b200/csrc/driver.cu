@@ -279,6 +279,10 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
   Launcher L(stream, profile);
   bool fused = false;  // the post-evaluation pass runs the next Cauchy scan (k_post_gcp)
   long long syncs = 0, evals = 0;
+  // direction passes that wrote the speculative z, and those that also applied the step
+  // (k_subsm_apply then returned at once): for the per-launch byte counts of the stats
+  long long dir_spec = 0, dir_applied = 0;
+  int prev_no_spec = 0;
   try {
     const size_t N = (size_t)n;
     for (int k = 0; k < 3; k++) w.X[k] = w.template alloc<R>(N);
@@ -453,8 +457,16 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
             k_gcp_scan<R, H, S, kConsWide><<<p_gcp.grid, p_gcp.threads, p_gcp.smem, stream>>>(c, xcur, gcur);
           });
         }
+        auto count_dir = [&]() {
+          if (hs.subsm_active && hs.gcp_state != GCP_WALK && hs.internal_fail == 0) {
+            if (!prev_no_spec) dir_spec++;
+            if (hs.spec_apply) dir_applied++;
+            prev_no_spec = hs.dir_no_spec;
+          }
+        };
         subspace();
         pull();
+        count_dir();
         if (hs.gcp_state == GCP_WALK && hs.internal_fail == 0) {
           if (!c.wl_t) {
             w.wl_t = w.template alloc<double>(N);
@@ -471,6 +483,7 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
           L.run(KID_WALK, [&] { k_walk<R, H, S><<<1, kWalkThreads, 0, stream>>>(c, xcur, gcur); });
           subspace();
           pull();
+          count_dir();
         }
         if (hs.internal_fail != 0) {  // cauchy/formk/cmprlb/subsm failed: reset (297-341)
           reset = 1;
@@ -638,8 +651,14 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
     const double Rb = sizeof(R), Hb = sizeof(H), hist = 2.0 * m * Hb, nn = (double)n;
     st.bytes[KID_GCP] = nn * (4 * Rb + 4 + hist + 1);
     st.bytes[KID_FREEV] = nn * (2 * Rb + hist + 1 + 0.25);
-    st.bytes[KID_SUBDIR] = nn * (5 * Rb + hist + 5);
-    st.bytes[KID_SUBAPPLY] = nn * (6 * Rb + 5);
+    // per launch, averaged over the launches made: the direction pass writes z when it
+    // speculates; k_subsm_apply does its work only when the direction pass did not apply
+    // the step
+    const double ndir = std::max<double>(1.0, (double)g_last_stats.launches[KID_SUBDIR]);
+    const double napp = (double)g_last_stats.launches[KID_SUBAPPLY];
+    st.bytes[KID_SUBDIR] = nn * (5 * Rb + hist + 5 + Rb * (double)dir_spec / ndir);
+    st.bytes[KID_SUBAPPLY] =
+        napp > 0 ? nn * (6 * Rb + 5) * std::max(0.0, napp - (double)dir_applied) / napp : 0.0;
     st.bytes[KID_POST] = nn * (6 * Rb + 4 + hist + 2 * Hb);
     st.bytes[KID_POSTGCP] = nn * (6 * Rb + 4 + hist + 2 * Hb + 1);
     st.bytes[KID_TRIAL] = nn * 3 * Rb;
@@ -648,7 +667,7 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
     st.bytes[KID_INIT] = nn * (4 * Rb + 4);
     st.bytes_per_iteration_model =
         (fused ? st.bytes[KID_POSTGCP] : st.bytes[KID_POST] + st.bytes[KID_GCP]) +
-        st.bytes[KID_FREEV] + st.bytes[KID_SUBDIR] + st.bytes[KID_SUBAPPLY];
+        st.bytes[KID_FREEV] + st.bytes[KID_SUBDIR] + st.bytes[KID_SUBAPPLY];  // averaged
   } catch (const CudaFailure& e) {
     char buf[256];
     std::snprintf(buf, sizeof(buf), "%s failed at driver.cu:%d: %s", e.call, e.line,
