@@ -19,6 +19,8 @@ ours:      W untimed iterations, then exactly K iterations timed with CUDA event
            the host-to-device copies of x0, l, u, nbd, the whole call (workspace, start
            point, K iterations) and the device-to-host copy of x inside the timed region.
            The objective's fields are the user's problem data and are uploaded before.
+batched:   a 256-instance sample of the batched workload (FP32 solves of n from 1,024 to
+           262,144): solves/s one after another on one stream and side by side on 16.
 dsscfg:    the reference's only published workload (its dsscfg example): our GPU path with
            the device dsscfg objective against the reference's CPU path with its own
            objective, at 256^2 FP64 and 2048^2 FP32, beside the published speedups.
@@ -310,6 +312,61 @@ def dsscfg_compare():
     return out
 
 
+def batched_compare(count: int = 256, workers: int = 16):
+    """A seeded sample of the batched workload (independent FP32 solves of the synthetic
+    bounded grid problem, each with its own seed, grid side log-uniform in [32, 512], m = 8,
+    eps_g = 1e-6, at most 500 iterations, device objectives): the same instances solved one
+    after another on one stream, then side by side by lbfgsb_b200_minimize_batch_f32 with
+    `workers` streams.  Reports solves/s of both, per-solve p50/p99 wall time in the batched
+    run, and whether both runs give identical results."""
+    import torch
+    import lbfgsb_b200 as LB
+    import synth
+    rng = np.random.default_rng(3)
+    sides = np.rint(np.exp(rng.uniform(np.log(32), np.log(512), count))).astype(int)
+    probs = [synth.synth_problem(int(s), seed=100 + k) for k, s in enumerate(sides)]
+    objs = [LB.SynthObjective(p, single_precision_fields=True) for p in probs]
+    dev = [dict(l=torch.from_numpy(p["l"].astype(np.float32)).cuda(),
+                u=torch.from_numpy(p["u"].astype(np.float32)).cuda(),
+                nbd=torch.from_numpy(p["nbd"]).cuda()) for p in probs]
+    opt = LB.default_option(np.float32)
+    opt.eps_g = 1e-6
+    opt.max_iteration = 500
+    ns = [p["nbd"].size for p in probs]
+
+    def run(conc):
+        xs = [torch.zeros(n, dtype=torch.float32, device="cuda") for n in ns]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rc, stat, summ, secs = LB.solve_batch(ns, xs, [d["nbd"] for d in dev], [d["l"] for d in dev],
+                                              [d["u"] for d in dev], opt, objs[0].f32,
+                                              [o.handle for o in objs], concurrency=conc,
+                                              dtype=np.float32)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        if rc != 0:
+            raise RuntimeError(LB.load().lbfgsb_b200_last_error())
+        return wall, xs, summ, secs
+
+    run(workers)  # warm the pool and the module for every size
+    wall1, x1, s1, _ = run(1)
+    wallb, xb, sb, secs = run(workers)
+    same = all(torch.equal(a, b) for a, b in zip(x1, xb)) and \
+        all((a.info, a.num_iteration) == (b.info, b.num_iteration) for a, b in zip(s1, sb))
+    for o in objs:
+        o.close()
+    its = np.array([s.num_iteration for s in sb])
+    return {"instances": count, "workers": workers, "n_total": int(sum(ns)),
+            "n_range": [int(min(ns)), int(max(ns))],
+            "sequential_solves_per_s": count / wall1, "batched_solves_per_s": count / wallb,
+            "speedup": wall1 / wallb,
+            "p50_solve_s": float(np.percentile(secs, 50)), "p99_solve_s": float(np.percentile(secs, 99)),
+            "iterations_mean": float(its.mean()), "iterations_max": int(its.max()),
+            "identical_results": bool(same),
+            "note": "a 256-instance sample of the 4096-instance workload; one worker stream per "
+                    "host thread, whole solves overlapped"}
+
+
 def max_over_ranks(values, dist, device):
     """Each value's maximum over the ranks (the job's time is its slowest rank's)."""
     import torch
@@ -464,8 +521,10 @@ def main():
                    "sample": f"{c['iters']} iterations (after 1) of the same n={c['n']} problem, "
                              "reference lbfgsbcpu.cpp built from source, 1 thread"}
     dss = None
+    batched = None
     if not args.no_cpu_baseline and world == 1:
         dss = dsscfg_compare()
+        batched = batched_compare()
     e2e_iters = max(1, r["e2e_iters"])
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
@@ -484,6 +543,7 @@ def main():
         "hbm_GBps_model": r["model_bytes_iter"] / (solver_ms / K / 1000.0) / 1e9 if solver_ms else None,
         "kernels": per_kernel,
         "dsscfg": dss,
+        "batched": batched,
     }
     print(json.dumps(line))
 

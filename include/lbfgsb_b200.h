@@ -114,6 +114,28 @@ int lbfgsb_b200_minimize_f32(int n, float* x, const int* nbd, const float* l, co
 
 /* ---- extensions (no counterpart in the reference) ---------------------------------- */
 
+/* Batched independent solves (the reference solves one problem per call): `count`
+ * instances of possibly different sizes n[k], each with its own device arrays x[k] (in /
+ * out), nbd[k], l[k], u[k] and funcgrad user pointer user[k], one option set for all.
+ * `concurrency` host workers (0: 16), each on its own non-blocking stream on the calling
+ * thread's device, run the plain solve on instances in turn, so small solves overlap on
+ * the GPU; funcgrad is called from those workers (at most one call per instance at a
+ * time).  Instance k's summary, x and status equal what its solo lbfgsb_b200_minimize
+ * call gives.  status[k]: its return code; seconds[k] (may be NULL): its wall time. */
+int lbfgsb_b200_minimize_batch_f64(int count, const int* n, double* const* x,
+                                   const int* const* nbd, const double* const* l,
+                                   const double* const* u, const lbfgsb_b200_option_f64* option,
+                                   lbfgsb_b200_callback_f64 funcgrad, void* const* user,
+                                   int concurrency, lbfgsb_b200_summary_f64* summary,
+                                   int* status, double* seconds);
+int lbfgsb_b200_minimize_batch_f32(int count, const int* n, float* const* x,
+                                   const int* const* nbd, const float* const* l,
+                                   const float* const* u, const lbfgsb_b200_option_f32* option,
+                                   lbfgsb_b200_callback_f32 funcgrad, void* const* user,
+                                   int concurrency, lbfgsb_b200_summary_f32* summary,
+                                   int* status, double* seconds);
+
+
 /* One record per accepted iteration, mirroring the CPU oracle's trace: the state the step
  * was computed from (col, head, theta, Cauchy-point and free-set statistics) and the
  * line-search outcome. */

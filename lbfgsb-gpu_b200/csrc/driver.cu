@@ -10,10 +10,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/lbfgsb_b200.h"
@@ -224,13 +227,26 @@ template <typename K>
 static PassCfg pass_cfg(K kernel, int cap, long long n, int threads) {
   PassCfg p;
   p.threads = threads;
-  p.stages = std::max(2, std::min(kMaxStages, kRingBudget / cap));
+  // a CTA never has more tiles in flight than it processes: small problems take fewer
+  // stages, which leaves room for other streams' CTAs on the same SM
+  const long long tiles = (n + kTile - 1) / kTile;
+  const long long per_cta = (tiles + device_sms() - 1) / device_sms();
+  p.stages = std::max(2, std::min<int>(std::min(kMaxStages, kRingBudget / cap), (int)per_cta + 1));
   p.smem = ring_bytes(p.stages, cap);
-  CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, p.smem));
+  // the attribute is per kernel and process-wide, while solves of different sizes may run
+  // concurrently on other threads: it is always set to the full opt-in allowance (the same
+  // value from every thread), and each launch asks only for its own ring
+  int dev = 0, optin = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa;
+  CK(cudaFuncGetAttributes(&fa, kernel));
+  const int allowance = optin - (int)fa.sharedSizeBytes;
+  if (p.smem > allowance) throw CudaFailure{cudaErrorInvalidValue, "stage ring exceeds shared memory", __LINE__};
+  CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, allowance));
   int per_sm = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, p.smem));
   per_sm = std::max(per_sm, 1);
-  const long long tiles = (n + kTile - 1) / kTile;
   p.grid = (int)std::max<long long>(1, std::min<long long>(tiles, (long long)device_sms() * per_sm));
   return p;
 }
@@ -689,6 +705,71 @@ static void default_option(Opt* o, R meps, R mmax) {
   o->step_scaling = (R)1.0;
 }
 
+// Independent solves side by side: `concurrency` host workers, each with its own
+// non-blocking stream on the caller's device, take instances in order and run the plain
+// solve on them; instance k's result is the one its solo solve gives (the solve is
+// deterministic and its workspace private).  status[k] gets the instance's return code
+// and seconds[k] (optional) its wall time; the return value is the first failing code.
+template <typename R>
+static int minimize_batch(int count, const int* n, R* const* x, const int* const* nbd,
+                          const R* const* l, const R* const* u,
+                          const typename Api<R>::Opt* option, typename Api<R>::Cb funcgrad,
+                          void* const* user, int concurrency, typename Api<R>::Sum* summary,
+                          int* status, double* seconds) {
+  g_last_error.clear();
+  if (count < 0 || (count > 0 && (!n || !x || !nbd || !l || !u || !option || !funcgrad ||
+                                  !summary || !status))) {
+    g_last_error = "minimize_batch: null argument";
+    return LBFGSB_B200_ERR_ARGUMENT;
+  }
+  if (count == 0) return LBFGSB_B200_OK;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    g_last_error = cudaGetErrorString(e);
+    return LBFGSB_B200_ERR_CUDA;
+  }
+  const int workers = std::max(1, std::min(concurrency > 0 ? concurrency : 16, count));
+  std::atomic<int> next{0};
+  std::mutex mu;
+  std::string first_error;
+  int first_status = LBFGSB_B200_OK;
+  auto work = [&]() {
+    cudaStream_t s = nullptr;
+    if (cudaSetDevice(dev) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+      std::lock_guard<std::mutex> lock(mu);
+      if (first_status == LBFGSB_B200_OK) {
+        first_status = LBFGSB_B200_ERR_CUDA;
+        first_error = "minimize_batch: worker stream set-up failed";
+      }
+      return;
+    }
+    for (int k = next++; k < count; k = next++) {
+      const auto t0 = std::chrono::steady_clock::now();
+      const int st = solve<R, R, R>(n[k], x[k], nbd[k], l[k], u[k], option, funcgrad, nullptr,
+                                    nullptr, user ? user[k] : nullptr, s, nullptr, &summary[k]);
+      status[k] = st;
+      if (seconds)
+        seconds[k] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      if (st != LBFGSB_B200_OK) {
+        std::lock_guard<std::mutex> lock(mu);
+        if (first_status == LBFGSB_B200_OK) {
+          first_status = st;
+          first_error = g_last_error;
+        }
+      }
+    }
+    cudaStreamDestroy(s);
+  };
+  for (int k = 0; k < count; k++) status[k] = -1;
+  std::vector<std::thread> pool;
+  for (int w = 0; w < workers; w++) pool.emplace_back(work);
+  for (auto& t : pool) t.join();
+  if (first_status != LBFGSB_B200_OK) g_last_error = first_error;
+  return first_status;
+}
+
 }  // namespace lbfgsb_b200
 
 using namespace lbfgsb_b200;
@@ -752,6 +833,26 @@ int lbfgsb_b200_minimize_f32(int n, float* x, const int* nbd, const float* l, co
                              void* stream, lbfgsb_b200_summary_f32* summary) {
   return lbfgsb_b200_minimize_ext_f32(n, x, nbd, l, u, option, funcgrad, after_iteration,
                                       customized_stopping, user, stream, nullptr, summary);
+}
+
+int lbfgsb_b200_minimize_batch_f64(int count, const int* n, double* const* x,
+                                   const int* const* nbd, const double* const* l,
+                                   const double* const* u, const lbfgsb_b200_option_f64* option,
+                                   lbfgsb_b200_callback_f64 funcgrad, void* const* user,
+                                   int concurrency, lbfgsb_b200_summary_f64* summary,
+                                   int* status, double* seconds) {
+  return lbfgsb_b200::minimize_batch<double>(count, n, x, nbd, l, u, option, funcgrad, user,
+                                             concurrency, summary, status, seconds);
+}
+
+int lbfgsb_b200_minimize_batch_f32(int count, const int* n, float* const* x,
+                                   const int* const* nbd, const float* const* l,
+                                   const float* const* u, const lbfgsb_b200_option_f32* option,
+                                   lbfgsb_b200_callback_f32 funcgrad, void* const* user,
+                                   int concurrency, lbfgsb_b200_summary_f32* summary,
+                                   int* status, double* seconds) {
+  return lbfgsb_b200::minimize_batch<float>(count, n, x, nbd, l, u, option, funcgrad, user,
+                                            concurrency, summary, status, seconds);
 }
 
 int lbfgsb_b200_last_stats(lbfgsb_b200_stats* out) {

@@ -90,6 +90,7 @@ EXPORTS = [
     "lbfgsb_b200_trim_memory", "lbfgsb_b200_dsscfg_create", "lbfgsb_b200_dsscfg_destroy",
     "lbfgsb_b200_dsscfg_funcgrad_f64", "lbfgsb_b200_dsscfg_funcgrad_f32",
     "lbfgsb_b200_dsscfg_start_f64", "lbfgsb_b200_dsscfg_start_f32",
+    "lbfgsb_b200_minimize_batch_f64", "lbfgsb_b200_minimize_batch_f32",
 ]
 
 _lib = None
@@ -128,6 +129,12 @@ def load() -> C.CDLL:
     lib.lbfgsb_b200_synth_destroy.argtypes = [C.c_void_p]
     lib.lbfgsb_b200_copy.restype = C.c_int
     lib.lbfgsb_b200_copy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
+    for sfx, opt, summ in (("f64", OptionF64, SummaryF64), ("f32", OptionF32, SummaryF32)):
+        fn = getattr(lib, f"lbfgsb_b200_minimize_batch_{sfx}")
+        fn.restype = C.c_int
+        fn.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                       C.POINTER(opt), C.c_void_p, C.c_void_p, C.c_int, C.POINTER(summ),
+                       C.c_void_p, C.c_void_p]
     lib.lbfgsb_b200_dsscfg_create.restype = C.c_void_p
     lib.lbfgsb_b200_dsscfg_create.argtypes = [C.c_int, C.c_int, C.c_double]
     lib.lbfgsb_b200_dsscfg_destroy.restype = None
@@ -164,6 +171,24 @@ def last_stats() -> dict:
         out["kernels"][name] = {"launches": st.launches[k], "ms": st.ms[k],
                                 "bytes": st.bytes[k]}
     return out
+
+
+def solve_batch(ns, xs, nbds, ls, us, option, funcgrad, users, concurrency=16, dtype=np.float64):
+    """lbfgsb_b200_minimize_batch over device tensors (lists of torch tensors); returns
+    (status, per-instance statuses, summaries, seconds)."""
+    lib = load()
+    k = len(ns)
+    is64 = np.dtype(dtype) == np.float64
+    ptrs = lambda ts: (C.c_void_p * k)(*[t.data_ptr() for t in ts])  # noqa: E731
+    n_arr = (C.c_int * k)(*ns)
+    summ = ((SummaryF64 if is64 else SummaryF32) * k)()
+    stat = (C.c_int * k)()
+    secs = (C.c_double * k)()
+    us_arr = (C.c_void_p * k)(*users)
+    fn = lib.lbfgsb_b200_minimize_batch_f64 if is64 else lib.lbfgsb_b200_minimize_batch_f32
+    rc = fn(k, n_arr, ptrs(xs), ptrs(nbds), ptrs(ls), ptrs(us), C.byref(option), funcgrad,
+            us_arr, concurrency, summ, stat, secs)
+    return rc, list(stat), list(summ), list(secs)
 
 
 class DsscfgObjective:
