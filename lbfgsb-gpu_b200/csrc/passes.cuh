@@ -370,9 +370,10 @@ __global__ void __launch_bounds__(CONS + 32) k_gcp_scan(Ctx<R, H, S> c, const R*
   __shared__ double red[W];
   fold_rows<CONS + 32>(c.part, gridDim.x, W, NS, NX, NM, red);
   __shared__ SmallWork<S> sw;
-  if (threadIdx.x != 0) return;
+  epilogue_on_shared<S>(st, [&](DevState<S>* st) {
 
-  gcp_epilogue<S>(st, red, col, sw);
+    gcp_epilogue<S>(st, red, col, sw);
+  });
 }
 
 // ------------------------------------------------------------------------------------
@@ -615,70 +616,71 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const
   __shared__ double red[W];
   fold_rows<CONS + 32>(c.part, gridDim.x, W, W, 0, 0, red);
   __shared__ SmallWork<S> sw;
-  if (threadIdx.x != 0) return;
+  epilogue_on_shared<S>(st, [&](DevState<S>* st) {
 
-  // epilogue: freev's counts and wrk (1143-1161), formk (907-1103), subsm's K solves
-  // (1459-1471)
-  const int nfree = (int)red[16];
-  if (!uncon) {
-    st->nfree = nfree;
-    st->nenter = (int)red[17];
-    st->nleave = (int)red[18];
-    st->wrk = (st->nleave > 0 || st->nenter > 0 || updatd) ? 1 : 0;
-  } else {
-    st->wrk = updatd ? 1 : 0;
-    st->nenter = 0;
-    st->nleave = 0;
-  }
-  st->free_hash = st->free_hash_acc;
-  st->free_hash_acc = 0;
-  st->spec_apply = 0;  // set by the direction pass when it applies an untruncated step
-  st->at_lower = (unsigned long long)red[19];
-  st->at_upper = (unsigned long long)red[20];
-  st->subsm_active = (st->nfree != 0 && col != 0) ? 1 : 0;
-  if (!st->subsm_active) return;
-  if (st->wrk) {
-    FormkSums<S>& fs = sw.fs;
-    for (int j = 0; j < kMaxM; j++) {
-      fs.yy_new[j] = (S)red[NA + j];
-      fs.sy_col[j] = (S)red[NA + kMaxM + j];
-      fs.ss_new[j] = (S)red[NA + NB + j];
-      fs.sy_row[j] = (S)red[NA + NB + kMaxM + j];
+    // epilogue: freev's counts and wrk (1143-1161), formk (907-1103), subsm's K solves
+    // (1459-1471)
+    const int nfree = (int)red[16];
+    if (!uncon) {
+      st->nfree = nfree;
+      st->nenter = (int)red[17];
+      st->nleave = (int)red[18];
+      st->wrk = (st->nleave > 0 || st->nenter > 0 || updatd) ? 1 : 0;
+    } else {
+      st->wrk = updatd ? 1 : 0;
+      st->nenter = 0;
+      st->nleave = 0;
     }
-    for (int q = 0; q < 32 * kLaneOwned; q++) {
-      int kind, a, b;
-      corr_map(q, kind, a, b);
-      if (kind >= 3) continue;
-      const S v = (S)red[NS + q];
-      if (kind == 0) fs.dyy[a][b] = v;
-      if (kind == 1) fs.dss[a][b] = v;
-      if (kind == 2) fs.dsy[a][b] = v;
+    st->free_hash = st->free_hash_acc;
+    st->free_hash_acc = 0;
+    st->spec_apply = 0;  // set by the direction pass when it applies an untruncated step
+    st->at_lower = (unsigned long long)red[19];
+    st->at_upper = (unsigned long long)red[20];
+    st->subsm_active = (st->nfree != 0 && col != 0) ? 1 : 0;
+    if (!st->subsm_active) return;
+    if (st->wrk) {
+      FormkSums<S>& fs = sw.fs;
+      for (int j = 0; j < kMaxM; j++) {
+        fs.yy_new[j] = (S)red[NA + j];
+        fs.sy_col[j] = (S)red[NA + kMaxM + j];
+        fs.ss_new[j] = (S)red[NA + NB + j];
+        fs.sy_row[j] = (S)red[NA + NB + kMaxM + j];
+      }
+      for (int q = 0; q < 32 * kLaneOwned; q++) {
+        int kind, a, b;
+        corr_map(q, kind, a, b);
+        if (kind >= 3) continue;
+        const S v = (S)red[NS + q];
+        if (kind == 0) fs.dyy[a][b] = v;
+        if (kind == 1) fs.dss[a][b] = v;
+        if (kind == 2) fs.dsy[a][b] = v;
+      }
+      const int info = sformk<S>(st->m, col, st->updatd, st->iupdat, theta, st->sy, st->wn,
+                                 st->wn1, fs, sw.work, sw.wm);
+      if (info != 0) {
+        st->internal_fail = info;
+        return;
+      }
     }
-    const int info = sformk<S>(st->m, col, st->updatd, st->iupdat, theta, st->sy, st->wn,
-                               st->wn1, fs, sw.work, sw.wm);
+    S* wv = sw.wv;
+    for (int j = 1; j <= col; j++) {
+      wv[j] = (S)red[j - 1];
+      wv[col + j] = theta * (S)red[8 + j - 1];
+    }
+    int info = 0;
+    sdtrsl(st->wn, 2 * kMaxM, 2 * col, wv, 11, &info);
     if (info != 0) {
       st->internal_fail = info;
       return;
     }
-  }
-  S* wv = sw.wv;
-  for (int j = 1; j <= col; j++) {
-    wv[j] = (S)red[j - 1];
-    wv[col + j] = theta * (S)red[8 + j - 1];
-  }
-  int info = 0;
-  sdtrsl(st->wn, 2 * kMaxM, 2 * col, wv, 11, &info);
-  if (info != 0) {
-    st->internal_fail = info;
-    return;
-  }
-  for (int j = 1; j <= col; j++) wv[j] = -wv[j];
-  sdtrsl(st->wn, 2 * kMaxM, 2 * col, wv, 1, &info);
-  if (info != 0) {
-    st->internal_fail = info;
-    return;
-  }
-  for (int j = 1; j <= 2 * col; j++) st->wv[j] = wv[j];
+    for (int j = 1; j <= col; j++) wv[j] = -wv[j];
+    sdtrsl(st->wn, 2 * kMaxM, 2 * col, wv, 1, &info);
+    if (info != 0) {
+      st->internal_fail = info;
+      return;
+    }
+    for (int j = 1; j <= 2 * col; j++) st->wv[j] = wv[j];
+  });
 }
 
 // lnsrlb's per-variable start at the subspace point z (lbfgsbcpu.cpp:1263-1299): d = z - x,
@@ -881,26 +883,27 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c, const R
   __shared__ double red[W];
   __shared__ double rl[3];
   fold_rows<CONS + 32>(c.part, gridDim.x, W, 2, 0, 2, red);
-  if (threadIdx.x != 0) return;
-  const S cand = (S)red[2];
-  if (cand < S(1)) {
-    st->alpha = cand;
-    st->ibd = (int)red[3];
-    st->iword = 1;
-    st->dir_no_spec = 1;
-    return;  // truncated: k_subsm_apply applies the step
-  }
-  st->alpha = 1;
-  st->ibd = -1;
-  st->iword = 0;
-  st->dir_no_spec = 0;
-  if (!spec) return;  // k_subsm_apply applies the step
-  // not truncated: the step written above is the subspace point; start the line search
-  rl[0] = red[0];
-  rl[1] = red[1];
-  rl[2] = red[4];
-  lnsrlb_start<S>(st, rl);
-  st->spec_apply = 1;
+  epilogue_on_shared<S>(st, [&](DevState<S>* st) {
+    const S cand = (S)red[2];
+    if (cand < S(1)) {
+      st->alpha = cand;
+      st->ibd = (int)red[3];
+      st->iword = 1;
+      st->dir_no_spec = 1;
+      return;  // truncated: k_subsm_apply applies the step
+    }
+    st->alpha = 1;
+    st->ibd = -1;
+    st->iword = 0;
+    st->dir_no_spec = 0;
+    if (!spec) return;  // k_subsm_apply applies the step
+    // not truncated: the step written above is the subspace point; start the line search
+    rl[0] = red[0];
+    rl[1] = red[1];
+    rl[2] = red[4];
+    lnsrlb_start<S>(st, rl);
+    st->spec_apply = 1;
+  });
 }
 
 // ------------------------------------------------------------------------------------
@@ -967,9 +970,10 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_apply(Ctx<R, H, S> c, const
   if (!last_cta(c.ticket)) return;
   __shared__ double red[W];
   fold_rows<CONS + 32>(c.part, gridDim.x, W, 2, 0, 1, red);
-  if (threadIdx.x != 0) return;
+  epilogue_on_shared<S>(st, [&](DevState<S>* st) {
 
-  lnsrlb_start<S>(st, red);
+    lnsrlb_start<S>(st, red);
+  });
 }
 
 // Trial point x = stp*d + t with d = z - t (lbfgsbcpu.cpp:1332-1334).
@@ -1157,9 +1161,10 @@ __global__ void __launch_bounds__(CONS + 32) k_post_eval(Ctx<R, H, S> c, const R
   if (!last_cta(c.ticket)) return;
   __shared__ double red[W];
   fold_rows<CONS + 32>(c.part, gridDim.x, W, NS, NX, 0, red);
-  if (threadIdx.x != 0) return;
+  epilogue_on_shared<S>(st, [&](DevState<S>* st) {
 
-  post_epilogue<S>(st, red, f, force_accept);
+    post_epilogue<S>(st, red, f, force_accept);
+  });
 }
 
 // ------------------------------------------------------------------------------------
@@ -1468,47 +1473,48 @@ __global__ void __launch_bounds__(CONS + 32) k_post_gcp(Ctx<R, H, S> c, const R*
   fold_rows<CONS + 32>(c.part, gridDim.x, W, NS, 2, 1, red);
   __shared__ SmallWork<S> sw;
   __shared__ double rp[NP + 1], rg[22];  // epilogue temporaries (shared, as all of them)
-  if (threadIdx.x != 0) return;
+  epilogue_on_shared<S>(st, [&](DevState<S>* st) {
 
-  for (int k = 0; k < NP; k++) rp[k] = red[k];
-  rp[NP] = red[NS];
-  st->spec_gcp = 0;
-  const int col_old = col;
-  if (!post_epilogue<S>(st, rp, f, force_accept) || st->internal_fail != 0) return;
-  // the next iteration's loop top and cauchy epilogue (279-284, 702-747) at the accepted x
-  begin_state(st, 0);
-  if (st->uncon_branch) {
+    for (int k = 0; k < NP; k++) rp[k] = red[k];
+    rp[NP] = red[NS];
+    st->spec_gcp = 0;
+    const int col_old = col;
+    if (!post_epilogue<S>(st, rp, f, force_accept) || st->internal_fail != 0) return;
+    // the next iteration's loop top and cauchy epilogue (279-284, 702-747) at the accepted x
+    begin_state(st, 0);
+    if (st->uncon_branch) {
+      st->spec_gcp = 1;
+      return;
+    }
+    const double* g = red + NP;
+    const int ncol = st->col;
+    const int shifted = (st->updatd && st->iupdat > st->m) ? 1 : 0;
+    rg[0] = g[0];
+    for (int j = 1; j <= kMaxM; j++) {
+      rg[j] = 0.0;
+      rg[8 + j] = 0.0;
+    }
+    if (!st->updatd) {
+      for (int j = 1; j <= col_old; j++) {
+        rg[j] = g[j];
+        rg[8 + j] = g[8 + j];
+      }
+    } else {
+      for (int j = 1; j <= ncol - 1; j++) {
+        rg[j] = g[j + shifted];
+        rg[8 + j] = g[8 + j + shifted];
+      }
+      rg[ncol] = g[17];
+      rg[8 + ncol] = g[18];
+    }
+    rg[17] = g[19];
+    rg[18] = g[20];
+    rg[19] = red[NS + 1];
+    rg[20] = red[NS + 2];
+    rg[21] = red[NS + 3];
+    gcp_epilogue<S>(st, rg, ncol, sw);
     st->spec_gcp = 1;
-    return;
-  }
-  const double* g = red + NP;
-  const int ncol = st->col;
-  const int shifted = (st->updatd && st->iupdat > st->m) ? 1 : 0;
-  rg[0] = g[0];
-  for (int j = 1; j <= kMaxM; j++) {
-    rg[j] = 0.0;
-    rg[8 + j] = 0.0;
-  }
-  if (!st->updatd) {
-    for (int j = 1; j <= col_old; j++) {
-      rg[j] = g[j];
-      rg[8 + j] = g[8 + j];
-    }
-  } else {
-    for (int j = 1; j <= ncol - 1; j++) {
-      rg[j] = g[j + shifted];
-      rg[8 + j] = g[8 + j + shifted];
-    }
-    rg[ncol] = g[17];
-    rg[8 + ncol] = g[18];
-  }
-  rg[17] = g[19];
-  rg[18] = g[20];
-  rg[19] = red[NS + 1];
-  rg[20] = red[NS + 2];
-  rg[21] = red[NS + 3];
-  gcp_epilogue<S>(st, rg, ncol, sw);
-  st->spec_gcp = 1;
+  });
 }
 
 }  // namespace lbfgsb_b200

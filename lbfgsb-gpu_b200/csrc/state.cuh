@@ -47,6 +47,25 @@ struct DevState {
   LineSearchSave<S> ls;
 };
 
+// The pass epilogues run in one thread and read and write the small matrices of the state
+// many times over; from global memory every such access would wait hundreds of cycles.  The
+// last CTA therefore copies the whole state into shared memory (all threads, 4-byte words,
+// loads that bypass L1 so that the other CTAs' writes are seen), its thread 0 runs the
+// epilogue f on that copy, and all threads store the copy back.
+template <typename S, typename F>
+__device__ __forceinline__ void epilogue_on_shared(DevState<S>* st, F&& f) {
+  static_assert(sizeof(DevState<S>) % 4 == 0, "the state is copied in 4-byte words");
+  constexpr int kWords = (int)(sizeof(DevState<S>) / 4);
+  __shared__ __align__(16) unsigned int words[kWords];
+  const unsigned int* src = reinterpret_cast<const unsigned int*>(st);
+  for (int k = threadIdx.x; k < kWords; k += blockDim.x) words[k] = __ldcg(src + k);
+  __syncthreads();
+  if (threadIdx.x == 0) f(reinterpret_cast<DevState<S>*>(words));
+  __syncthreads();
+  unsigned int* dst = reinterpret_cast<unsigned int*>(st);
+  for (int k = threadIdx.x; k < kWords; k += blockDim.x) dst[k] = words[k];
+}
+
 // A (value, index) pair reduced by minimum value, ties to the lower index.  kNoIndex
 // marks "no candidate" (exactly representable in the double rows of the reduction).
 constexpr long long kNoIndex = 1LL << 62;

@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(Ctx<R, H, S> c, const R* 
   __shared__ unsigned long long k_hi[kChunk];
   __shared__ unsigned int k_lo[kChunk];
   __shared__ unsigned int hist[256];
-  __shared__ int sh_count, sh_digit, sh_done;
+  __shared__ int sh_count, sh_done;
   __shared__ Key96 sh_prefix, sh_last;
   __shared__ long long sh_kk;
   __shared__ S b_wbp[kBatch][2 * kMaxM + 1];
