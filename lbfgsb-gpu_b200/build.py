@@ -19,7 +19,7 @@ REPO = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "liblbfgsb_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", f) for f in ("driver.cu", "objective.cu", "dsscfg.cu", "noalloc.cu")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in
-           ("common.cuh", "small.cuh", "state.cuh", "reduce.cuh", "tiles.cuh", "passes.cuh", "walk.cuh")]
+           ("common.cuh", "small.cuh", "state.cuh", "reduce.cuh", "tiles.cuh", "warp_small.cuh", "passes.cuh", "walk.cuh")]
 HEADERS.append(os.path.join(REPO, "include", "lbfgsb_b200.h"))
 
 NVCC_FLAGS = [

@@ -30,6 +30,7 @@
 #include "small.cuh"
 #include "state.cuh"
 #include "tiles.cuh"
+#include "warp_small.cuh"
 
 namespace lbfgsb_b200 {
 
@@ -223,74 +224,92 @@ __device__ __forceinline__ S reduced_grad(bool uncon, R x, R z, R g, int col,
 // red[18] movable variables without a breakpoint, red[19] > 0 if one of them has g != 0,
 // red[20] / red[21] the smallest breakpoint and its index.
 template <typename S>
-__device__ void gcp_epilogue(DevState<S>* st, const double* red, int col, SmallWork<S>& sw) {
+__device__ void gcp_epilogue(DevState<S>* st, const double* red, int col, SmallWork<S>& sw,
+                             int lane) {
+  // run by the 32 lanes of one warp: lane 0 writes the scalars, the products with the
+  // middle matrix are shared out (wbmv); every branch below depends only on red, st->theta
+  // and values that all lanes compute alike, so the warp never splits
   const S theta = st->theta;
   const S f1 = -(S)red[0];
   const int col2 = 2 * col;
-  for (int j = 1; j <= col; j++) {
-    st->p[j] = (S)red[j];
-    st->p[col + j] = (S)red[8 + j];
+  const int nbreak = (int)red[17], nfree_mov = (int)red[18];
+  if (lane == 0) {
+    for (int j = 1; j <= col; j++) {
+      st->p[j] = (S)red[j];
+      st->p[col + j] = (S)red[8 + j];
+    }
+    if (theta != S(1))
+      for (int j = col + 1; j <= col2; j++) st->p[j] *= theta;
+    st->nbreak = nbreak;
+    st->nfree_mov = nfree_mov;
+    st->bnded = red[19] > 0.0 ? 0 : 1;
+    st->internal_fail = 0;
   }
-  if (theta != S(1))
-    for (int j = col + 1; j <= col2; j++) st->p[j] *= theta;
-  st->nbreak = (int)red[17];
-  st->nfree_mov = (int)red[18];
-  st->bnded = red[19] > 0.0 ? 0 : 1;
-  st->internal_fail = 0;
-  if (st->nbreak == 0 && st->nfree_mov == 0) {
+  __syncwarp();
+  if (nbreak == 0 && nfree_mov == 0) {
     // xcp = x; c is left as it was (lbfgsbcpu.cpp:706-708), and cmprlb still applies the
     // current middle matrix to it
-    st->gcp_state = GCP_EARLY;
-    st->tsum = 0;
+    if (lane == 0) {
+      st->gcp_state = GCP_EARLY;
+      st->tsum = 0;
+    }
     if (col > 0) {
-      int info = 0;
-      sbmv(st->sy, st->wt, col, st->c, st->mc, &info, sw.work);
-      if (info != 0) st->internal_fail = -8;
+      const int info = wbmv(st->sy, st->wt, col, st->c, st->mc, sw.work, lane);
+      if (lane == 0 && info != 0) st->internal_fail = -8;
     }
     return;
   }
-  for (int j = 1; j <= col2; j++) st->c[j] = 0;
+  if (lane == 0)
+    for (int j = 1; j <= col2; j++) st->c[j] = 0;
   S f2 = -theta * f1;
   const S f2org = f2;
   if (col > 0) {
     S* v = sw.v;
-    int info = 0;
-    sbmv(st->sy, st->wt, col, st->p, v, &info, sw.work);
+    const int info = wbmv(st->sy, st->wt, col, st->p, v, sw.work, lane);
     if (info != 0) {
-      st->internal_fail = info;
+      if (lane == 0) st->internal_fail = info;
       return;
     }
     f2 = f2 - sdot(&v[1], 1, &st->p[1], 1, col2);
   }
   S dtm = -f1 / f2;
-  st->f1 = f1;
-  st->f2 = f2;
-  st->f1_0 = f1;
-  st->f2_0 = f2;
-  st->f2org = f2org;
-  st->tsum = 0;
-  st->tj = 0;
-  st->nint = 1;
-  st->nleft = st->nbreak;
-  if (st->nbreak != 0) {
-    st->bkmin = (S)red[20];
-    st->ibkmin = (int)red[21];
-    if (!(dtm < st->bkmin - S(0))) {
-      st->dtm = dtm;
-      st->gcp_state = GCP_WALK;  // at least one breakpoint is passed
+  if (lane == 0) {
+    st->f1 = f1;
+    st->f2 = f2;
+    st->f1_0 = f1;
+    st->f2_0 = f2;
+    st->f2org = f2org;
+    st->tsum = 0;
+    st->tj = 0;
+    st->nint = 1;
+    st->nleft = nbreak;
+  }
+  if (nbreak != 0) {
+    const S bkmin = (S)red[20];
+    if (lane == 0) {
+      st->bkmin = bkmin;
+      st->ibkmin = (int)red[21];
+    }
+    if (!(dtm < bkmin - S(0))) {
+      if (lane == 0) {
+        st->dtm = dtm;
+        st->gcp_state = GCP_WALK;  // at least one breakpoint is passed
+      }
       return;
     }
   }
   if (dtm <= S(0)) dtm = 0;
-  st->dtm = dtm;
-  st->tsum = st->tsum + dtm;
-  for (int j = 1; j <= col2; j++) st->c[j] += dtm * st->p[j];
-  if (col > 0) {
-    int info = 0;
-    sbmv(st->sy, st->wt, col, st->c, st->mc, &info, sw.work);  // cmprlb's M c (852)
-    if (info != 0) st->internal_fail = -8;
+  if (lane == 0) {
+    st->dtm = dtm;
+    st->tsum = st->tsum + dtm;
+    for (int j = 1; j <= col2; j++) st->c[j] += dtm * st->p[j];
   }
-  st->gcp_state = GCP_DONE;
+  __syncwarp();
+  if (col > 0) {
+    const int info = wbmv(st->sy, st->wt, col, st->c, st->mc, sw.work, lane);  // cmprlb's M c (852)
+    if (lane == 0 && info != 0) st->internal_fail = -8;
+  }
+  if (lane == 0) st->gcp_state = GCP_DONE;
 }
 
 // ------------------------------------------------------------------------------------
@@ -370,9 +389,8 @@ __global__ void __launch_bounds__(CONS + 32) k_gcp_scan(Ctx<R, H, S> c, const R*
   __shared__ double red[W];
   fold_rows<CONS + 32>(c.part, gridDim.x, W, NS, NX, NM, red);
   __shared__ SmallWork<S> sw;
-  epilogue_on_shared<S>(st, [&](DevState<S>* st) {
-
-    gcp_epilogue<S>(st, red, col, sw);
+  epilogue_on_shared_warp<S>(st, [&](DevState<S>* st, int lane) {
+    gcp_epilogue<S>(st, red, col, sw, lane);
   });
 }
 
@@ -616,37 +634,41 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const
   __shared__ double red[W];
   fold_rows<CONS + 32>(c.part, gridDim.x, W, W, 0, 0, red);
   __shared__ SmallWork<S> sw;
-  epilogue_on_shared<S>(st, [&](DevState<S>* st) {
-
+  __shared__ S wn1_snap[4 * kMaxM * kMaxM];
+  epilogue_on_shared_warp<S>(st, [&](DevState<S>* st, int lane) {
     // epilogue: freev's counts and wrk (1143-1161), formk (907-1103), subsm's K solves
-    // (1459-1471)
-    const int nfree = (int)red[16];
-    if (!uncon) {
-      st->nfree = nfree;
-      st->nenter = (int)red[17];
-      st->nleave = (int)red[18];
-      st->wrk = (st->nleave > 0 || st->nenter > 0 || updatd) ? 1 : 0;
-    } else {
-      st->wrk = updatd ? 1 : 0;
-      st->nenter = 0;
-      st->nleave = 0;
+    // (1459-1471); lane 0 writes the scalars, the matrix work is shared out over the warp
+    if (lane == 0) {
+      const int nfree = (int)red[16];
+      if (!uncon) {
+        st->nfree = nfree;
+        st->nenter = (int)red[17];
+        st->nleave = (int)red[18];
+        st->wrk = (st->nleave > 0 || st->nenter > 0 || updatd) ? 1 : 0;
+      } else {
+        st->wrk = updatd ? 1 : 0;
+        st->nenter = 0;
+        st->nleave = 0;
+      }
+      st->free_hash = st->free_hash_acc;
+      st->free_hash_acc = 0;
+      st->spec_apply = 0;  // set by the direction pass when it applies an untruncated step
+      st->at_lower = (unsigned long long)red[19];
+      st->at_upper = (unsigned long long)red[20];
+      st->subsm_active = (st->nfree != 0 && col != 0) ? 1 : 0;
     }
-    st->free_hash = st->free_hash_acc;
-    st->free_hash_acc = 0;
-    st->spec_apply = 0;  // set by the direction pass when it applies an untruncated step
-    st->at_lower = (unsigned long long)red[19];
-    st->at_upper = (unsigned long long)red[20];
-    st->subsm_active = (st->nfree != 0 && col != 0) ? 1 : 0;
+    __syncwarp();
     if (!st->subsm_active) return;
     if (st->wrk) {
       FormkSums<S>& fs = sw.fs;
-      for (int j = 0; j < kMaxM; j++) {
+      if (lane < kMaxM) {
+        const int j = lane;
         fs.yy_new[j] = (S)red[NA + j];
         fs.sy_col[j] = (S)red[NA + kMaxM + j];
         fs.ss_new[j] = (S)red[NA + NB + j];
         fs.sy_row[j] = (S)red[NA + NB + kMaxM + j];
       }
-      for (int q = 0; q < 32 * kLaneOwned; q++) {
+      for (int q = lane; q < 32 * kLaneOwned; q += 32) {
         int kind, a, b;
         corr_map(q, kind, a, b);
         if (kind >= 3) continue;
@@ -655,31 +677,31 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const
         if (kind == 1) fs.dss[a][b] = v;
         if (kind == 2) fs.dsy[a][b] = v;
       }
-      const int info = sformk<S>(st->m, col, st->updatd, st->iupdat, theta, st->sy, st->wn,
-                                 st->wn1, fs, sw.work, sw.wm);
+      __syncwarp();
+      const int info = wformk<S>(st->m, col, st->updatd, st->iupdat, theta, st->sy, st->wn,
+                                 st->wn1, fs, sw.wm, wn1_snap, lane);
       if (info != 0) {
-        st->internal_fail = info;
+        if (lane == 0) st->internal_fail = info;
         return;
       }
     }
     S* wv = sw.wv;
-    for (int j = 1; j <= col; j++) {
+    if (lane < col) {
+      const int j = lane + 1;
       wv[j] = (S)red[j - 1];
       wv[col + j] = theta * (S)red[8 + j - 1];
     }
-    int info = 0;
-    sdtrsl(st->wn, 2 * kMaxM, 2 * col, wv, 11, &info);
+    __syncwarp();
+    const int info = wdiag_zero(st->wn, 2 * kMaxM, 2 * col, lane);
     if (info != 0) {
-      st->internal_fail = info;
+      if (lane == 0) st->internal_fail = info;
       return;
     }
-    for (int j = 1; j <= col; j++) wv[j] = -wv[j];
-    sdtrsl(st->wn, 2 * kMaxM, 2 * col, wv, 1, &info);
-    if (info != 0) {
-      st->internal_fail = info;
-      return;
-    }
-    for (int j = 1; j <= 2 * col; j++) st->wv[j] = wv[j];
+    wdtrsl11(st->wn, 2 * kMaxM, 2 * col, wv, lane);
+    if (lane < col) wv[lane + 1] = -wv[lane + 1];
+    __syncwarp();
+    wdtrsl1(st->wn, 2 * kMaxM, 2 * col, wv, lane);  // the same diagonal: no zero
+    if (lane < 2 * col) st->wv[lane + 1] = wv[lane + 1];
   });
 }
 
@@ -993,9 +1015,12 @@ __global__ void k_trial(int n, const R* __restrict__ t, const R* __restrict__ z,
 // acceptance the stopping-test quantities (394-417) and matupd/formt (431-461, 1105-1133),
 // committing the spare slot that holds (s, y) to the ring.  red[0] g'd, red[1] |xold-x|^2,
 // red[2] y'y, red[3..10] s'y_j and red[11..18] s_j's by old ring position, red[19] the
-// projected-gradient norm.  Returns false while the line search goes on.
+// projected-gradient norm.  post_scalar runs on one lane and returns 0 while the line
+// search goes on, 1 when the step is accepted without an update, 2 when formt is due;
+// post_epilogue is run by the 32 lanes of a warp and returns false while the line search
+// goes on.
 template <typename S>
-__device__ bool post_epilogue(DevState<S>* st, const double* red, S f, int force_accept) {
+__device__ int post_scalar(DevState<S>* st, const double* red, S f, int force_accept) {
   st->f = f;
   st->gd = (S)red[0];
   if (!force_accept) {
@@ -1008,7 +1033,7 @@ __device__ bool post_epilogue(DevState<S>* st, const double* red, S f, int force
       st->ifun = st->ifun + 1;
       st->nfgv = st->nfgv + 1;
       st->iback = st->ifun - 1;
-      return false;
+      return 0;
     }
     st->ls_task = 5;
   }
@@ -1033,7 +1058,7 @@ __device__ bool post_epilogue(DevState<S>* st, const double* red, S f, int force
   st->internal_fail = 0;
   if ((double)dr <= 5e-16 * (double)ddum) {
     st->updatd = 0;
-    return true;
+    return 1;
   }
   st->updatd = 1;
   st->iupdat = st->iupdat + 1;
@@ -1065,9 +1090,21 @@ __device__ bool post_epilogue(DevState<S>* st, const double* red, S f, int force
   }
   LB_AT(st->ss, ld, ncol, ncol) = (sstp == S(1)) ? st->dtd : sstp * sstp * st->dtd;
   LB_AT(st->sy, ld, ncol, ncol) = dr;
-  const int info = sformt<S>(st->wt, st->sy, st->ss, ncol, st->theta);
-  if (info != 0) st->internal_fail = info;
-  return true;
+  return 2;
+}
+template <typename S>
+__device__ bool post_epilogue(DevState<S>* st, const double* red, S f, int force_accept,
+                              int lane) {
+  int r = 0;
+  if (lane == 0) r = post_scalar<S>(st, red, f, force_accept);
+  r = __shfl_sync(kFullMask, r, 0);
+  __syncwarp();
+  if (r == 2) {
+    const int info = wformt<S>(st->wt, st->sy, st->ss, st->col, st->theta, lane);
+    if (lane == 0 && info != 0) st->internal_fail = info;
+    __syncwarp();
+  }
+  return r != 0;
 }
 
 // ------------------------------------------------------------------------------------
@@ -1161,9 +1198,8 @@ __global__ void __launch_bounds__(CONS + 32) k_post_eval(Ctx<R, H, S> c, const R
   if (!last_cta(c.ticket)) return;
   __shared__ double red[W];
   fold_rows<CONS + 32>(c.part, gridDim.x, W, NS, NX, 0, red);
-  epilogue_on_shared<S>(st, [&](DevState<S>* st) {
-
-    post_epilogue<S>(st, red, f, force_accept);
+  epilogue_on_shared_warp<S>(st, [&](DevState<S>* st, int lane) {
+    post_epilogue<S>(st, red, f, force_accept, lane);
   });
 }
 
@@ -1473,47 +1509,53 @@ __global__ void __launch_bounds__(CONS + 32) k_post_gcp(Ctx<R, H, S> c, const R*
   fold_rows<CONS + 32>(c.part, gridDim.x, W, NS, 2, 1, red);
   __shared__ SmallWork<S> sw;
   __shared__ double rp[NP + 1], rg[22];  // epilogue temporaries (shared, as all of them)
-  epilogue_on_shared<S>(st, [&](DevState<S>* st) {
-
-    for (int k = 0; k < NP; k++) rp[k] = red[k];
-    rp[NP] = red[NS];
-    st->spec_gcp = 0;
+  epilogue_on_shared_warp<S>(st, [&](DevState<S>* st, int lane) {
+    if (lane == 0) {
+      for (int k = 0; k < NP; k++) rp[k] = red[k];
+      rp[NP] = red[NS];
+      st->spec_gcp = 0;
+    }
+    __syncwarp();
     const int col_old = col;
-    if (!post_epilogue<S>(st, rp, f, force_accept) || st->internal_fail != 0) return;
+    if (!post_epilogue<S>(st, rp, f, force_accept, lane) || st->internal_fail != 0) return;
     // the next iteration's loop top and cauchy epilogue (279-284, 702-747) at the accepted x
-    begin_state(st, 0);
+    if (lane == 0) begin_state(st, 0);
+    __syncwarp();
     if (st->uncon_branch) {
-      st->spec_gcp = 1;
+      if (lane == 0) st->spec_gcp = 1;
       return;
     }
-    const double* g = red + NP;
     const int ncol = st->col;
-    const int shifted = (st->updatd && st->iupdat > st->m) ? 1 : 0;
-    rg[0] = g[0];
-    for (int j = 1; j <= kMaxM; j++) {
-      rg[j] = 0.0;
-      rg[8 + j] = 0.0;
-    }
-    if (!st->updatd) {
-      for (int j = 1; j <= col_old; j++) {
-        rg[j] = g[j];
-        rg[8 + j] = g[8 + j];
+    if (lane == 0) {
+      const double* g = red + NP;
+      const int shifted = (st->updatd && st->iupdat > st->m) ? 1 : 0;
+      rg[0] = g[0];
+      for (int j = 1; j <= kMaxM; j++) {
+        rg[j] = 0.0;
+        rg[8 + j] = 0.0;
       }
-    } else {
-      for (int j = 1; j <= ncol - 1; j++) {
-        rg[j] = g[j + shifted];
-        rg[8 + j] = g[8 + j + shifted];
+      if (!st->updatd) {
+        for (int j = 1; j <= col_old; j++) {
+          rg[j] = g[j];
+          rg[8 + j] = g[8 + j];
+        }
+      } else {
+        for (int j = 1; j <= ncol - 1; j++) {
+          rg[j] = g[j + shifted];
+          rg[8 + j] = g[8 + j + shifted];
+        }
+        rg[ncol] = g[17];
+        rg[8 + ncol] = g[18];
       }
-      rg[ncol] = g[17];
-      rg[8 + ncol] = g[18];
+      rg[17] = g[19];
+      rg[18] = g[20];
+      rg[19] = red[NS + 1];
+      rg[20] = red[NS + 2];
+      rg[21] = red[NS + 3];
     }
-    rg[17] = g[19];
-    rg[18] = g[20];
-    rg[19] = red[NS + 1];
-    rg[20] = red[NS + 2];
-    rg[21] = red[NS + 3];
-    gcp_epilogue<S>(st, rg, ncol, sw);
-    st->spec_gcp = 1;
+    __syncwarp();
+    gcp_epilogue<S>(st, rg, ncol, sw, lane);
+    if (lane == 0) st->spec_gcp = 1;
   });
 }
 

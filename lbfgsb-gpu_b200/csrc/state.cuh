@@ -47,23 +47,37 @@ struct DevState {
   LineSearchSave<S> ls;
 };
 
-// The pass epilogues run in one thread and read and write the small matrices of the state
-// many times over; from global memory every such access would wait hundreds of cycles.  The
-// last CTA therefore copies the whole state into shared memory (all threads, 4-byte words,
-// loads that bypass L1 so that the other CTAs' writes are seen), its thread 0 runs the
-// epilogue f on that copy, and all threads store the copy back.
-template <typename S, typename F>
-__device__ __forceinline__ void epilogue_on_shared(DevState<S>* st, F&& f) {
+// The pass epilogues read and write the small matrices of the state many times over; from
+// global memory every such access would wait hundreds of cycles.  The last CTA therefore
+// copies the whole state into shared memory (all threads, 4-byte words, loads that bypass
+// L1 so that the other CTAs' writes are seen), runs the epilogue f on that copy, and all
+// threads store the copy back.  epilogue_on_shared runs f(st) on thread 0;
+// epilogue_on_shared_warp runs f(st, lane) on the 32 lanes of warp 0, for epilogues whose
+// matrix algebra is shared out over a warp (warp_small.cuh).
+template <bool kWarp, typename S, typename F>
+__device__ __forceinline__ void epilogue_in_shared(DevState<S>* st, F&& f) {
   static_assert(sizeof(DevState<S>) % 4 == 0, "the state is copied in 4-byte words");
   constexpr int kWords = (int)(sizeof(DevState<S>) / 4);
   __shared__ __align__(16) unsigned int words[kWords];
   const unsigned int* src = reinterpret_cast<const unsigned int*>(st);
   for (int k = threadIdx.x; k < kWords; k += blockDim.x) words[k] = __ldcg(src + k);
   __syncthreads();
-  if (threadIdx.x == 0) f(reinterpret_cast<DevState<S>*>(words));
+  if constexpr (kWarp) {
+    if (threadIdx.x < 32) f(reinterpret_cast<DevState<S>*>(words), (int)threadIdx.x);
+  } else {
+    if (threadIdx.x == 0) f(reinterpret_cast<DevState<S>*>(words));
+  }
   __syncthreads();
   unsigned int* dst = reinterpret_cast<unsigned int*>(st);
   for (int k = threadIdx.x; k < kWords; k += blockDim.x) dst[k] = words[k];
+}
+template <typename S, typename F>
+__device__ __forceinline__ void epilogue_on_shared(DevState<S>* st, F&& f) {
+  epilogue_in_shared<false>(st, f);
+}
+template <typename S, typename F>
+__device__ __forceinline__ void epilogue_on_shared_warp(DevState<S>* st, F&& f) {
+  epilogue_in_shared<true>(st, f);
 }
 
 // A (value, index) pair reduced by minimum value, ties to the lower index.  kNoIndex
