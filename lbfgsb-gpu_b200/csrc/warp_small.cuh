@@ -26,52 +26,71 @@ __device__ __forceinline__ int wdiag_zero(const S* t, int ld, int n, int lane) {
   return bal ? __ffs(bal) : 0;
 }
 
-// sdpofa as a wavefront (n <= 32): step k first finishes the diagonal of column k (lane
-// k-1, which has accumulated that column's sum of squares over the earlier steps in the
-// serial order), then computes entry (k, j) of every later column j (lane j-1).  Entry
-// (k, j) reads column k and entries 1..k-1 of column j, all final by then.  On a
-// non-positive pivot the columns after it are left partly updated; every caller discards
-// the matrix in that case, as after a failure of the serial routine.
+// sdpofa as a wavefront (n <= 32): step k finishes the diagonal of column k and then
+// entry (k, j) of every later column j (lane j-1).  Entry (k, j) reads column k and
+// entries 1..k-1 of column j, all final after step k-1, so its dot product is formed
+// while the diagonal's square root is taken; lane k-1 holds that column's sum of squares
+// (accumulated over the earlier steps in the serial order) and every lane takes the same
+// square root of the broadcast value, so the warp does not split.  No lane reads a(k, k)
+// after step k except lane k-1, which stores it.  Lanes past n work on column n and
+// discard the result.  On a non-positive pivot the columns after it are left partly
+// updated; every caller discards the matrix in that case, as after a failure of the
+// serial routine.
 template <typename S>
 __device__ bool wdpofa(S* a, int ld, int n, int lane) {
   S s = 0;
-  const int j = lane + 1;
+  const int j = lane + 1 <= n ? lane + 1 : n;
+  const bool mine = lane + 1 <= n;
   for (int k = 1; k <= n; k++) {
-    int ok = 1;
-    if (lane == k - 1) {
-      const S d = LB_AT(a, ld, k, k) - s;
-      if (d <= 0)
-        ok = 0;
-      else
-        LB_AT(a, ld, k, k) = ssqrt(d);
-    }
-    ok = __shfl_sync(kFullMask, ok, k - 1);
-    if (!ok) return false;
-    __syncwarp();
-    if (j > k && j <= n) {
-      const S v = sdot(&LB_AT(a, ld, 1, k), ld, &LB_AT(a, ld, 1, j), ld, k - 1);
+    const S v = sdot(&LB_AT(a, ld, 1, k), ld, &LB_AT(a, ld, 1, j), ld, k - 1);
+    const S d = LB_AT(a, ld, k, k) - __shfl_sync(kFullMask, s, k - 1);
+    if (d <= 0) return false;
+    const S dk = ssqrt(d);
+    if (mine && j > k) {
       S t = LB_AT(a, ld, k, j) - v;
-      t = t / LB_AT(a, ld, k, k);
+      t = t / dk;
       LB_AT(a, ld, k, j) = t;
       s = s + t * t;
     }
-    __syncwarp();
+    __syncwarp();  // every lane has read a(k, k) before it is replaced
+    if (lane == k - 1) LB_AT(a, ld, k, k) = dk;
   }
+  __syncwarp();
   return true;
 }
 
-// sdtrsl job 11 (t' x = b) for one right-hand side b (1-based, length n): the steps
-// depend on one another, so lane 0 runs them.  The caller has checked the diagonal.
+// sdtrsl job 11 (t' x = b) for one right-hand side b (1-based, n <= 32).  Lane j-1 owns
+// b[j] and forms the dot product of row j incrementally: at step i it receives the
+// finished b[i] and adds t(i, j) b[i] exactly where sdot adds it (inside a group of four,
+// then the group into the sum, or one by one past the last full group).  The caller has
+// checked the diagonal.
 template <typename S>
 __device__ __forceinline__ void wdtrsl11(const S* t, int ld, int n, S* b, int lane) {
-  if (lane == 0) {
-    b[1] = b[1] / LB_AT(t, ld, 1, 1);
-    for (int j = 2; j <= n; j++) {
-      const S v = sdot(&LB_AT(t, ld, 1, j), ld, &b[1], 1, j - 1);
-      b[j] = b[j] - v;
-      b[j] = b[j] / LB_AT(t, ld, j, j);
+  const int j = lane + 1;
+  const bool mine = j <= n;
+  S bj = mine ? b[j] : S(0);
+  if (j == 1) bj = bj / LB_AT(t, ld, 1, 1);
+  const int full = 4 * ((j - 1) / 4);  // row j's indices inside full groups
+  S r = 0, gp = 0;
+  for (int i = 1; i < n; i++) {
+    const S bi = __shfl_sync(kFullMask, bj, i - 1);
+    if (mine && j > i) {
+      const S pr = LB_AT(t, ld, i, j) * bi;
+      if (i <= full) {
+        const int pos = (i - 1) & 3;
+        gp = pos == 0 ? pr : gp + pr;
+        if (pos == 3) r += gp;
+      } else {
+        r += pr;
+      }
+      if (i == j - 1) {
+        bj = bj - r;
+        bj = bj / LB_AT(t, ld, j, j);
+      }
     }
   }
+  __syncwarp();
+  if (mine) b[j] = bj;
   __syncwarp();
 }
 
@@ -139,15 +158,13 @@ template <typename S>
 __device__ int wformt(S* wt, const S* sy, const S* ss, int col, S theta, int lane) {
   constexpr int ld = kMaxM;
   if (lane < col) LB_AT(wt, ld, 1, lane + 1) = theta * LB_AT(ss, ld, 1, lane + 1);
-  int q = 0;
-  for (int i = 2; i <= col; i++) {
-    for (int j = i; j <= col; j++, q++) {
-      if ((q & 31) != lane) continue;
-      const int k1 = (i < j ? i : j) - 1;
-      S ddum = 0;
-      for (int k = 1; k <= k1; k++) ddum = ddum + LB_AT(sy, ld, i, k) * LB_AT(sy, ld, j, k) / LB_AT(sy, ld, k, k);
-      LB_AT(wt, ld, i, j) = ddum + theta * LB_AT(ss, ld, i, j);
-    }
+  for (int q = lane; q < col * col; q += 32) {
+    const int i = q / col + 1, j = q % col + 1;
+    if (i < 2 || j < i) continue;
+    const int k1 = (i < j ? i : j) - 1;
+    S ddum = 0;
+    for (int k = 1; k <= k1; k++) ddum = ddum + LB_AT(sy, ld, i, k) * LB_AT(sy, ld, j, k) / LB_AT(sy, ld, k, k);
+    LB_AT(wt, ld, i, j) = ddum + theta * LB_AT(ss, ld, i, j);
   }
   __syncwarp();
   return wdpofa(wt, ld, col, lane) ? 0 : -3;
@@ -155,7 +172,10 @@ __device__ int wformt(S* wt, const S* sy, const S* ss, int col, S theta, int lan
 
 // sformk.  snap holds 4 kMaxM^2 scalars: the shift of wn1 writes every entry from one to
 // its lower right that the serial loops have not yet rewritten, so each write is a copy
-// from a snapshot taken before it.
+// from a snapshot taken before it.  The serial loops write entry (r, c) of three regions,
+// (c <= r <= m-1), (m+1 <= c <= r <= 2m-1) and (m+1 <= r <= 2m-1, c <= m-1), each from
+// (r+1, c+1).  Items are dealt to the lanes by index (q = lane, lane + 32, ...), so that
+// the lanes work at the same time.
 template <typename S>
 __device__ int wformk(int m, int col, int updatd, int iupdat, S theta, const S* sy, S* wn,
                       S* wn1, const FormkSums<S>& fs, S* wm, S* snap, int lane) {
@@ -165,15 +185,12 @@ __device__ int wformk(int m, int col, int updatd, int iupdat, S theta, const S* 
     if (iupdat > m) {
       for (int e = lane; e < L2 * L2; e += 32) snap[e] = wn1[e];
       __syncwarp();
-      int q = 0;
-      for (int jy = 1; jy <= m - 1; jy++) {
-        const int js = m + jy;
-        for (int i = 0; i <= m - 1 - jy; i++, q++)
-          if ((q & 31) == lane) LB_AT(wn1, L2, jy + i, jy) = LB_AT(snap, L2, jy + 1 + i, jy + 1);
-        for (int i = 0; i <= m - 1 - jy; i++, q++)
-          if ((q & 31) == lane) LB_AT(wn1, L2, js + i, js) = LB_AT(snap, L2, js + 1 + i, js + 1);
-        for (int i = 0; i <= m - 2; i++, q++)
-          if ((q & 31) == lane) LB_AT(wn1, L2, m + 1 + i, jy) = LB_AT(snap, L2, m + 2 + i, jy + 1);
+      for (int e = lane; e < L2 * L2; e += 32) {
+        const int r = e / L2 + 1, c = e % L2 + 1;
+        const bool lo = c <= r && r <= m - 1;
+        const bool hi = m + 1 <= c && c <= r && r <= 2 * m - 1;
+        const bool mid = m + 1 <= r && r <= 2 * m - 1 && c <= m - 1;
+        if (lo || hi || mid) LB_AT(wn1, L2, r, c) = LB_AT(snap, L2, r + 1, c + 1);
       }
       __syncwarp();
     }
@@ -227,13 +244,11 @@ __device__ int wformk(int m, int col, int updatd, int iupdat, S theta, const S* 
     }
   }
   __syncwarp();
-  int q = 0;
-  for (int iis = col + 1; iis <= 2 * col; iis++) {
-    for (int js = iis; js <= 2 * col; js++, q++) {
-      if ((q & 31) != lane) continue;
-      const S v = sdot(&LB_AT(wn, L2, 1, iis), L2, &LB_AT(wn, L2, 1, js), L2, col);
-      LB_AT(wn, L2, iis, js) = LB_AT(wn, L2, iis, js) + v;
-    }
+  for (int q = lane; q < col * col; q += 32) {
+    const int iis = col + 1 + q / col, js = col + 1 + q % col;
+    if (js < iis) continue;
+    const S v = sdot(&LB_AT(wn, L2, 1, iis), L2, &LB_AT(wn, L2, 1, js), L2, col);
+    LB_AT(wn, L2, iis, js) = LB_AT(wn, L2, iis, js) + v;
   }
   __syncwarp();
   for (int e = lane; e < col * col; e += 32) {
