@@ -367,6 +367,97 @@ def batched_compare(count: int = 256, workers: int = 16):
                     "host thread, whole solves overlapped"}
 
 
+def serving_compare(count: int = 64, rate: float = 2000.0, workers: int = 16):
+    """A bounded sample of the serving workload: `count` solve requests with Poisson
+    arrivals at `rate` per second, each a synthetic bounded grid problem with its own seed
+    and grid side log-uniform in [64, 2048] (n 4,096 .. 4,194,304), FP32 vectors with FP64
+    small-matrix steps, eps_g = 1e-6, at most 500 iterations, device objectives, admitted
+    against a 150 GB workspace budget by the library's server (lbfgsb_b200_server_*) on
+    `workers` streams; latency is submit to result.  The one-at-a-time baseline solves the
+    same requests alone, one after another, and its latencies are those of a first come,
+    first served single server with the same arrival times and the measured solve times."""
+    import ctypes as C
+    import torch
+    import lbfgsb_b200 as LB
+    import synth
+    lib = LB.load()
+    rng = np.random.default_rng(4)
+    sides = np.rint(np.exp(rng.uniform(np.log(64), np.log(2048), count))).astype(int)
+    gaps = rng.exponential(1.0 / rate, count)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    probs = [synth.synth_problem(int(s), seed=500 + k) for k, s in enumerate(sides)]
+    objs = [LB.SynthObjective(p, single_precision_fields=True) for p in probs]
+    dev = [dict(l=torch.from_numpy(p["l"].astype(np.float32)).cuda(),
+                u=torch.from_numpy(p["u"].astype(np.float32)).cuda(),
+                nbd=torch.from_numpy(p["nbd"]).cuda()) for p in probs]
+    ns = [p["nbd"].size for p in probs]
+    opt = LB.default_option(np.float32)
+    opt.eps_g = 1e-6
+    opt.max_iteration = 500
+    form = LB.FORM_MIXED
+    ext = LB.Ext(form, 0, LB.TRACE_CB(), None)
+
+    def alone(k):
+        x = torch.zeros(ns[k], dtype=torch.float32, device="cuda")
+        summ = LB.SummaryF32()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = lib.lbfgsb_b200_minimize_ext_f32(ns[k], x.data_ptr(), dev[k]["nbd"].data_ptr(),
+                                              dev[k]["l"].data_ptr(), dev[k]["u"].data_ptr(),
+                                              C.byref(opt), objs[k].f32, None, None,
+                                              objs[k].handle, None, C.byref(ext), C.byref(summ))
+        torch.cuda.synchronize()
+        if st != 0:
+            raise RuntimeError(lib.lbfgsb_b200_last_error().decode())
+        return time.perf_counter() - t0, x, summ
+
+    alone(int(np.argmax(ns)))  # grow the workspace pool once
+    solo = [alone(k) for k in range(count)]
+    finish, lat1 = 0.0, []
+    for a, (d, _, _) in zip(arrivals, solo):
+        finish = max(a, finish) + d
+        lat1.append(finish - a)
+    span1 = finish - arrivals[0]
+
+    sv = LB.Server(workers=workers, hbm_budget_bytes=150 * 10**9, form=form)
+    xs = [torch.zeros(n, dtype=torch.float32, device="cuda") for n in ns]
+    torch.cuda.synchronize()
+    ids = []
+    t0 = time.perf_counter()
+    for k in range(count):
+        delay = t0 + arrivals[k] - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        rc, rid = sv.submit(ns[k], xs[k], dev[k]["nbd"], dev[k]["l"], dev[k]["u"], opt,
+                            objs[k].f32, objs[k].handle)
+        if rc != 0:
+            raise RuntimeError(lib.lbfgsb_b200_last_error().decode())
+        ids.append(rid)
+    outs = [sv.wait(rid) for rid in ids]
+    span = time.perf_counter() - t0
+    peak_bytes, peak_running = sv.peak()
+    sv.close()
+    torch.cuda.synchronize()
+    same = all(o[0] == 0 and torch.equal(xs[k], solo[k][1]) and
+               (o[1].info, o[1].num_iteration) == (solo[k][2].info, solo[k][2].num_iteration)
+               for k, o in enumerate(outs))
+    for o in objs:
+        o.close()
+    lat = np.array([o[2] for o in outs])
+    its = np.array([o[1].num_iteration for o in outs])
+    return {"requests": count, "offered_per_s": rate, "workers": workers,
+            "hbm_budget_gb": 150, "n_range": [int(min(ns)), int(max(ns))], "n_total": int(sum(ns)),
+            "solves_per_s": count / span, "p50_latency_s": float(np.percentile(lat, 50)),
+            "p99_latency_s": float(np.percentile(lat, 99)),
+            "one_at_a_time_solves_per_s": count / span1,
+            "one_at_a_time_p50_latency_s": float(np.percentile(lat1, 50)),
+            "one_at_a_time_p99_latency_s": float(np.percentile(lat1, 99)),
+            "peak_admitted": peak_running, "peak_workspace_gb": peak_bytes / 1e9,
+            "iterations_mean": float(its.mean()), "identical_results": bool(same),
+            "note": f"a {count}-request sample of the 60 s stream at the same arrival rate "
+                    "(all arrive within a fraction of a second, so the queue builds up)"}
+
+
 def max_over_ranks(values, dist, device):
     """Each value's maximum over the ranks (the job's time is its slowest rank's)."""
     import torch
@@ -522,9 +613,11 @@ def main():
                              "reference lbfgsbcpu.cpp built from source, 1 thread"}
     dss = None
     batched = None
+    serving = None
     if not args.no_cpu_baseline and world == 1:
         dss = dsscfg_compare()
         batched = batched_compare()
+        serving = serving_compare()
     e2e_iters = max(1, r["e2e_iters"])
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
@@ -543,6 +636,7 @@ def main():
         "hbm_GBps_model": r["model_bytes_iter"] / (solver_ms / K / 1000.0) / 1e9 if solver_ms else None,
         "kernels": per_kernel,
         "dsscfg": dss,
+        "serving": serving,
         "batched": batched,
     }
     print(json.dumps(line))

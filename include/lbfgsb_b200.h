@@ -136,6 +136,42 @@ int lbfgsb_b200_minimize_batch_f32(int count, const int* n, float* const* x,
                                    int* status, double* seconds);
 
 
+/* An upper bound on the device bytes one solve of n elements takes from the workspace pool
+ * (real_size 8: the f64 entry points; 4: the f32 ones with `form` as in lbfgsb_b200_ext).
+ * Host-only arithmetic; 0 for a bad argument. */
+unsigned long long lbfgsb_b200_workspace_bytes(int n, int real_size, int form);
+
+/* Serving front end (the reference has none: it solves one problem per call).  A server
+ * owns `workers` host threads (0: 16), each with its own non-blocking stream on the device
+ * that is current when it is created.  lbfgsb_b200_server_submit_f32 queues one whole FP32
+ * solve on the caller's device arrays (x in / out, nbd, l, u; they must stay valid until
+ * the request is waited on) and returns at once with its id.  Requests are admitted in
+ * arrival order, each when its workspace bound (lbfgsb_b200_workspace_bytes) fits beside
+ * the solves already running within `hbm_budget_bytes`; a request that does not fit holds
+ * back the ones behind it.  A request larger than the whole budget is refused at submit
+ * (LBFGSB_B200_ERR_ARGUMENT).  `form` is the precision form of every request
+ * (LBFGSB_B200_FORM_MIXED: FP32 vectors with FP64 small-matrix steps).  funcgrad is
+ * called from the worker that runs the request, with that worker's stream.
+ * lbfgsb_b200_server_wait blocks until request `id` has finished and gives its summary,
+ * its solve's return code, the seconds from submit to result and the seconds it waited
+ * for admission; a request's result equals what the same solve gives through
+ * lbfgsb_b200_minimize_ext_f32 with that form.  lbfgsb_b200_server_peak reports the most
+ * workspace bytes and the most solves that were admitted at once.
+ * lbfgsb_b200_server_destroy finishes every queued request, then stops the workers. */
+typedef struct lbfgsb_b200_server lbfgsb_b200_server;
+int lbfgsb_b200_server_create(int workers, unsigned long long hbm_budget_bytes, int form,
+                              lbfgsb_b200_server** server);
+int lbfgsb_b200_server_submit_f32(lbfgsb_b200_server* server, int n, float* x, const int* nbd,
+                                  const float* l, const float* u,
+                                  const lbfgsb_b200_option_f32* option,
+                                  lbfgsb_b200_callback_f32 funcgrad, void* user, long long* id);
+int lbfgsb_b200_server_wait(lbfgsb_b200_server* server, long long id,
+                            lbfgsb_b200_summary_f32* summary, int* status, double* latency_s,
+                            double* queue_s);
+int lbfgsb_b200_server_peak(lbfgsb_b200_server* server, unsigned long long* peak_bytes,
+                            int* peak_running);
+int lbfgsb_b200_server_destroy(lbfgsb_b200_server* server);
+
 /* One record per accepted iteration, mirroring the CPU oracle's trace: the state the step
  * was computed from (col, head, theta, Cauchy-point and free-set statistics) and the
  * line-search outcome. */

@@ -12,8 +12,10 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -770,6 +772,100 @@ static int minimize_batch(int count, const int* n, R* const* x, const int* const
   return first_status;
 }
 
+// Bytes that one solve of n elements may take from the workspace pool: an upper bound
+// (the 16-byte aligned copies of l, u and nbd, the breakpoint-walk buffers, and reduction
+// rows for up to 4096 CTAs included).  It calls nothing on the device.
+static size_t workspace_bound(long long n, size_t real, size_t hist) {
+  const size_t N = (size_t)std::max<long long>(n, 1);
+  const size_t ld = ((N + kTile - 1) / kTile) * kTile;
+  constexpr size_t kRowsBound = 4096;
+  return N * (8 * real + 4 + 1 + 12) + 2 * ld * kSlots * hist + (N / 32 + 2) * 4 +
+         sizeof(DevState<double>) + kRowsBound * 256 * 8 + ((size_t)1 << 20);
+}
+
+// Serving front end.  Requests (whole FP32 solves on the caller's device arrays) arrive
+// one by one, wait in arrival order until their workspace fits in the HBM budget beside
+// the solves already running, and run on a pool of host workers, each with its own
+// stream.  Admission is first come, first served: a request that does not fit holds back
+// the ones behind it until running solves release enough memory.
+struct ServeRequest {
+  int n = 0;
+  float* x = nullptr;
+  const int* nbd = nullptr;
+  const float* l = nullptr;
+  const float* u = nullptr;
+  lbfgsb_b200_option_f32 option{};
+  lbfgsb_b200_callback_f32 funcgrad = nullptr;
+  void* user = nullptr;
+  size_t bytes = 0;
+  std::chrono::steady_clock::time_point arrive, start, finish;
+  lbfgsb_b200_summary_f32 summary{};
+  int status = -1;
+  bool done = false;
+  std::string error;
+};
+
+struct Server {
+  int dev = 0, form = LBFGSB_B200_FORM_MIXED;
+  size_t budget = 0, in_use = 0, peak_bytes = 0;
+  int running = 0, peak_running = 0;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<ServeRequest> reqs;  // by id (push_back keeps references to the others valid)
+  std::deque<long long> queue;    // ids waiting for admission, in arrival order
+  bool stop = false;
+  std::vector<std::thread> workers;
+};
+
+static void serve_worker(Server* sv) {
+  cudaStream_t s = nullptr;
+  const bool ok = cudaSetDevice(sv->dev) == cudaSuccess &&
+                  cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
+  std::unique_lock<std::mutex> lock(sv->mu);
+  for (;;) {
+    sv->cv_work.wait(lock, [&] {
+      return (sv->stop && sv->queue.empty()) ||
+             (!sv->queue.empty() && sv->in_use + sv->reqs[(size_t)sv->queue.front()].bytes <= sv->budget);
+    });
+    if (sv->queue.empty()) break;
+    const long long id = sv->queue.front();
+    sv->queue.pop_front();
+    ServeRequest& r = sv->reqs[(size_t)id];
+    sv->in_use += r.bytes;
+    sv->peak_bytes = std::max(sv->peak_bytes, sv->in_use);
+    sv->peak_running = std::max(sv->peak_running, ++sv->running);
+    r.start = std::chrono::steady_clock::now();
+    lock.unlock();
+    int st = LBFGSB_B200_ERR_CUDA;
+    std::string err = "server: worker stream set-up failed";
+    if (ok) {
+      lbfgsb_b200_ext ext{};
+      ext.form = sv->form;
+      if (sv->form == LBFGSB_B200_FORM_MIXED)
+        st = solve<float, float, double>(r.n, r.x, r.nbd, r.l, r.u, &r.option, r.funcgrad, nullptr,
+                                         nullptr, r.user, s, &ext, &r.summary);
+      else if (sv->form == LBFGSB_B200_FORM_MIXED_BF16)
+        st = solve<float, __nv_bfloat16, double>(r.n, r.x, r.nbd, r.l, r.u, &r.option, r.funcgrad,
+                                                 nullptr, nullptr, r.user, s, &ext, &r.summary);
+      else
+        st = solve<float, float, float>(r.n, r.x, r.nbd, r.l, r.u, &r.option, r.funcgrad, nullptr,
+                                        nullptr, r.user, s, &ext, &r.summary);
+      err = st == LBFGSB_B200_OK ? std::string() : g_last_error;
+    }
+    lock.lock();
+    sv->in_use -= r.bytes;
+    sv->running--;
+    r.finish = std::chrono::steady_clock::now();
+    r.status = st;
+    r.error = err;
+    r.done = true;
+    sv->cv_done.notify_all();
+    sv->cv_work.notify_all();
+  }
+  lock.unlock();
+  if (s) cudaStreamDestroy(s);
+}
+
 }  // namespace lbfgsb_b200
 
 using namespace lbfgsb_b200;
@@ -853,6 +949,122 @@ int lbfgsb_b200_minimize_batch_f32(int count, const int* n, float* const* x,
                                    int* status, double* seconds) {
   return lbfgsb_b200::minimize_batch<float>(count, n, x, nbd, l, u, option, funcgrad, user,
                                             concurrency, summary, status, seconds);
+}
+
+unsigned long long lbfgsb_b200_workspace_bytes(int n, int real_size, int form) {
+  if (n <= 0 || (real_size != 4 && real_size != 8)) return 0;
+  const size_t hist = (real_size == 4 && form == LBFGSB_B200_FORM_MIXED_BF16) ? 2 : (size_t)real_size;
+  return (unsigned long long)workspace_bound(n, (size_t)real_size, hist);
+}
+
+int lbfgsb_b200_server_create(int workers, unsigned long long hbm_budget_bytes, int form,
+                              lbfgsb_b200_server** out) {
+  g_last_error.clear();
+  if (!out || workers < 0 || form < LBFGSB_B200_FORM_PLAIN || form > LBFGSB_B200_FORM_MIXED_BF16) {
+    g_last_error = "server_create: bad argument";
+    return LBFGSB_B200_ERR_ARGUMENT;
+  }
+  *out = nullptr;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    g_last_error = cudaGetErrorString(e);
+    return LBFGSB_B200_ERR_CUDA;
+  }
+  auto* sv = new Server;
+  sv->dev = dev;
+  sv->form = form;
+  sv->budget = (size_t)hbm_budget_bytes;
+  const int nw = workers > 0 ? workers : 16;
+  for (int w = 0; w < nw; w++) sv->workers.emplace_back(serve_worker, sv);
+  *out = reinterpret_cast<lbfgsb_b200_server*>(sv);
+  return LBFGSB_B200_OK;
+}
+
+int lbfgsb_b200_server_submit_f32(lbfgsb_b200_server* server, int n, float* x, const int* nbd,
+                                  const float* l, const float* u,
+                                  const lbfgsb_b200_option_f32* option,
+                                  lbfgsb_b200_callback_f32 funcgrad, void* user, long long* id) {
+  g_last_error.clear();
+  auto* sv = reinterpret_cast<Server*>(server);
+  if (!sv || n <= 0 || !x || !nbd || !l || !u || !option || !funcgrad || !id) {
+    g_last_error = "server_submit: null argument or n <= 0";
+    return LBFGSB_B200_ERR_ARGUMENT;
+  }
+  const size_t bytes = workspace_bound(n, 4, sv->form == LBFGSB_B200_FORM_MIXED_BF16 ? 2 : 4);
+  if (bytes > sv->budget) {
+    g_last_error = "server_submit: the solve's workspace (" + std::to_string(bytes) +
+                   " bytes) exceeds the server's HBM budget (" + std::to_string(sv->budget) + ")";
+    return LBFGSB_B200_ERR_ARGUMENT;
+  }
+  std::lock_guard<std::mutex> lock(sv->mu);
+  if (sv->stop) {
+    g_last_error = "server_submit: the server is shutting down";
+    return LBFGSB_B200_ERR_ARGUMENT;
+  }
+  sv->reqs.emplace_back();
+  ServeRequest& r = sv->reqs.back();
+  r.n = n;
+  r.x = x;
+  r.nbd = nbd;
+  r.l = l;
+  r.u = u;
+  r.option = *option;
+  r.funcgrad = funcgrad;
+  r.user = user;
+  r.bytes = bytes;
+  r.arrive = std::chrono::steady_clock::now();
+  *id = (long long)sv->reqs.size() - 1;
+  sv->queue.push_back(*id);
+  sv->cv_work.notify_all();
+  return LBFGSB_B200_OK;
+}
+
+int lbfgsb_b200_server_wait(lbfgsb_b200_server* server, long long id,
+                            lbfgsb_b200_summary_f32* summary, int* status, double* latency_s,
+                            double* queue_s) {
+  g_last_error.clear();
+  auto* sv = reinterpret_cast<Server*>(server);
+  if (!sv || id < 0) {
+    g_last_error = "server_wait: bad argument";
+    return LBFGSB_B200_ERR_ARGUMENT;
+  }
+  std::unique_lock<std::mutex> lock(sv->mu);
+  if ((size_t)id >= sv->reqs.size()) {
+    g_last_error = "server_wait: unknown request id";
+    return LBFGSB_B200_ERR_ARGUMENT;
+  }
+  sv->cv_done.wait(lock, [&] { return sv->reqs[(size_t)id].done; });
+  const ServeRequest& r = sv->reqs[(size_t)id];
+  if (summary) *summary = r.summary;
+  if (status) *status = r.status;
+  if (latency_s) *latency_s = std::chrono::duration<double>(r.finish - r.arrive).count();
+  if (queue_s) *queue_s = std::chrono::duration<double>(r.start - r.arrive).count();
+  if (r.status != LBFGSB_B200_OK) g_last_error = r.error;
+  return LBFGSB_B200_OK;
+}
+
+int lbfgsb_b200_server_peak(lbfgsb_b200_server* server, unsigned long long* peak_bytes,
+                            int* peak_running) {
+  auto* sv = reinterpret_cast<Server*>(server);
+  if (!sv) return LBFGSB_B200_ERR_ARGUMENT;
+  std::lock_guard<std::mutex> lock(sv->mu);
+  if (peak_bytes) *peak_bytes = (unsigned long long)sv->peak_bytes;
+  if (peak_running) *peak_running = sv->peak_running;
+  return LBFGSB_B200_OK;
+}
+
+int lbfgsb_b200_server_destroy(lbfgsb_b200_server* server) {
+  auto* sv = reinterpret_cast<Server*>(server);
+  if (!sv) return LBFGSB_B200_ERR_ARGUMENT;
+  {
+    std::lock_guard<std::mutex> lock(sv->mu);
+    sv->stop = true;
+  }
+  sv->cv_work.notify_all();
+  for (auto& t : sv->workers) t.join();
+  delete sv;
+  return LBFGSB_B200_OK;
 }
 
 int lbfgsb_b200_last_stats(lbfgsb_b200_stats* out) {

@@ -91,6 +91,8 @@ EXPORTS = [
     "lbfgsb_b200_dsscfg_funcgrad_f64", "lbfgsb_b200_dsscfg_funcgrad_f32",
     "lbfgsb_b200_dsscfg_start_f64", "lbfgsb_b200_dsscfg_start_f32",
     "lbfgsb_b200_minimize_batch_f64", "lbfgsb_b200_minimize_batch_f32",
+    "lbfgsb_b200_workspace_bytes", "lbfgsb_b200_server_create", "lbfgsb_b200_server_submit_f32",
+    "lbfgsb_b200_server_wait", "lbfgsb_b200_server_peak", "lbfgsb_b200_server_destroy",
 ]
 
 _lib = None
@@ -145,6 +147,21 @@ def load() -> C.CDLL:
         fn.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     lib.lbfgsb_b200_projgr_noalloc_f64.restype = C.c_int
     lib.lbfgsb_b200_projgr_noalloc_f64.argtypes = [C.c_int] + [C.c_void_p] * 7
+    lib.lbfgsb_b200_workspace_bytes.restype = C.c_ulonglong
+    lib.lbfgsb_b200_workspace_bytes.argtypes = [C.c_int, C.c_int, C.c_int]
+    lib.lbfgsb_b200_server_create.restype = C.c_int
+    lib.lbfgsb_b200_server_create.argtypes = [C.c_int, C.c_ulonglong, C.c_int, C.POINTER(C.c_void_p)]
+    lib.lbfgsb_b200_server_submit_f32.restype = C.c_int
+    lib.lbfgsb_b200_server_submit_f32.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 4 + \
+        [C.POINTER(OptionF32), C.c_void_p, C.c_void_p, C.POINTER(C.c_longlong)]
+    lib.lbfgsb_b200_server_wait.restype = C.c_int
+    lib.lbfgsb_b200_server_wait.argtypes = [C.c_void_p, C.c_longlong, C.POINTER(SummaryF32),
+                                            C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                            C.POINTER(C.c_double)]
+    lib.lbfgsb_b200_server_peak.restype = C.c_int
+    lib.lbfgsb_b200_server_peak.argtypes = [C.c_void_p, C.POINTER(C.c_ulonglong), C.POINTER(C.c_int)]
+    lib.lbfgsb_b200_server_destroy.restype = C.c_int
+    lib.lbfgsb_b200_server_destroy.argtypes = [C.c_void_p]
     _lib = lib
     return lib
 
@@ -189,6 +206,50 @@ def solve_batch(ns, xs, nbds, ls, us, option, funcgrad, users, concurrency=16, d
     rc = fn(k, n_arr, ptrs(xs), ptrs(nbds), ptrs(ls), ptrs(us), C.byref(option), funcgrad,
             us_arr, concurrency, summ, stat, secs)
     return rc, list(stat), list(summ), list(secs)
+
+
+class Server:
+    """The serving front end (lbfgsb_b200_server_*): FP32 solves queued one by one,
+    admitted in arrival order within an HBM budget, run on `workers` streams."""
+
+    def __init__(self, workers=16, hbm_budget_bytes=150 * 10**9, form=FORM_MIXED):
+        self.lib = load()
+        h = C.c_void_p()
+        rc = self.lib.lbfgsb_b200_server_create(workers, hbm_budget_bytes, form, C.byref(h))
+        if rc != 0:
+            raise RuntimeError(self.lib.lbfgsb_b200_last_error().decode())
+        self.handle = h
+
+    def submit(self, n, x, nbd, l, u, option, funcgrad, user):
+        """Queue one solve on device tensors; returns (status, request id)."""
+        rid = C.c_longlong(-1)
+        rc = self.lib.lbfgsb_b200_server_submit_f32(self.handle, n, x.data_ptr(), nbd.data_ptr(),
+                                                    l.data_ptr(), u.data_ptr(), C.byref(option),
+                                                    funcgrad, user, C.byref(rid))
+        return rc, rid.value
+
+    def wait(self, rid):
+        """(status, summary, seconds from submit to result, seconds waiting for admission)."""
+        summ = SummaryF32()
+        st = C.c_int(-1)
+        lat = C.c_double()
+        q = C.c_double()
+        rc = self.lib.lbfgsb_b200_server_wait(self.handle, rid, C.byref(summ), C.byref(st),
+                                              C.byref(lat), C.byref(q))
+        if rc != 0:
+            raise RuntimeError(self.lib.lbfgsb_b200_last_error().decode())
+        return st.value, summ, lat.value, q.value
+
+    def peak(self):
+        b = C.c_ulonglong()
+        r = C.c_int()
+        self.lib.lbfgsb_b200_server_peak(self.handle, C.byref(b), C.byref(r))
+        return b.value, r.value
+
+    def close(self):
+        if self.handle:
+            self.lib.lbfgsb_b200_server_destroy(self.handle)
+            self.handle = None
 
 
 class DsscfgObjective:
