@@ -581,7 +581,8 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const
     };
     const bool need_row = updatd && col > 0;
     run_stages<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
-                     &st->device_error, [&](const unsigned char* buf, long long t, int valid) {
+                     &st->device_error, [&](const unsigned char* buf, long long t, int valid,
+                                            auto release) {
       if (role == 0) {
   #pragma unroll
         for (int h = 0; h < kTile / (32 * kRole0Warps); h++)
@@ -591,6 +592,7 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const
         for (int h = 0; h < kTile / (32 * kRole12Warps); h++)
           rowprod(buf, valid, rt + h * 32 * kRole12Warps);
       }
+      release();
     });
   });
   // the free-set hash sums mod 2^64 (order free), one atomic per warp
@@ -780,6 +782,14 @@ __device__ void lnsrlb_start(DevState<S>* st, const double* red) {
   }
 }
 
+// One variable's inputs to the direction pass, read from the stage into registers.
+template <typename R, typename S>
+struct DirElem {
+  int code, nb;
+  R x, g, l, u;
+  S yv[kMaxM], sv[kMaxM];
+};
+
 // ------------------------------------------------------------------------------------
 // C: subspace direction on the free set and the step to the first bound it meets.
 template <typename R, typename H, typename S, int CONS>
@@ -829,30 +839,42 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c, const R
   const int cap = stage_capacity(StageBytes<R>::dir, 0, st->m, (int)sizeof(H));
   dispatch_cols(col, [&](auto cols_tag) {
     constexpr bool kFull = decltype(cols_tag)::value == kMaxM;
-    run_tiles<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
+    // each thread reads its variable's inputs and history row into registers and the stage
+    // is released before the arithmetic, so that the producer refills it sooner
+    run_tiles_split<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
               &st->device_error, [&](const unsigned char* buf, long long t, int valid, int e) {
+      DirElem<R, S> v{};
+      if (e < valid) {
+        v.code = stage_at<int8_t>(buf, o_code, e);
+        v.x = stage_at<R>(buf, o_x, e);
+        v.g = stage_at<R>(buf, o_g, e);
+        v.l = stage_at<R>(buf, o_l, e);
+        v.u = stage_at<R>(buf, o_u, e);
+        v.nb = stage_at<int>(buf, o_nb, e);
+        if (uncon || iw_free(v.code)) {
+  #pragma unroll
+          for (int j = 0; j < kMaxM; j++) {
+            v.yv[j] = (kFull || j < col) ? (S)hist_at<H>(buf, hy + j * hb, e) : S(0);
+            v.sv[j] = (kFull || j < col) ? (S)hist_at<H>(buf, hs + j * hb, e) : S(0);
+          }
+        }
+      }
+      return v;
+    }, [&](const DirElem<R, S>& v, long long t, int valid, int e) {
       if (e >= valid) return;
       const long long i = t * kTile + e;
-      const int code = stage_at<int8_t>(buf, o_code, e);
+      const int code = v.code;
       if (!(uncon || iw_free(code))) {
         if (!spec) return;
         // an active variable: z is its Cauchy point
-        const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
-        const R li = stage_at<R>(buf, o_l, e), ui = stage_at<R>(buf, o_u, e);
-        const R zi = gcp_point<R, S>(code, xi, gi, li, ui, tsum);
+        const R zi = gcp_point<R, S>(code, v.x, v.g, v.l, v.u, tsum);
         z[i] = zi;
-        lnsrlb_elem<R>(zi, xi, gi, li, ui, stage_at<int>(buf, o_nb, e), want_stpmx, i, sl[0],
-                       sl[1], mn[1]);
+        lnsrlb_elem<R>(zi, v.x, v.g, v.l, v.u, v.nb, want_stpmx, i, sl[0], sl[1], mn[1]);
         return;
       }
-      S yv[kMaxM], sv[kMaxM];
-  #pragma unroll
-      for (int j = 0; j < kMaxM; j++) {
-        yv[j] = (kFull || j < col) ? (S)hist_at<H>(buf, hy + j * hb, e) : S(0);
-        sv[j] = (kFull || j < col) ? (S)hist_at<H>(buf, hs + j * hb, e) : S(0);
-      }
-      const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
-      const R li = stage_at<R>(buf, o_l, e), ui = stage_at<R>(buf, o_u, e);
+      const S(&yv)[kMaxM] = v.yv;
+      const S(&sv)[kMaxM] = v.sv;
+      const R xi = v.x, gi = v.g, li = v.l, ui = v.u;
       const R zi = uncon ? xi : gcp_point<R, S>(code, xi, gi, li, ui, tsum);
       S d = reduced_grad<R, S>(uncon, xi, zi, gi, kFull ? kMaxM : col, yv, sv, a1, a2);
       // ... + wy*wv(jy)/theta + ws*wv(js), then d/theta (1472-1483): the divisions by the
@@ -865,7 +887,7 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c, const R
       const R dr = (R)d;
       c.dsub[i] = dr;
       // candidate step to the bound (1486-1516), filtered as for alpha = 1
-      const int nb = stage_at<int>(buf, o_nb, e);
+      const int nb = v.nb;
       const S dk = (S)dr;
       if (nb != 0) {
         double cand = INFINITY;
@@ -1453,7 +1475,7 @@ __global__ void __launch_bounds__(CONS + 32) k_post_gcp(Ctx<R, H, S> c, const R*
     };
     run_stages<CONS>(ss, n, c.stages, dyn,
                      reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap), &st->device_error,
-                     [&](const unsigned char* buf, long long tt, int valid) {
+                     [&](const unsigned char* buf, long long tt, int valid, auto release) {
       if (role == 0) {
 #pragma unroll
         for (int h = 0; h < kTile / kRoleThreads; h++) post_elem(buf, tt, valid, rt + h * kRoleThreads);
@@ -1461,6 +1483,7 @@ __global__ void __launch_bounds__(CONS + 32) k_post_gcp(Ctx<R, H, S> c, const R*
 #pragma unroll
         for (int h = 0; h < kTile / kRoleThreads; h++) gcp_elem(buf, tt, valid, rt + h * kRoleThreads);
       }
+      release();
     });
   });
   // CTA row: [ role P sums (19) | role G sums (21) | role P max | role G max | min pair ]

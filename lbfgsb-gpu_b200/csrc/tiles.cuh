@@ -135,7 +135,10 @@ constexpr int kMaxStages = 8;
 // body(buf, t, valid) once per tile.  full[s] completes when the bytes of the tile in
 // stage s have landed; empty[s] completes when every consumer warp has finished with it.
 // There is no CTA-wide barrier per tile, and the producer issues a freed stage's next
-// tile while the consumers work on the other stages.  body must not contain block-level
+// tile while the consumers work on the other stages.  body(buf, t, valid, release) must
+// call release() exactly once, with the whole warp, after its last read of the stage
+// buffer; a body that reads its data into registers first can release the stage before it
+// computes, so that the producer refills it sooner.  body must not contain block-level
 // barriers nor write the stage buffer.  Every wait is bounded; on a timeout the CTA sets
 // *err and leaves the loop (returns false).
 template <int CONSUMERS, typename Body>
@@ -186,9 +189,10 @@ __device__ __forceinline__ bool run_stages(const StreamSet& ss, long long n, int
         break;
       }
       const int valid = t * kTile + kTile <= n ? kTile : (int)(n - t * kTile);
-      body(buf, t, valid);
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[s]);
+      body(buf, t, valid, [&] {
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+      });
     }
   }
   __syncthreads();
@@ -215,10 +219,27 @@ __device__ __forceinline__ bool run_tiles(const StreamSet& ss, long long n, int 
                                           unsigned char* ring, uint64_t* bars, int* err,
                                           Body&& body) {
   return run_stages<CONSUMERS>(ss, n, stages, ring, bars, err,
-                               [&](const unsigned char* buf, long long t, int valid) {
+                               [&](const unsigned char* buf, long long t, int valid, auto release) {
 #pragma unroll
     for (int h = 0; h < kTile / CONSUMERS; h++)
       body(buf, t, valid, (int)threadIdx.x + h * CONSUMERS);
+    release();
+  });
+}
+
+// run_tiles in two phases: load(buf, t, valid, e) reads element e of the tile into a value
+// (registers), the stage is released, then compute(value, t, valid, e) runs.
+template <int CONSUMERS, typename Load, typename Compute>
+__device__ __forceinline__ bool run_tiles_split(const StreamSet& ss, long long n, int stages,
+                                                unsigned char* ring, uint64_t* bars, int* err,
+                                                Load&& load, Compute&& compute) {
+  static_assert(kTile == CONSUMERS, "one element per consumer thread and tile");
+  return run_stages<CONSUMERS>(ss, n, stages, ring, bars, err,
+                               [&](const unsigned char* buf, long long t, int valid, auto release) {
+    const int e = (int)threadIdx.x;
+    const auto v = load(buf, t, valid, e);
+    release();
+    compute(v, t, valid, e);
   });
 }
 
