@@ -117,38 +117,65 @@ __device__ __forceinline__ bool last_cta(unsigned int* ticket) {
 // Final fold in the last CTA: out[k] for the `width` columns of part[0..rows).  Sums
 // for k < ns and k >= ns + nx + 2*nm (lane-owned block), max for the next nx columns,
 // min pairs for the next 2*nm columns.  Warps take columns round robin; lanes stride over
-// rows; a fixed butterfly finishes each column.
+// rows; a fixed butterfly finishes each column.  A warp works on kFoldCols of its columns
+// at once (their loads of a row are independent), so that the fold waits about one
+// memory round trip per kFoldCols columns; each column's operations and their order do
+// not depend on that grouping.
+constexpr int kFoldCols = 4;
 template <int NT>
 __device__ __forceinline__ void fold_rows(const double* part, int rows, int width, int ns,
                                           int nx, int nm, double* out) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int kWarps = NT / 32;
-  for (int k = warp; k < width; k += kWarps) {
-    const bool is_max = (k >= ns && k < ns + nx);
-    const bool is_min = (k >= ns + nx && k < ns + nx + 2 * nm);
-    if (is_min) {
-      if (((k - ns - nx) & 1) != 0) continue;  // handled with its value column
-      MinPair a = {INFINITY, kNoIndex};
-      for (int r = lane; r < rows; r += 32)
-        a = minpair(a, MinPair{part[(size_t)r * width + k], (long long)part[(size_t)r * width + k + 1]});
-      a = warp_min(a);
-      if (lane == 0) {
-        out[k] = a.v;
-        out[k + 1] = (double)a.i;
+  // column kinds: 0 sum, 1 max, 2 min pair (value column; the index is the next one),
+  // 3 nothing (past the end, or the index column of a min pair)
+  auto kind_of = [&](int k) {
+    if (k >= width) return 3;
+    if (k >= ns && k < ns + nx) return 1;
+    if (k >= ns + nx && k < ns + nx + 2 * nm) return ((k - ns - nx) & 1) ? 3 : 2;
+    return 0;
+  };
+  for (int k0 = warp; k0 < width; k0 += kWarps * kFoldCols) {
+    int kind[kFoldCols];
+    double acc[kFoldCols];
+    MinPair mp[kFoldCols];
+#pragma unroll
+    for (int u = 0; u < kFoldCols; u++) {
+      kind[u] = kind_of(k0 + u * kWarps);
+      acc[u] = kind[u] == 1 ? -INFINITY : 0.0;
+      mp[u] = MinPair{INFINITY, kNoIndex};
+    }
+    for (int r = lane; r < rows; r += 32) {
+      const double* row = part + (size_t)r * width;
+#pragma unroll
+      for (int u = 0; u < kFoldCols; u++) {
+        const int k = k0 + u * kWarps;
+        if (kind[u] == 0) {
+          acc[u] += row[k];
+        } else if (kind[u] == 1) {
+          const double v = row[k];
+          acc[u] = (v > acc[u]) ? v : acc[u];
+        } else if (kind[u] == 2) {
+          mp[u] = minpair(mp[u], MinPair{row[k], (long long)row[k + 1]});
+        }
       }
-    } else if (is_max) {
-      double a = -INFINITY;
-      for (int r = lane; r < rows; r += 32) {
-        double v = part[(size_t)r * width + k];
-        a = (v > a) ? v : a;
+    }
+#pragma unroll
+    for (int u = 0; u < kFoldCols; u++) {
+      const int k = k0 + u * kWarps;
+      if (kind[u] == 0) {
+        const double a = warp_sum(acc[u]);
+        if (lane == 0) out[k] = a;
+      } else if (kind[u] == 1) {
+        const double a = warp_max(acc[u]);
+        if (lane == 0) out[k] = a;
+      } else if (kind[u] == 2) {
+        const MinPair a = warp_min(mp[u]);
+        if (lane == 0) {
+          out[k] = a.v;
+          out[k + 1] = (double)a.i;
+        }
       }
-      a = warp_max(a);
-      if (lane == 0) out[k] = a;
-    } else {
-      double a = 0;
-      for (int r = lane; r < rows; r += 32) a += part[(size_t)r * width + k];
-      a = warp_sum(a);
-      if (lane == 0) out[k] = a;
     }
   }
   __syncthreads();
