@@ -37,6 +37,28 @@ def test_workspace_bound_covers_the_solve_arrays():
     assert lib.lbfgsb_b200_workspace_bytes(4096, 4, 2) < lib.lbfgsb_b200_workspace_bytes(4096, 4, 1)
 
 
+def test_server_calls_reject_bad_arguments():
+    LB = _lib()
+    lib = LB.load()
+    opt = LB.default_option(np.float32)
+    rid = C.c_longlong(-1)
+    assert lib.lbfgsb_b200_server_submit_f32(None, 10, None, None, None, None, C.byref(opt),
+                                             None, None, C.byref(rid)) == 1
+    assert rid.value == -1
+    summ = LB.SummaryF32()
+    st = C.c_int(-5)
+    lat = C.c_double()
+    q = C.c_double()
+    assert lib.lbfgsb_b200_server_wait(None, 0, C.byref(summ), C.byref(st), C.byref(lat),
+                                       C.byref(q)) == 1
+    assert lib.lbfgsb_b200_server_peak(None, None, None) == 1
+    assert lib.lbfgsb_b200_server_destroy(None) == 1
+    h = C.c_void_p()
+    # a bad precision form or a null out-pointer is refused before any device call
+    assert lib.lbfgsb_b200_server_create(2, 1 << 30, 7, C.byref(h)) == 1 and not h.value
+    assert lib.lbfgsb_b200_server_create(2, 1 << 30, 1, None) == 1
+
+
 def _setup(dtype=np.float32):
     import torch
     import synth
