@@ -297,9 +297,9 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
   Launcher L(stream, profile);
   bool fused = false;  // the post-evaluation pass runs the next Cauchy scan (k_post_gcp)
   long long syncs = 0, evals = 0;
-  // direction passes that wrote the speculative z, and those that also applied the step
-  // (k_subsm_apply then returned at once): for the per-launch byte counts of the stats
-  long long dir_spec = 0, dir_applied = 0;
+  // direction passes that wrote the speculative z: for the per-launch byte counts of the
+  // stats
+  long long dir_spec = 0;
   int prev_no_spec = 0;
   try {
     const size_t N = (size_t)n;
@@ -464,10 +464,16 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
             c.stages = p_dir.stages;
             k_subsm_dir<R, H, S, kConsWide><<<p_dir.grid, p_dir.threads, p_dir.smem, stream>>>(c, xcur, gcur, zb);
           });
-          L.run(KID_SUBAPPLY, [&] {
-            c.stages = p_apply.stages;
-            k_subsm_apply<R, H, S, kConsWide><<<p_apply.grid, p_apply.threads, p_apply.smem, stream>>>(c, xcur, gcur, zb);
-          });
+          // the direction pass applies an untruncated step itself (spec_apply); the apply
+          // pass runs only when it has work, which the host learns from the state
+          pull();
+          if (!(hs.gcp_state == GCP_WALK || hs.internal_fail != 0 || hs.spec_apply)) {
+            L.run(KID_SUBAPPLY, [&] {
+              c.stages = p_apply.stages;
+              k_subsm_apply<R, H, S, kConsWide><<<p_apply.grid, p_apply.threads, p_apply.smem, stream>>>(c, xcur, gcur, zb);
+            });
+            pull();
+          }
         };
         if (!uncon && start_here) {
           L.run(KID_GCP, [&] {
@@ -478,12 +484,10 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
         auto count_dir = [&]() {
           if (hs.subsm_active && hs.gcp_state != GCP_WALK && hs.internal_fail == 0) {
             if (!prev_no_spec) dir_spec++;
-            if (hs.spec_apply) dir_applied++;
             prev_no_spec = hs.dir_no_spec;
           }
         };
         subspace();
-        pull();
         count_dir();
         if (hs.gcp_state == GCP_WALK && hs.internal_fail == 0) {
           if (!c.wl_t) {
@@ -500,7 +504,6 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
           });
           L.run(KID_WALK, [&] { k_walk<R, H, S><<<1, kWalkThreads, 0, stream>>>(c, xcur, gcur); });
           subspace();
-          pull();
           count_dir();
         }
         if (hs.internal_fail != 0) {  // cauchy/formk/cmprlb/subsm failed: reset (297-341)
@@ -670,13 +673,10 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
     st.bytes[KID_GCP] = nn * (4 * Rb + 4 + hist + 1);
     st.bytes[KID_FREEV] = nn * (2 * Rb + hist + 1 + 0.25);
     // per launch, averaged over the launches made: the direction pass writes z when it
-    // speculates; k_subsm_apply does its work only when the direction pass did not apply
-    // the step
+    // speculates; k_subsm_apply is launched only for the steps it applies
     const double ndir = std::max<double>(1.0, (double)g_last_stats.launches[KID_SUBDIR]);
-    const double napp = (double)g_last_stats.launches[KID_SUBAPPLY];
     st.bytes[KID_SUBDIR] = nn * (5 * Rb + hist + 5 + Rb * (double)dir_spec / ndir);
-    st.bytes[KID_SUBAPPLY] =
-        napp > 0 ? nn * (6 * Rb + 5) * std::max(0.0, napp - (double)dir_applied) / napp : 0.0;
+    st.bytes[KID_SUBAPPLY] = nn * (6 * Rb + 5);
     st.bytes[KID_POST] = nn * (6 * Rb + 4 + hist + 2 * Hb);
     st.bytes[KID_POSTGCP] = nn * (6 * Rb + 4 + hist + 2 * Hb + 1);
     st.bytes[KID_TRIAL] = nn * 3 * Rb;
@@ -685,7 +685,8 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
     st.bytes[KID_INIT] = nn * (4 * Rb + 4);
     st.bytes_per_iteration_model =
         (fused ? st.bytes[KID_POSTGCP] : st.bytes[KID_POST] + st.bytes[KID_GCP]) +
-        st.bytes[KID_FREEV] + st.bytes[KID_SUBDIR] + st.bytes[KID_SUBAPPLY];  // averaged
+        st.bytes[KID_FREEV] + st.bytes[KID_SUBDIR] +
+        st.bytes[KID_SUBAPPLY] * (double)g_last_stats.launches[KID_SUBAPPLY] / ndir;  // averaged
   } catch (const CudaFailure& e) {
     char buf[256];
     std::snprintf(buf, sizeof(buf), "%s failed at driver.cu:%d: %s", e.call, e.line,
