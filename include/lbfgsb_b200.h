@@ -157,7 +157,9 @@ unsigned long long lbfgsb_b200_workspace_bytes(int n, int real_size, int form);
  * for admission; a request's result equals what the same solve gives through
  * lbfgsb_b200_minimize_ext_f32 with that form.  lbfgsb_b200_server_peak reports the most
  * workspace bytes and the most solves that were admitted at once.
- * lbfgsb_b200_server_destroy finishes every queued request, then stops the workers. */
+ * lbfgsb_b200_server_destroy finishes every queued request, then stops the workers and
+ * frees the server: no other call on the server may overlap it or follow it.  Submit, wait
+ * and peak may be called from any threads. */
 typedef struct lbfgsb_b200_server lbfgsb_b200_server;
 int lbfgsb_b200_server_create(int workers, unsigned long long hbm_budget_bytes, int form,
                               lbfgsb_b200_server** server);
