@@ -199,6 +199,10 @@ typedef struct {
   int profile;                        /* 1: time every kernel with CUDA events */
   lbfgsb_b200_trace_callback trace;   /* may be NULL */
   void* trace_user;
+  /* 1: the L-BFGS-B 3.0 subspace step (Morales and Nocedal, ACM TOMS 38(1), 2011): the
+   * subspace minimizer projected onto the box when that gives a descent direction, else
+   * the 2.1 step truncated at the first bound.  0 (default): the reference's 2.1 step. */
+  int subsm_projection;
 } lbfgsb_b200_ext;
 
 int lbfgsb_b200_minimize_ext_f64(int n, double* x, const int* nbd, const double* l,

@@ -390,6 +390,7 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
     std::memset(&hs, 0, sizeof(hs));
     hs.n = n;
     hs.m = m;
+    hs.subsm_proj = (ext && ext->subsm_projection) ? 1 : 0;
     hs.boxed = 1;
     hs.head = 1;
     hs.theta = 1;

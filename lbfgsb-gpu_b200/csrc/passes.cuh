@@ -814,8 +814,11 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c, const R
   MinPair mn[2] = {MinPair{INFINITY, kNoIndex}, MinPair{INFINITY, kNoIndex}};
   double sl[2] = {0.0, 0.0};
   const bool want_stpmx = st->cnstnd && st->iter > 0;
-  // speculate unless the last step was truncated (then this one likely is too)
-  const bool spec = st->dir_no_spec == 0;
+  // speculate unless the last step was truncated (then this one likely is too); the 3.0
+  // step always needs the projected point
+  const bool proj = st->subsm_proj != 0;
+  const bool spec = proj || st->dir_no_spec == 0;
+  double projected = 0.0;  // 1 if the 3.0 projection put a variable on a bound
   const FixedDiv<S> divt(theta);
 
   extern __shared__ __align__(128) unsigned char dyn[];
@@ -911,40 +914,52 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c, const R
         }
         if (!skip) mn[0] = minpair(mn[0], MinPair{cand, i});
       }
-      // the subspace step with alpha = 1 (1517-1533): z = xcp + d
+      // the subspace step with alpha = 1 (1517-1533): z = xcp + d; with the 3.0 step,
+      // projected onto the box (the lower bound, then the upper one)
       if (spec) {
-        const R zs = (R)((S)zi + dk);
+        R zs = (R)((S)zi + dk);
+        if (proj) {
+          const bool lo = nb == 1 || nb == 2, hi = nb == 2 || nb == 3;
+          if (lo) zs = li > zs ? li : zs;
+          if (hi) zs = ui > zs ? zs : ui;
+          if ((lo && zs == li) || (hi && zs == ui)) projected = 1.0;
+        }
         z[i] = zs;
         lnsrlb_elem<R>(zs, xi, gi, li, ui, nb, want_stpmx, i, sl[0], sl[1], mn[1]);
       }
     });
   });
-  // row: [ d'd, g'd | alpha candidate (value, index) | stpmx candidate (value, index) ]
-  constexpr int W = 6;
-  double xdum[1] = {0.0}, ldum[1] = {0.0};
-  cta_reduce_to_row<CONS + 32, 2, 0, 2, 0>(sl, xdum, mn, ldum, c.part, W);
+  // row: [ d'd, g'd | projected | alpha candidate (value, index) | stpmx candidate
+  // (value, index) ]
+  constexpr int W = 7;
+  double xm[1] = {projected}, ldum[1] = {0.0};
+  cta_reduce_to_row<CONS + 32, 2, 1, 2, 0>(sl, xm, mn, ldum, c.part, W);
   if (!last_cta(c.ticket)) return;
   __shared__ double red[W];
   __shared__ double rl[3];
-  fold_rows<CONS + 32>(c.part, gridDim.x, W, 2, 0, 2, red);
+  fold_rows<CONS + 32>(c.part, gridDim.x, W, 2, 1, 2, red);
   epilogue_on_shared<S>(st, [&](DevState<S>* st) {
-    const S cand = (S)red[2];
-    if (cand < S(1)) {
+    // the 3.0 step keeps the projected point when it gives a descent direction from x
+    // (g'd <= 0 over the written z); otherwise, and always with the 2.1 step, the step is
+    // truncated at the first bound when one is met before alpha = 1
+    const bool keep_projection = proj && red[2] > 0.0 && red[1] <= 0.0;
+    const S cand = (S)red[3];
+    if (!keep_projection && cand < S(1)) {
       st->alpha = cand;
-      st->ibd = (int)red[3];
+      st->ibd = (int)red[4];
       st->iword = 1;
-      st->dir_no_spec = 1;
+      st->dir_no_spec = proj ? 0 : 1;
       return;  // truncated: k_subsm_apply applies the step
     }
     st->alpha = 1;
     st->ibd = -1;
-    st->iword = 0;
+    st->iword = keep_projection ? 1 : 0;
     st->dir_no_spec = 0;
     if (!spec) return;  // k_subsm_apply applies the step
-    // not truncated: the step written above is the subspace point; start the line search
+    // the step written above is the subspace point; start the line search
     rl[0] = red[0];
     rl[1] = red[1];
-    rl[2] = red[4];
+    rl[2] = red[5];
     lnsrlb_start<S>(st, rl);
     st->spec_apply = 1;
   });

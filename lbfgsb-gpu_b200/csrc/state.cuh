@@ -32,6 +32,7 @@ struct DevState {
   int spec_gcp;       // 1: the post-evaluation pass also ran the next Cauchy scan
   int spec_apply;     // 1: the direction pass also applied the (untruncated) step
   int dir_no_spec;    // 1 after a truncated step: the next direction pass does not try
+  int subsm_proj;     // 1: the L-BFGS-B 3.0 subspace step (projection), 0: the 2.1 step
   unsigned long long free_hash, free_hash_acc, at_lower, at_upper;
   S theta, f, fold, gd, gdold, stp, dnrm, dtd, xstep, stpmx;
   S sbgnrm, tf, rr, dr, ddum_dr;

@@ -63,7 +63,7 @@ TRACE_CB = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(TraceRecord))
 
 class Ext(C.Structure):
     _fields_ = [("form", C.c_int), ("profile", C.c_int), ("trace", TRACE_CB),
-                ("trace_user", C.c_void_p)]
+                ("trace_user", C.c_void_p), ("subsm_projection", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -328,8 +328,12 @@ _TRACE_KEYS = [f for f, _ in TraceRecord._fields_]
 
 def solve(prob: dict, dtype=np.float64, x0=None, option=None, objective: str = "host",
           form: int = FORM_PLAIN, trace: bool = False, record: bool = True,
-          custom_stop_at: int | None = None, profile: bool = False, stream=None) -> GpuResult:
+          custom_stop_at: int | None = None, profile: bool = False, stream=None,
+          subsm_projection: bool = False) -> GpuResult:
     """One solve on the GPU through the C ABI.
+
+    subsm_projection: the L-BFGS-B 3.0 subspace step (lbfgsb_b200_ext.subsm_projection)
+    instead of the reference's 2.1 step.
 
     objective="host": funcgrad copies x to the host and evaluates the CPU objective of
     oracle/objective.c (so f and g are bit-identical to what the oracle sees);
@@ -413,7 +417,7 @@ def solve(prob: dict, dtype=np.float64, x0=None, option=None, objective: str = "
 
     cb_tr = TRACE_CB(tr) if trace else TRACE_CB()
     keep.append(cb_tr)
-    ext = Ext(form, 1 if profile else 0, cb_tr, None)
+    ext = Ext(form, 1 if profile else 0, cb_tr, None, 1 if subsm_projection else 0)
     sfx = "f64" if is64 else "f32"
     fn = getattr(lib, f"lbfgsb_b200_minimize_ext_{sfx}")
     torch.cuda.synchronize()

@@ -212,8 +212,9 @@ def dsscfg_start(prob: dict, dtype, source: str = "oracle") -> np.ndarray:
 
 def run_cpu(which: str, prob: dict, dtype=np.float64, x0=None, option=None, record=True,
             trace=False, custom_stop_at: int | None = None,
-            objective_source: str = "oracle") -> RunResult:
-    """Run the oracle ('oracle') or the reference build ('ref') on a synthetic problem."""
+            objective_source: str = "oracle", subsm_projection: bool = False) -> RunResult:
+    """Run the oracle ('oracle') or the reference build ('ref') on a synthetic problem.
+    subsm_projection: the oracle's L-BFGS-B 3.0 subspace step (the reference has only 2.1)."""
     dtype = np.dtype(dtype)
     is64 = dtype == np.float64
     real = C.c_double if is64 else C.c_float
@@ -254,11 +255,18 @@ def run_cpu(which: str, prob: dict, dtype=np.float64, x0=None, option=None, reco
 
     sfx = "f64" if is64 else "f32"
     P = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
+    if subsm_projection and which != "oracle":
+        raise ValueError("the reference build has only the 2.1 subspace step")
     if which == "oracle":
-        fn = getattr(oracle_lib(), f"orc_lbfgsb_minimize_{sfx}")
+        lib = oracle_lib()
+        fn = getattr(lib, f"orc_lbfgsb_minimize_{sfx}")
         cb_tr = TRACE_CB(tr) if trace else TRACE_CB()
-        fn(n, P(x, real), P(nbd, C.c_int), P(l, real), P(u, real), C.byref(opt), cb_fg,
-           cb_after, cb_stop, None, cb_tr, None, C.byref(summ))
+        lib.orc_set_subsm_projection(1 if subsm_projection else 0)
+        try:
+            fn(n, P(x, real), P(nbd, C.c_int), P(l, real), P(u, real), C.byref(opt), cb_fg,
+               cb_after, cb_stop, None, cb_tr, None, C.byref(summ))
+        finally:
+            lib.orc_set_subsm_projection(0)
     elif which == "ref":
         fn = getattr(ref_lib(), f"ref_lbfgsb_minimize_{sfx}")
         fn(n, P(x, real), P(nbd, C.c_int), P(l, real), P(u, real), C.byref(opt), cb_fg,

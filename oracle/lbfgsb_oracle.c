@@ -17,6 +17,10 @@
 
 #include "oracle_api.h"
 
+/* Test switch for the L-BFGS-B 3.0 subspace step (see subsm); off = the reference's 2.1. */
+static int g_subsm_projection = 0;
+void orc_set_subsm_projection(int on) { g_subsm_projection = on ? 1 : 0; }
+
 /* lbfgsbdefaultoption, culbfgsb/lbfgsb.cpp:43-66 */
 void orc_default_option_f64(orc_option_f64* o) {
   o->eps_f = o->eps_g = o->eps_x = 1e-15;

@@ -684,14 +684,14 @@ static void FN(cmprlb)(int n, int m, const REAL* x, const REAL* g, const REAL* w
 }
 
 /* lbfgsbsubsm, lbfgsbcpu.cpp:1416-1539: subspace Newton step on the free set, then the
- * L-BFGS-B 2.1 truncation of the step at the first bound it meets.  x here is xcp. */
+ * L-BFGS-B 2.1 truncation of the step at the first bound it meets.  x here is xcp; xx and
+ * gg are the iterate and its gradient, used by the 3.0 option only. */
 static void FN(subsm)(int n, int m, int nsub, const int* ind, const REAL* l,
                       const REAL* u, const int* nbd, REAL* x, REAL* d, const REAL* ws,
                       const REAL* wy, REAL theta, int col, int head, int* iword, REAL* wv,
-                      REAL* wn, int* info) {
+                      REAL* wn, int* info, const REAL* xx, const REAL* gg) {
   int pointr, col2, ibd = 0, jy, js, i, j, k;
   REAL alpha, dk, temp1, temp2;
-  (void)n;
   if (nsub <= 0) return;
   pointr = head;
   for (i = 1; i <= col; i++) {
@@ -723,6 +723,40 @@ static void FN(subsm)(int n, int m, int nsub, const int* ind, const REAL* l,
     pointr = pointr % m + 1;
   }
   for (i = 1; i <= nsub; i++) V1(d, i) = V1(d, i) / theta;
+  if (g_subsm_projection) {
+    /* L-BFGS-B 3.0 (J. L. Morales and J. Nocedal, "Remark on Algorithm 778", ACM TOMS
+     * 38(1), 2011): project xcp + d onto the box, variable by variable (the lower bound,
+     * then the upper one).  If no variable lands on a bound, that is the step; if some do,
+     * keep the projected point when (x_p - xx)'gg <= 0, a descent direction from the
+     * iterate, and otherwise fall back to the 2.1 truncated step below. */
+    int projected = 0;
+    REAL ddp = 0;
+    REAL* keep = (REAL*)malloc(sizeof(REAL) * (size_t)(nsub + 1));
+    for (i = 1; i <= nsub; i++) {
+      const int lo = V1(nbd, V1(ind, i)) == 1 || V1(nbd, V1(ind, i)) == 2;
+      const int hi = V1(nbd, V1(ind, i)) == 2 || V1(nbd, V1(ind, i)) == 3;
+      k = V1(ind, i);
+      V1(keep, i) = V1(x, k);
+      temp1 = V1(x, k) + V1(d, i);
+      if (lo) temp1 = FN(maxr)(V1(l, k), temp1);
+      if (hi) temp1 = FN(minr)(V1(u, k), temp1);
+      if ((lo && temp1 == V1(l, k)) || (hi && temp1 == V1(u, k))) projected = 1;
+      V1(x, k) = temp1;
+    }
+    if (!projected) {
+      free(keep);
+      *iword = 0;
+      return;
+    }
+    for (i = 1; i <= n; i++) ddp = ddp + (V1(x, i) - V1(xx, i)) * V1(gg, i);
+    if (ddp <= 0) {
+      free(keep);
+      *iword = 1;
+      return;
+    }
+    for (i = 1; i <= nsub; i++) V1(x, V1(ind, i)) = V1(keep, i);
+    free(keep);
+  }
   /* step length to the first bound (temp1 carries across variables, as in the source) */
   alpha = 1;
   temp1 = alpha;
@@ -1228,7 +1262,7 @@ void CAT2(orc_lbfgsb_minimize, SFX)(int n, REAL* x_, const int* nbd_, const REAL
                  &internalinfo, work, work2);
       if (internalinfo == 0)
         FN(subsm)(n, m, nfree, index, l, u, nbd, z, r, ws, wy, theta, col, head, &iword, wa,
-                  wn, &internalinfo);
+                  wn, &internalinfo, x, g);
       if (internalinfo != 0) {
         internalinfo = 0;
         col = 0;

@@ -86,6 +86,10 @@ void orc_lbfgsb_minimize_f32(int n, float* x, const int* nbd, const float* l,
                              orc_cb_f32 custom_stop, void* user,
                              orc_trace_cb trace, void* trace_user,
                              orc_summary_f32* summary);
+/* 1: subsm takes the L-BFGS-B 3.0 step (the projection of the subspace minimizer onto the
+ * box when that is a descent direction, else the 2.1 truncated step); 0 (default): the
+ * reference's 2.1 step.  Process-wide, for tests. */
+void orc_set_subsm_projection(int on);
 void orc_default_option_f64(orc_option_f64* opt);
 void orc_default_option_f32(orc_option_f32* opt);
 
