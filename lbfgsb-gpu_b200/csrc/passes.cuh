@@ -818,13 +818,14 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c, const R
   // step always needs the projected point
   const bool proj = st->subsm_proj != 0;
   const bool spec = proj || st->dir_no_spec == 0;
-  double projected = 0.0;  // 1 if the 3.0 projection put a variable on a bound
+  __shared__ int s_projected;  // 1 once the 3.0 projection has put a variable on a bound
   const FixedDiv<S> divt(theta);
 
   extern __shared__ __align__(128) unsigned char dyn[];
   __shared__ StreamSet ss;
   __shared__ int s_hy, s_hs;
   if (threadIdx.x == 0) {
+    s_projected = 0;
     ss.count = 0;
     ss.stage_bytes = 0;
     add_stream(ss, c.code, kTile);
@@ -922,7 +923,7 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c, const R
           const bool lo = nb == 1 || nb == 2, hi = nb == 2 || nb == 3;
           if (lo) zs = li > zs ? li : zs;
           if (hi) zs = ui > zs ? zs : ui;
-          if ((lo && zs == li) || (hi && zs == ui)) projected = 1.0;
+          if ((lo && zs == li) || (hi && zs == ui)) s_projected = 1;
         }
         z[i] = zs;
         lnsrlb_elem<R>(zs, xi, gi, li, ui, nb, want_stpmx, i, sl[0], sl[1], mn[1]);
@@ -932,7 +933,8 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c, const R
   // row: [ d'd, g'd | projected | alpha candidate (value, index) | stpmx candidate
   // (value, index) ]
   constexpr int W = 7;
-  double xm[1] = {projected}, ldum[1] = {0.0};
+  // (the pipeline ends with a block barrier, so every thread's flag store is visible)
+  double xm[1] = {s_projected ? 1.0 : 0.0}, ldum[1] = {0.0};
   cta_reduce_to_row<CONS + 32, 2, 1, 2, 0>(sl, xm, mn, ldum, c.part, W);
   if (!last_cta(c.ticket)) return;
   __shared__ double red[W];
