@@ -128,6 +128,125 @@ def make_problem(side: int, seed: int = 0):
     return synth.synth_problem(side, seed=seed)
 
 
+class Runner:
+    """Solves of one synthetic problem through the C ABI on device-resident inputs:
+    eps_f = eps_g = eps_x = 0, so a solve of `iters` iterations runs exactly that many.
+    FP32 solves subtract f0 = f(x0) (FP64) from the objective, so that a float f resolves
+    the ~1e-8 decrease of an iteration (the minimiser and g are unchanged)."""
+
+    def __init__(self, LB, lib, prob, dtype: str, form: int, dev):
+        import torch
+        self.LB, self.lib, self.dev = LB, lib, dev
+        self.is64 = dtype == "f64"
+        self.dt = np.float64 if self.is64 else np.float32
+        tdt = torch.float64 if self.is64 else torch.float32
+        self.form = form
+        if not self.is64:
+            prob = dict(prob, f_offset=LB.synth_value(prob))
+        self.prob = prob
+        self.n = prob["nbd"].size
+        self.so = LB.SynthObjective(prob, single_precision_fields=not self.is64)
+        self.fg = self.so.f64 if self.is64 else self.so.f32
+        self.x = torch.zeros(self.n, dtype=tdt, device=dev)
+        self.l = torch.from_numpy(prob["l"].astype(self.dt)).to(dev)
+        self.u = torch.from_numpy(prob["u"].astype(self.dt)).to(dev)
+        self.nbd = torch.from_numpy(prob["nbd"]).to(dev)
+        self.cbt = LB.CB64 if self.is64 else LB.CB32
+        self.summ_t = LB.SummaryF64 if self.is64 else LB.SummaryF32
+        self.minimize = lib.lbfgsb_b200_minimize_ext_f64 if self.is64 else lib.lbfgsb_b200_minimize_ext_f32
+
+    def option(self, iters):
+        o = self.LB.default_option(self.dt)
+        o.eps_f = o.eps_g = o.eps_x = 0.0
+        o.max_iteration = iters - 1  # the solve stops after iteration `iters`
+        return o
+
+    def solve(self, iters, after=None, profile=False):
+        import torch
+        self.x.zero_()
+        summ = self.summ_t()
+        ext = self.LB.Ext(self.form, 1 if profile else 0, self.LB.TRACE_CB(), None)
+        st = self.minimize(self.n, self.x.data_ptr(), self.nbd.data_ptr(), self.l.data_ptr(),
+                           self.u.data_ptr(), C.byref(self.option(iters)), self.fg, after, None,
+                           self.so.handle, None, C.byref(ext), C.byref(summ))
+        torch.cuda.synchronize()
+        if st != 0:
+            raise RuntimeError(f"status {st}: {self.lib.lbfgsb_b200_last_error()}")
+        return summ, self.LB.last_stats()
+
+    def steady_kernels(self, W, K):
+        """Per-kernel launches, summed CUDA-event ms and algorithmic bytes per launch over
+        iterations W+1 .. W+K (two profiled solves, W and W+K iterations, subtracted)."""
+        _, st_w = self.solve(W, profile=True)
+        _, st_wk = self.solve(W + K, profile=True)
+        kern = {}
+        for name, v in st_wk["kernels"].items():
+            launches = v["launches"] - st_w["kernels"][name]["launches"]
+            kms = v["ms"] - st_w["kernels"][name]["ms"]
+            if launches > 0:
+                kern[name] = {"launches": launches, "ms": kms, "bytes": v["bytes"]}
+        evals_k = st_wk["evaluations"] - st_w["evaluations"]
+        launches_k = st_wk["total_launches"] - st_w["total_launches"] + evals_k  # + objective
+        return kern, evals_k, launches_k, st_wk["bytes_per_iteration_model"]
+
+    def timed(self, W, K, dist=None, sampler=None):
+        """ms of iterations W+1 .. W+K, CUDA events recorded in the after-iteration callback
+        on the solver's stream."""
+        import torch
+        ev = {"start": torch.cuda.Event(enable_timing=True), "end": torch.cuda.Event(enable_timing=True)}
+
+        def after_cb(_user, _x, _f, _g, _stream, sp):
+            it = sp[0].num_iteration
+            if it == W:
+                torch.cuda.synchronize()
+                if dist is not None:
+                    dist.barrier()
+                ev["start"].record()
+            elif it == W + K:
+                ev["end"].record()
+                ev["end"].synchronize()
+            return 0
+
+        cb = self.cbt(after_cb)
+        if sampler is not None:
+            with sampler:
+                summ, _ = self.solve(W + K, after=C.cast(cb, C.c_void_p).value)
+        else:
+            summ, _ = self.solve(W + K, after=C.cast(cb, C.c_void_p).value)
+        torch.cuda.synchronize()
+        if summ.num_iteration != W + K:
+            raise RuntimeError(f"solve stopped early: {summ.num_iteration} iterations, info {summ.info}")
+        return ev["start"].elapsed_time(ev["end"])
+
+    def close(self):
+        self.so.close()
+
+
+def roofline_of(kern, n, hbm, hbm_kind, traffic_table=None):
+    """The dominant kernel (most summed time) with its achieved algorithmic GB/s and the
+    fraction of the HBM peak, and every kernel's share, average time and GB/s."""
+    if not kern:
+        return None, {}
+    name, v = max(kern.items(), key=lambda kv: kv[1]["ms"])
+    avg_s = v["ms"] / v["launches"] / 1000.0
+    achieved = v["bytes"] / avg_s / 1e9
+    traffic = None
+    if traffic_table and name in traffic_table.get("bytes_per_element", {}):
+        traffic = traffic_table["bytes_per_element"][name] * n
+    roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm,
+            "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+            "peak_source": hbm_kind,
+            "algorithmic_bytes_per_launch": v["bytes"], "avg_launch_ms": avg_s * 1000.0}
+    total = sum(x["ms"] for x in kern.values())
+    per_kernel = {}
+    for k, v in kern.items():
+        gbps = (v["bytes"] / (v["ms"] / v["launches"] / 1000.0) / 1e9) if v["bytes"] else None
+        per_kernel[k] = {"launches": v["launches"], "avg_ms": v["ms"] / v["launches"],
+                         "share": v["ms"] / total, "GBps": gbps,
+                         "frac": (gbps / hbm) if gbps else None}
+    return roof, per_kernel
+
+
 def run_ours(args, rank: int, world: int, dist):
     import torch
     import lbfgsb_b200 as LB
@@ -141,75 +260,21 @@ def run_ours(args, rank: int, world: int, dist):
     prob = make_problem(args.side, seed=rank)
     n = prob["nbd"].size
     W, K = args.warmup, args.steps
-
-    def option(iters):
-        o = LB.default_option(dt)
-        o.eps_f = o.eps_g = o.eps_x = 0.0
-        o.max_iteration = iters - 1  # the solve stops after iteration `iters`
-        return o
-
-    so = LB.SynthObjective(prob, single_precision_fields=not is64)
-    fg = so.f64 if is64 else so.f32
-    x = torch.zeros(n, dtype=tdt, device=dev)
-    l = torch.from_numpy(prob["l"].astype(dt)).to(dev)
-    u = torch.from_numpy(prob["u"].astype(dt)).to(dev)
-    nbd = torch.from_numpy(prob["nbd"]).to(dev)
-    cbt = LB.CB64 if is64 else LB.CB32
-    summ_t = LB.SummaryF64 if is64 else LB.SummaryF32
-    minimize = lib.lbfgsb_b200_minimize_ext_f64 if is64 else lib.lbfgsb_b200_minimize_ext_f32
-
-    def solve(iters, after=None, profile=False):
-        x.zero_()
-        summ = summ_t()
-        ext = LB.Ext(0, 1 if profile else 0, LB.TRACE_CB(), None)
-        st = minimize(n, x.data_ptr(), nbd.data_ptr(), l.data_ptr(), u.data_ptr(),
-                      C.byref(option(iters)), fg, after, None, so.handle, None, C.byref(ext),
-                      C.byref(summ))
-        torch.cuda.synchronize()
-        if st != 0:
-            raise RuntimeError(f"status {st}: {lib.lbfgsb_b200_last_error()}")
-        return summ, LB.last_stats()
+    run = Runner(LB, lib, prob, args.dtype, args.form if not is64 else 0, dev)
+    prob = run.prob
+    option = run.option
 
     # warm the whole path once (allocator pool, module load)
-    solve(2)
+    run.solve(2)
 
     # ---- headline: K iterations after W, timed between after-iteration callbacks ----
-    ev = {"start": torch.cuda.Event(enable_timing=True), "end": torch.cuda.Event(enable_timing=True)}
-
-    def after_cb(_user, _x, _f, _g, _stream, sp):
-        it = sp[0].num_iteration
-        if it == W:
-            torch.cuda.synchronize()
-            if dist is not None:
-                dist.barrier()
-            ev["start"].record()
-        elif it == W + K:
-            ev["end"].record()
-            ev["end"].synchronize()
-        return 0
-
-    cb = cbt(after_cb)
     sampler = ClockSampler(dev.index)
-    with sampler:
-        summ, st_plain = solve(W + K, after=C.cast(cb, C.c_void_p).value)
-    torch.cuda.synchronize()
+    ms = run.timed(W, K, dist=dist, sampler=sampler)
     if dist is not None:
         dist.barrier()
-    ms = ev["start"].elapsed_time(ev["end"])
-    if summ.num_iteration != W + K:
-        raise RuntimeError(f"solve stopped early: {summ.num_iteration} iterations, info {summ.info}")
 
     # ---- per-kernel device times of the K steady-state iterations (profiled runs) ----
-    _, st_w = solve(W, profile=True)
-    _, st_wk = solve(W + K, profile=True)
-    kern = {}
-    for name, v in st_wk["kernels"].items():
-        launches = v["launches"] - st_w["kernels"][name]["launches"]
-        kms = v["ms"] - st_w["kernels"][name]["ms"]
-        if launches > 0:
-            kern[name] = {"launches": launches, "ms": kms, "bytes": v["bytes"]}
-    evals_k = st_wk["evaluations"] - st_w["evaluations"]
-    launches_k = st_wk["total_launches"] - st_w["total_launches"] + evals_k  # + objective
+    kern, evals_k, launches_k, model_bytes = run.steady_kernels(W, K)
 
     # ---- e2e through the C ABI from pinned host buffers ----
     hx = torch.zeros(n, dtype=tdt).pin_memory()
@@ -219,6 +284,7 @@ def run_ours(args, rank: int, world: int, dist):
     hout = torch.empty(n, dtype=tdt).pin_memory()
     # the objective's fields are the user's problem data, set up before the solve call
     so2 = LB.SynthObjective(prob, single_precision_fields=not is64)
+    ext2 = LB.Ext(run.form, 0, LB.TRACE_CB(), None)
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -227,10 +293,10 @@ def run_ours(args, rank: int, world: int, dist):
     dl = hl.to(dev, non_blocking=True)
     du = hu.to(dev, non_blocking=True)
     dn = hn.to(dev, non_blocking=True)
-    summ2 = summ_t()
-    st = (lib.lbfgsb_b200_minimize_f64 if is64 else lib.lbfgsb_b200_minimize_f32)(
-        n, dx.data_ptr(), dn.data_ptr(), dl.data_ptr(), du.data_ptr(), C.byref(option(K)),
-        so2.f64 if is64 else so2.f32, None, None, so2.handle, None, C.byref(summ2))
+    summ2 = run.summ_t()
+    st = run.minimize(n, dx.data_ptr(), dn.data_ptr(), dl.data_ptr(), du.data_ptr(),
+                      C.byref(option(K)), so2.f64 if is64 else so2.f32, None, None, so2.handle,
+                      None, C.byref(ext2), C.byref(summ2))
     hout.copy_(dx, non_blocking=True)
     e1.record()
     e1.synchronize()
@@ -240,14 +306,72 @@ def run_ours(args, rank: int, world: int, dist):
     so2.close()
     h2d = hx.nbytes + hl.nbytes + hu.nbytes + hn.nbytes
     d2h = hout.nbytes + 8 * summ2.num_iteration  # x and the per-evaluation f
-    so.close()
+    run.close()
 
     # ---- gather over ranks (max time) ----
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], dist, dev)
     return {"ms": ms, "kern": kern, "launches_k": launches_k, "evals_k": evals_k,
             "clocks": sampler.summary(), "e2e_ms": e2e_ms, "e2e_iters": summ2.num_iteration,
-            "h2d": h2d, "d2h": d2h, "n": n,
-            "model_bytes_iter": st_wk["bytes_per_iteration_model"]}
+            "h2d": h2d, "d2h": d2h, "n": n, "model_bytes_iter": model_bytes}
+
+
+def forms_compare(hbm, hbm_kind, sides=(4096, 2048), W=5, K=20, err_iters=300):
+    """The precision forms at n = 4096^2 and 2048^2 (the same synthetic problem, seed 0):
+    FP64 plain, FP32 plain, FP32 mixed (FP64 small-matrix, Cauchy and line-search scalars)
+    and FP32 mixed with BF16 history storage.  Per form: ms per iteration of K iterations
+    after W (CUDA events), every solver kernel's algorithmic GB/s and fraction of the HBM
+    peak over those iterations, and, after err_iters iterations of each form from the same
+    start, the FP32 forms' f, x and ||proj g||_inf against the FP64 run's."""
+    import torch
+    import lbfgsb_b200 as LB
+    lib = LB.load()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    out = {}
+    for side in sides:
+        prob = make_problem(side, seed=0)
+        rows = {}
+        ref = None
+        for key, dtype, form in (("f64_plain", "f64", 0), ("f32_plain", "f32", 0),
+                                 ("f32_mixed", "f32", 1), ("f32_mixed_bf16", "f32", 2)):
+            run = Runner(LB, lib, prob, dtype, form, dev)
+            run.solve(2)
+            ms = run.timed(W, K)
+            kern, evals_k, launches_k, _ = run.steady_kernels(W, K)
+            roof, per_kernel = roofline_of(kern, run.n, hbm, hbm_kind)
+            pg = []
+
+            def after(_u, _x, _f, _g, _s, sp):
+                pg.append(float(sp[0].residual_g))
+                return 0
+
+            cb = run.cbt(after)
+            summ, _ = run.solve(err_iters, after=C.cast(cb, C.c_void_p).value)
+            x = run.x.double().cpu().numpy()
+            row = {"ms_per_iteration": ms / K, "iters_per_s": 1000.0 * K / ms,
+                   "evaluations_per_iteration": evals_k / K,
+                   "solver_kernels_ms_per_iteration": sum(v["ms"] for v in kern.values()) / K,
+                   "kernels": per_kernel, "dominant": roof,
+                   "min_kernel_frac": min((v["frac"] for v in per_kernel.values()
+                                           if v["frac"] is not None and v["share"] > 0.05),
+                                          default=None),
+                   "after_iterations": summ.num_iteration, "info": summ.info,
+                   "proj_g_inf": pg[-1] if pg else None}
+            # f at the final x, in FP64 (the FP32 forms report f - f0)
+            fx = LB.synth_value(prob, x)
+            row["f"] = fx
+            if dtype == "f64":
+                ref = (fx, x, row["proj_g_inf"])
+            else:
+                row["vs_f64"] = {"f_rel": abs(fx - ref[0]) / max(1.0, abs(ref[0])),
+                                 "x_max_abs": float(np.max(np.abs(x - ref[1]))),
+                                 "proj_g_inf_rel": abs(row["proj_g_inf"] - ref[2]) / max(ref[2], 1e-300)}
+            rows[key] = row
+            run.close()
+        out[f"n{side}sq"] = rows
+    out["note"] = ("FP32 forms subtract f0 = f(0) (FP64) in the objective so that f resolves the "
+                   "per-iteration decrease; errors compare the iterates after the same number "
+                   "of iterations from the same start (not converged solves)")
+    return out
 
 
 def dsscfg_compare():
@@ -529,6 +653,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--side", type=int, default=4096)
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--form", type=int, default=0, choices=[0, 1, 2],
+                    help="f32 precision form: 0 plain, 1 mixed, 2 mixed with bf16 history")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -585,24 +711,7 @@ def main():
     value = job_throughput(world, K, r["ms"])
     hbm, hbm_kind = peaks()
     kern = r["kern"]
-    top = max(kern.items(), key=lambda kv: kv[1]["ms"]) if kern else None
-    roof = None
-    if top:
-        name, v = top
-        avg_s = v["ms"] / v["launches"] / 1000.0
-        achieved = v["bytes"] / avg_s / 1e9
-        tr = ncu_traffic()
-        traffic = None
-        if tr and name in tr.get("bytes_per_element", {}):
-            traffic = tr["bytes_per_element"][name] * r["n"]
-        roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm,
-                "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
-                "peak_source": hbm_kind,
-                "algorithmic_bytes_per_launch": v["bytes"], "avg_launch_ms": avg_s * 1000.0}
-    per_kernel = {k: {"launches": v["launches"], "avg_ms": v["ms"] / v["launches"],
-                      "share": v["ms"] / sum(x["ms"] for x in kern.values()),
-                      "GBps": (v["bytes"] / (v["ms"] / v["launches"] / 1000.0) / 1e9) if v["bytes"] else None}
-                  for k, v in kern.items()}
+    roof, per_kernel = roofline_of(kern, r["n"], hbm, hbm_kind, ncu_traffic())
     solver_ms = sum(v["ms"] for v in kern.values())
     cpu = None
     if not args.no_cpu_baseline and world == 1:
@@ -614,7 +723,9 @@ def main():
     dss = None
     batched = None
     serving = None
+    forms = None
     if not args.no_cpu_baseline and world == 1:
+        forms = forms_compare(hbm, hbm_kind)
         dss = dsscfg_compare()
         batched = batched_compare()
         serving = serving_compare()
@@ -635,6 +746,7 @@ def main():
         "evaluations_per_step": r["evals_k"] / K,
         "hbm_GBps_model": r["model_bytes_iter"] / (solver_ms / K / 1000.0) / 1e9 if solver_ms else None,
         "kernels": per_kernel,
+        "forms": forms,
         "dsscfg": dss,
         "serving": serving,
         "batched": batched,

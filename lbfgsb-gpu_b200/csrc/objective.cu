@@ -27,6 +27,7 @@ struct SynthCtx {
   double* fhost;        // pinned
   unsigned int* ticket;
   int grid[2];          // launch grid of the double / float kernel: one wave of CTAs
+  double f0;            // constant subtracted from the double sum before f is rounded
 };
 
 // exp, log1p and sincos in the kernel's precision.
@@ -44,7 +45,7 @@ __global__ void __launch_bounds__(kThreads) k_synth(int s, const R* __restrict__
                                                     const F* __restrict__ tt,
                                                     const F* __restrict__ b, R* __restrict__ g,
                                                     double* part, unsigned int* ticket,
-                                                    double* fout) {
+                                                    double f0, double* fout) {
   const long long n = (long long)s * s;
   const R h = R(1) / (R)(s + 1), h2 = h * h;
   double acc = 0.0;
@@ -78,7 +79,7 @@ __global__ void __launch_bounds__(kThreads) k_synth(int s, const R* __restrict__
   if (!last_cta(ticket)) return;
   __shared__ double red[1];
   fold_rows<kThreads>(part, gridDim.x, 1, 1, 0, 0, red);
-  if (threadIdx.x == 0) *fout = red[0];
+  if (threadIdx.x == 0) *fout = red[0] - f0;
 }
 
 template <typename R>
@@ -88,11 +89,12 @@ static int synth_eval(void* handle, R* x, R* f, R* g, void* stream) {
   if (c->single) {
     k_synth<R, float><<<c->grid[sizeof(R) == 8 ? 0 : 1], kThreads, 0, s>>>(
         c->s, x, (const float*)c->field[0], (const float*)c->field[1],
-        (const float*)c->field[2], (const float*)c->field[3], g, c->part, c->ticket, c->fdev);
+        (const float*)c->field[2], (const float*)c->field[3], g, c->part, c->ticket, c->f0,
+        c->fdev);
   } else {
     k_synth<R, double><<<c->grid[sizeof(R) == 8 ? 0 : 1], kThreads, 0, s>>>(
         c->s, x, (const double*)c->field[0], (const double*)c->field[1],
-        (const double*)c->field[2], (const double*)c->field[3], g, c->part, c->ticket,
+        (const double*)c->field[2], (const double*)c->field[3], g, c->part, c->ticket, c->f0,
         c->fdev);
   }
   cudaMemcpyAsync(c->fhost, c->fdev, sizeof(double), cudaMemcpyDeviceToHost, s);
@@ -158,6 +160,10 @@ void* lbfgsb_b200_synth_create(int s, const double* kappa, const double* w, cons
     return nullptr;
   }
   return c;
+}
+
+void lbfgsb_b200_synth_set_offset(void* handle, double f0) {
+  if (handle) static_cast<SynthCtx*>(handle)->f0 = f0;
 }
 
 void lbfgsb_b200_synth_destroy(void* handle) {

@@ -85,7 +85,7 @@ EXPORTS = [
     "lbfgsb_b200_minimize_f64", "lbfgsb_b200_minimize_f32",
     "lbfgsb_b200_minimize_ext_f64", "lbfgsb_b200_minimize_ext_f32",
     "lbfgsb_b200_last_stats", "lbfgsb_b200_last_error", "lbfgsb_b200_synth_create",
-    "lbfgsb_b200_synth_destroy", "lbfgsb_b200_synth_funcgrad_f64",
+    "lbfgsb_b200_synth_destroy", "lbfgsb_b200_synth_set_offset", "lbfgsb_b200_synth_funcgrad_f64",
     "lbfgsb_b200_synth_funcgrad_f32", "lbfgsb_b200_copy", "lbfgsb_b200_projgr_noalloc_f64",
     "lbfgsb_b200_trim_memory", "lbfgsb_b200_dsscfg_create", "lbfgsb_b200_dsscfg_destroy",
     "lbfgsb_b200_dsscfg_funcgrad_f64", "lbfgsb_b200_dsscfg_funcgrad_f32",
@@ -129,6 +129,8 @@ def load() -> C.CDLL:
     lib.lbfgsb_b200_synth_create.argtypes = [C.c_int] + [C.c_void_p] * 4 + [C.c_int]
     lib.lbfgsb_b200_synth_destroy.restype = None
     lib.lbfgsb_b200_synth_destroy.argtypes = [C.c_void_p]
+    lib.lbfgsb_b200_synth_set_offset.restype = None
+    lib.lbfgsb_b200_synth_set_offset.argtypes = [C.c_void_p, C.c_double]
     lib.lbfgsb_b200_copy.restype = C.c_int
     lib.lbfgsb_b200_copy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
     for sfx, opt, summ in (("f64", OptionF64, SummaryF64), ("f32", OptionF32, SummaryF32)):
@@ -289,6 +291,8 @@ class SynthObjective:
             1 if single_precision_fields else 0)
         if not self.handle:
             raise RuntimeError("lbfgsb_b200_synth_create failed")
+        if prob.get("f_offset", 0.0):
+            lib.lbfgsb_b200_synth_set_offset(self.handle, float(prob["f_offset"]))
         self.f64 = C.cast(lib.lbfgsb_b200_synth_funcgrad_f64, C.c_void_p).value
         self.f32 = C.cast(lib.lbfgsb_b200_synth_funcgrad_f32, C.c_void_p).value
 
@@ -302,6 +306,29 @@ class SynthObjective:
             self.close()
         except Exception:
             pass
+
+
+def synth_value(prob: dict, x0=None) -> float:
+    """f of a synth.py problem at x0 (default 0; a host array), evaluated in FP64 by the
+    device objective; at 0 it is the f_offset that lets a float f resolve the decrease of
+    the first iterations."""
+    import torch
+    lib = load()
+    n = int(prob["nbd"].size)
+    so = SynthObjective({k: v for k, v in prob.items() if k != "f_offset"})
+    if x0 is None:
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    else:
+        x = torch.from_numpy(np.ascontiguousarray(x0, dtype=np.float64)).to("cuda")
+    g = torch.empty_like(x)
+    f = C.c_double(0.0)
+    fn = lib.lbfgsb_b200_synth_funcgrad_f64
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_void_p, C.c_void_p, C.c_void_p]
+    fn(so.handle, x.data_ptr(), C.byref(f), g.data_ptr(), None, None)
+    torch.cuda.synchronize()
+    so.close()
+    return float(f.value)
 
 
 def _digest(a: np.ndarray) -> str:

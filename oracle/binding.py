@@ -19,6 +19,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libref_lbfgsb.so")
+DROPIN_EXE = os.path.join(HERE, "_ref", "dsscfg_dropin")
 
 
 class SummaryF64(C.Structure):
@@ -67,13 +68,20 @@ _TRACE_KEYS = [f for f, _ in TraceRec._fields_]
 
 
 def build(reference_dir: str | None = None, quiet: bool = True) -> None:
-    """Build liboracle.so, and the reference build when the reference tree is present."""
+    """Build liboracle.so, and the reference build when `reference_dir` (or the
+    environment variable LBFGSB_REFERENCE_DIR) names a reference tree."""
     cmd = ["make", "-C", HERE, os.path.join(HERE, "liboracle.so")]
     subprocess.run(cmd, check=True, capture_output=quiet)
-    ref_dir = reference_dir or "/root/reference"
-    if os.path.isfile(os.path.join(ref_dir, "culbfgsb", "lbfgsbcpu.cpp")):
+    ref_dir = reference_dir or os.environ.get("LBFGSB_REFERENCE_DIR")
+    if ref_dir and os.path.isfile(os.path.join(ref_dir, "culbfgsb", "lbfgsbcpu.cpp")):
         subprocess.run(["make", "-C", HERE, "ref", f"REFERENCE_DIR={ref_dir}"], check=True,
                        capture_output=quiet)
+        # the reference's dsscfg example program on this library's drop-in header (needs
+        # the built library)
+        lib = os.path.join(os.path.dirname(HERE), "lbfgsb-gpu_b200", "liblbfgsb_b200.so")
+        if os.path.exists(lib):
+            subprocess.run(["make", "-C", HERE, "dropin", f"REFERENCE_DIR={ref_dir}"],
+                           check=True, capture_output=quiet)
 
 
 _libs: dict[str, C.CDLL] = {}
@@ -149,7 +157,8 @@ def host_objective(prob: dict, dtype, source: str = "oracle"):
     """Host objective callback body for a problem dict: (xp, fp, gp) pointers -> fills f, g.
 
     prob["kind"] == "synth" (default): the grid objective of objective.c with fields
-    kappa, w, t, b; "quad": the separable quadratic with vectors a, c; "dsscfg": the
+    kappa, w, t, b, minus the constant prob["f_offset"] when that is given; "quad": the
+    separable quadratic with vectors a, c; "dsscfg": the
     steady-state combustion objective on an nx x ny grid with parameter lam, from
     objective.c (source "oracle") or from the reference's own example code (source
     "ref", the reference build)."""
@@ -172,10 +181,23 @@ def host_objective(prob: dict, dtype, source: str = "oracle"):
     names = ("kappa", "w", "t", "b") if kind == "synth" else ("a", "c")
     arrs = [np.ascontiguousarray(prob[k], dtype=np.float64) for k in names]
     ptrs = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in arrs]
+    lead = int(prob["s"]) if kind == "synth" else int(prob["nbd"].size)
+    f0 = float(prob.get("f_offset", 0.0))
+    if kind == "synth" and f0 != 0.0:
+        # f minus the constant f0, subtracted before f is rounded (objective.c)
+        fn = getattr(lib, f"orc_synth_eval_off_{sfx}")
+        fn.restype = None
+        fn.argtypes = [C.c_int] + [C.POINTER(C.c_double)] * 4 + [C.c_double] + \
+            [C.POINTER(real)] * 3
+
+        def evaluate_off(xp, fp, gp):
+            fn(lead, *ptrs, f0, xp, fp, gp)
+
+        evaluate_off.keepalive = arrs  # type: ignore[attr-defined]
+        return evaluate_off
     fn = getattr(lib, f"orc_{kind}_eval_{sfx}")
     fn.restype = None
     fn.argtypes = [C.c_int] + [C.POINTER(C.c_double)] * len(arrs) + [C.POINTER(real)] * 3
-    lead = int(prob["s"]) if kind == "synth" else int(prob["nbd"].size)
 
     def evaluate_ptr(xp, fp, gp):
         fn(lead, *ptrs, xp, fp, gp)

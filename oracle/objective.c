@@ -27,8 +27,8 @@ static float sigmoid_f(float z) {
   return e / (1.0f + e);
 }
 
-void orc_synth_eval_f64(int s, const double* kappa, const double* w, const double* t,
-                        const double* b, const double* x, double* f, double* g) {
+void orc_synth_eval_off_f64(int s, const double* kappa, const double* w, const double* t,
+                            const double* b, double f0, const double* x, double* f, double* g) {
   const double h = 1.0 / (double)(s + 1), h2 = h * h;
   double acc = 0.0;
   long k;
@@ -52,11 +52,11 @@ void orc_synth_eval_f64(int s, const double* kappa, const double* w, const doubl
       }
     }
   }
-  *f = acc;
+  *f = acc - f0;
 }
 
-void orc_synth_eval_f32(int s, const double* kappa, const double* w, const double* t,
-                        const double* b, const float* x, float* f, float* g) {
+void orc_synth_eval_off_f32(int s, const double* kappa, const double* w, const double* t,
+                            const double* b, double f0, const float* x, float* f, float* g) {
   const float h = 1.0f / (float)(s + 1), h2 = h * h;
   double acc = 0.0;
   long k;
@@ -82,7 +82,21 @@ void orc_synth_eval_f32(int s, const double* kappa, const double* w, const doubl
       }
     }
   }
-  *f = (float)acc;
+  *f = (float)(acc - f0);
+}
+
+/* The objective minus a constant f0, subtracted from the double sum before f is rounded to
+ * the caller's precision: the minimiser and g are unchanged, while a float f keeps the
+ * resolution of the decrease near f0 (on a 4096 x 4096 grid f is about 0.45 and an
+ * iteration lowers it by about 1e-8, below the spacing of floats there). */
+void orc_synth_eval_f64(int s, const double* kappa, const double* w, const double* t,
+                        const double* b, const double* x, double* f, double* g) {
+  orc_synth_eval_off_f64(s, kappa, w, t, b, 0.0, x, f, g);
+}
+
+void orc_synth_eval_f32(int s, const double* kappa, const double* w, const double* t,
+                        const double* b, const float* x, float* f, float* g) {
+  orc_synth_eval_off_f32(s, kappa, w, t, b, 0.0, x, f, g);
 }
 
 /* Separable quadratic f = sum_k 0.5*a_k*(x_k - c_k)^2 (ties and zero gradients on demand:

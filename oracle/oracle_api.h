@@ -99,6 +99,11 @@ void orc_synth_eval_f64(int s, const double* kappa, const double* w, const doubl
                         const double* b, const double* x, double* f, double* g);
 void orc_synth_eval_f32(int s, const double* kappa, const double* w, const double* t,
                         const double* b, const float* x, float* f, float* g);
+/* The same with f0 subtracted from the double sum before f is rounded. */
+void orc_synth_eval_off_f64(int s, const double* kappa, const double* w, const double* t,
+                            const double* b, double f0, const double* x, double* f, double* g);
+void orc_synth_eval_off_f32(int s, const double* kappa, const double* w, const double* t,
+                            const double* b, double f0, const float* x, float* f, float* g);
 
 /* dsscfg, the reference example's steady-state combustion objective (objective.c): start
  * point and f, g on an nx x ny grid; g may be NULL.  The ref_ variants run the

@@ -36,16 +36,28 @@ def OB():
     return binding
 
 
-@pytest.mark.parametrize("form", [0, 1, 2])
-@pytest.mark.parametrize("name", CASES)
-def test_form_against_fp64_oracle(LB, OB, name, form):
+BOUND = {0: 1e-5, 1: 1e-6, 2: 1e-6}
+# the mixed form's known miss of 1e-6 (float objective); still held to the FP32 tolerance
+MIXED_MISS = {"synth_s64_f32_b002"}
+
+
+def _final_rel(LB, OB, name, form):
     prob, dt, x0, over, stop = make_case(name)
     ref = OB.run_cpu("oracle", prob, np.float64, x0=x0,
                      option=apply_options(OB.default_option(np.float64), over))
     r = LB.solve(prob, np.float32, x0=x0, option=apply_options(LB.default_option(np.float32), over),
                  objective="host", form=form)
     fref = ref.evals[-1][0]
-    assert abs(r.evals[-1][0] - fref) <= 1e-5 * max(1.0, abs(fref))
+    return prob, r, abs(r.evals[-1][0] - fref) / max(1.0, abs(fref))
+
+
+@pytest.mark.parametrize("form", [0, 1, 2])
+@pytest.mark.parametrize("name", CASES)
+def test_form_against_fp64_oracle(LB, OB, name, form):
+    prob, r, rel = _final_rel(LB, OB, name, form)
+    print(f"{name} form {form}: final f relative error {rel:.2e}")
+    bound = 1e-5 if (form == 1 and name in MIXED_MISS) else BOUND[form]
+    assert rel <= bound, rel
     assert r.info in (1, 2, 4)
     nbd = prob["nbd"]
     x = r.x.astype(np.float64)
@@ -54,3 +66,11 @@ def test_form_against_fp64_oracle(LB, OB, name, form):
     has_l = (nbd == 1) | (nbd == 2)
     has_u = (nbd == 2) | (nbd == 3)
     assert np.all(x[has_l] >= lo[has_l]) and np.all(x[has_u] <= hi[has_u])
+
+
+@pytest.mark.xfail(reason="mixed form on s = 64, bounds +-0.02: the float objective's gradient "
+                          "error moves the stopping point ~3e-6 from the FP64 optimum", strict=False)
+@pytest.mark.parametrize("name", sorted(MIXED_MISS))
+def test_mixed_form_one_in_a_million(LB, OB, name):
+    _, _, rel = _final_rel(LB, OB, name, 1)
+    assert rel <= 1e-6, rel
