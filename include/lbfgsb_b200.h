@@ -220,6 +220,43 @@ int lbfgsb_b200_minimize_ext_f32(int n, float* x, const int* nbd, const float* l
                                  void* stream, const lbfgsb_b200_ext* ext,
                                  lbfgsb_b200_summary_f32* summary);
 
+/* ---- device-driven solves (no counterpart in the reference) ------------------------
+ * The reference's funcgrad returns f on the host, so every evaluation costs the solver a
+ * device-to-host synchronisation and the host must steer each step.  An objective that
+ * leaves f in device memory lets the whole outer loop run on the device: one round of
+ * launches (the loop top, the Cauchy point and the subspace step, the trial point, one
+ * evaluation, the line-search decision and the stopping tests) is captured once into a
+ * CUDA graph and relaunched; the host reads the solver's state before the first iteration
+ * and then only every few rounds.
+ *
+ * The objective is called once to evaluate at x0 and once while the round is captured, so
+ * it must only enqueue work on `stream` (no synchronisation, no allocation, nothing a
+ * stream capture rejects).  Its arguments are DEVICE addresses: *x (the pointer to the n
+ * values of x to evaluate at) and *g (the pointer to the n values of g to write) are read
+ * by the objective's kernels on the device, because the solver rotates its buffers without
+ * the host; f receives f(x) as a double; *active is 0 when the result of this round's
+ * evaluation is not used (the objective may then skip its work, e.g. return at once from
+ * its kernels).  The solve gives the same iterates and summary as lbfgsb_b200_minimize_ext
+ * with a funcgrad that computes the same f and g.  Not supported in this mode: the
+ * after_iteration / customized_stopping callbacks and ext->trace / ext->profile (ignored);
+ * ext->form and ext->subsm_projection apply. */
+typedef int (*lbfgsb_b200_device_objective_f64)(void* user, const double* const* x,
+                                                double* const* g, double* f, const int* active,
+                                                void* stream);
+typedef int (*lbfgsb_b200_device_objective_f32)(void* user, const float* const* x,
+                                                float* const* g, double* f, const int* active,
+                                                void* stream);
+int lbfgsb_b200_minimize_device_f64(int n, double* x, const int* nbd, const double* l,
+                                    const double* u, const lbfgsb_b200_option_f64* option,
+                                    lbfgsb_b200_device_objective_f64 objective, void* user,
+                                    void* stream, const lbfgsb_b200_ext* ext,
+                                    lbfgsb_b200_summary_f64* summary);
+int lbfgsb_b200_minimize_device_f32(int n, float* x, const int* nbd, const float* l,
+                                    const float* u, const lbfgsb_b200_option_f32* option,
+                                    lbfgsb_b200_device_objective_f32 objective, void* user,
+                                    void* stream, const lbfgsb_b200_ext* ext,
+                                    lbfgsb_b200_summary_f32* summary);
+
 /* Statistics of the calling thread's last solve. */
 #define LBFGSB_B200_MAX_KERNELS 16
 typedef struct {
@@ -232,6 +269,7 @@ typedef struct {
   long long host_syncs;              /* stream synchronisations of the solver */
   long long evaluations;             /* funcgrad calls */
   double bytes_per_iteration_model;  /* algorithmic bytes of one steady-state iteration */
+  long long rounds;                  /* rounds of a device-driven solve (else 0) */
 } lbfgsb_b200_stats;
 int lbfgsb_b200_last_stats(lbfgsb_b200_stats* out);
 
@@ -263,6 +301,13 @@ int lbfgsb_b200_synth_funcgrad_f64(void* handle, double* x, double* f, double* g
                                    const lbfgsb_b200_summary_f64* summary);
 int lbfgsb_b200_synth_funcgrad_f32(void* handle, float* x, float* f, float* g, void* stream,
                                    const lbfgsb_b200_summary_f32* summary);
+/* The same objective for device-driven solves (lbfgsb_b200_device_objective_*): one kernel
+ * launch, f written to device memory, nothing synchronised; it does no work when *active
+ * is 0. */
+int lbfgsb_b200_synth_device_f64(void* handle, const double* const* x, double* const* g,
+                                 double* f, const int* active, void* stream);
+int lbfgsb_b200_synth_device_f32(void* handle, const float* const* x, float* const* g,
+                                 double* f, const int* active, void* stream);
 
 /* ---- dsscfg objective (the reference example's objective, examples/dsscfg/dsscfg_cuda.cu)
  * The MINPACK-2 steady-state combustion problem on an nx x ny grid with parameter lambda,

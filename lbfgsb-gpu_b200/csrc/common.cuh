@@ -129,6 +129,15 @@ struct FixedDiv<float> : FixedDiv32 {
   using FixedDiv32::FixedDiv32;
 };
 
+// A CTA's place among the CTAs that share one problem instance: rank 0..count-1.  A
+// single-instance launch is the whole grid; a batched launch gives each instance its own
+// contiguous range of CTAs (batch.cuh).
+struct CtaPos {
+  int rank;
+  int count;
+};
+__device__ __forceinline__ CtaPos cta_here() { return CtaPos{(int)blockIdx.x, (int)gridDim.x}; }
+
 // Splitmix64 finaliser: the order-free hash of the free set used by the trace.
 __host__ __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
   z += 0x9E3779B97F4A7C15ULL;

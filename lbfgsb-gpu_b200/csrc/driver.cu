@@ -23,6 +23,7 @@
 
 #include "../../include/lbfgsb_b200.h"
 #include "passes.cuh"
+#include "rounds.cuh"
 #include "walk.cuh"
 
 namespace lbfgsb_b200 {
@@ -185,13 +186,16 @@ struct Workspace {
     blocks.push_back(p);
     return static_cast<T*>(p);
   }
-  ~Workspace() {
+  void release() {
     for (void* p : blocks) cudaFreeAsync(p, s);
+    blocks.clear();
   }
+  ~Workspace() { release(); }
 };
 
-// Pinned host mirror of the state header, kept per thread (one page, allocated once).
-static void* pinned_mirror(size_t bytes) {
+// Pinned host scratch of the calling thread, `which` = 0 the state header's mirror, 1 the
+// device-driven solve's evaluation slot (each allocated once, grown when needed).
+static void* pinned_scratch(int which, size_t bytes) {
   struct Mirror {
     void* p = nullptr;
     size_t bytes = 0;
@@ -199,16 +203,19 @@ static void* pinned_mirror(size_t bytes) {
       if (p) cudaFreeHost(p);
     }
   };
-  thread_local Mirror m;
-  if (m.bytes < bytes) {
-    if (m.p) CK(cudaFreeHost(m.p));
-    m.p = nullptr;
-    m.bytes = 0;
-    CK(cudaMallocHost(&m.p, bytes));
-    m.bytes = bytes;
+  thread_local Mirror m[2];
+  Mirror& mm = m[which];
+  if (mm.bytes < bytes) {
+    if (mm.p) CK(cudaFreeHost(mm.p));
+    mm.p = nullptr;
+    mm.bytes = 0;
+    CK(cudaMallocHost(&mm.p, bytes));
+    mm.bytes = bytes;
   }
-  return m.p;
+  return mm.p;
 }
+static void* pinned_mirror(size_t bytes) { return pinned_scratch(0, bytes); }
+static void* pinned_mirror_slot(size_t bytes) { return pinned_scratch(1, bytes); }
 
 static int device_sms() {
   int dev = 0, sms = 0;
@@ -263,6 +270,138 @@ static int grid_for(K kernel, int n, int threads) {
   return (int)std::max<long long>(1, std::min(want, cap));
 }
 
+// Launch shapes of one solve's passes.
+struct Plan {
+  PassCfg gcp, freev, dir, apply, post, pgcp;
+  int g_proj = 1, g_elem = 1;
+};
+
+// Takes one solve's workspace from the pool, checks its alignment, fills the pass context
+// and the launch shapes, zeroes the history, and fills the host copy of the state (w.hs)
+// with the start of the reference driver (head = 1, theta = 1, col = 0).  walk: allocate
+// the breakpoint-walk buffers now (device-driven solves cannot allocate them on demand).
+template <typename R, typename H, typename S>
+static void prepare(Workspace<R, H, S>& w, Ctx<R, H, S>& c, Plan& p, int n, int m, const int* nbd,
+                    const R* l, const R* u, cudaStream_t stream, const lbfgsb_b200_ext* ext,
+                    bool walk) {
+  const size_t N = (size_t)n;
+  for (int k = 0; k < 3; k++) w.X[k] = w.template alloc<R>(N);
+  for (int k = 0; k < 2; k++) w.G[k] = w.template alloc<R>(N);
+  w.dsub = w.template alloc<R>(N);
+  const size_t ld = ((N + kTile - 1) / kTile) * kTile;  // 16-byte aligned slots
+  w.ws = w.template alloc<H>(ld * kSlots);
+  w.wy = w.template alloc<H>(ld * kSlots);
+  w.code = w.template alloc<int8_t>(N);
+  const size_t words = (N + 31) / 32 + 1;
+  w.fbits = w.template alloc<uint32_t>(words);
+  w.st = w.template alloc<DevState<S>>(1);
+  w.ticket = w.template alloc<unsigned int>(1);
+  w.hs = static_cast<DevState<S>*>(pinned_mirror(sizeof(DevState<S>)));
+
+  // the staged passes copy l, u and nbd in 16-byte aligned tiles
+  const R* la = l;
+  const R* ua = u;
+  const int* nbda = nbd;
+  auto misaligned = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) != 0; };
+  if (misaligned(l) || misaligned(u) || misaligned(nbd)) {
+    R* lc = w.template alloc<R>(N);
+    R* uc = w.template alloc<R>(N);
+    int* nc = w.template alloc<int>(N);
+    CK(cudaMemcpyAsync(lc, l, N * sizeof(R), cudaMemcpyDeviceToDevice, stream));
+    CK(cudaMemcpyAsync(uc, u, N * sizeof(R), cudaMemcpyDeviceToDevice, stream));
+    CK(cudaMemcpyAsync(nc, nbd, N * sizeof(int), cudaMemcpyDeviceToDevice, stream));
+    la = lc;
+    ua = uc;
+    nbda = nc;
+  }
+
+  // every stream the staged passes copy with cp.async.bulk starts on a 16-byte boundary
+  for (const void* q : {(const void*)la, (const void*)ua, (const void*)nbda, (const void*)w.X[0],
+                        (const void*)w.X[1], (const void*)w.X[2], (const void*)w.G[0],
+                        (const void*)w.G[1], (const void*)w.dsub, (const void*)w.code,
+                        (const void*)w.fbits, (const void*)w.ws, (const void*)w.wy}) {
+    if (misaligned(q)) throw CudaFailure{cudaErrorMisalignedAddress, "workspace alignment", __LINE__};
+  }
+
+  c = Ctx<R, H, S>{};
+  c.n = n;
+  c.l = la;
+  c.u = ua;
+  c.nbd = nbda;
+  c.ws = w.ws;
+  c.wy = w.wy;
+  c.ld = (long long)ld;
+  c.stages = 2;
+  c.code = w.code;
+  c.fbits = w.fbits;
+  c.dsub = w.dsub;
+  c.st = w.st;
+  c.ticket = w.ticket;
+  c.wl_t = nullptr;
+  c.wl_i = nullptr;
+  c.wl_n = nullptr;
+  c.rounds = 0;
+  for (int k = 0; k < 3; k++) c.X[k] = w.X[k];
+  for (int k = 0; k < 2; k++) c.G[k] = w.G[k];
+  c.gdummy = nullptr;
+  c.ev_x = nullptr;
+  c.ev_g = nullptr;
+  c.ev_f = nullptr;
+  c.ev_act = nullptr;
+  if (walk) {
+    w.wl_t = w.template alloc<double>(N);
+    w.wl_i = w.template alloc<int>(N);
+    w.wl_n = w.template alloc<unsigned int>(1);
+    c.wl_t = w.wl_t;
+    c.wl_i = w.wl_i;
+    c.wl_n = w.wl_n;
+  }
+
+  const int hsz = (int)sizeof(H);
+  p.gcp = pass_cfg(k_gcp_scan<R, H, S, kConsWide>,
+                   stage_capacity(StageBytes<R>::gcp, 0, m, hsz), n, kConsWide + 32);
+  p.freev = pass_cfg(k_freev_formk<R, H, S, kConsWide>,
+                     stage_capacity(StageBytes<R>::freev, kTile / 8, m, hsz), n, kConsWide + 32);
+  p.dir = pass_cfg(k_subsm_dir<R, H, S, kConsWide>,
+                   stage_capacity(StageBytes<R>::dir, 0, m, hsz), n, kConsWide + 32);
+  p.apply = pass_cfg(k_subsm_apply<R, H, S, kConsWide>,
+                     stage_capacity(StageBytes<R>::apply, 0, 0, hsz), n, kConsWide + 32);
+  p.post = pass_cfg(k_post_eval<R, H, S, kConsWide>,
+                    stage_capacity(StageBytes<R>::post, 0, m, hsz), n, kConsWide + 32);
+  p.pgcp = pass_cfg(k_post_gcp<R, H, S, kConsWide>,
+                    stage_capacity(StageBytes<R>::post, 0, m, hsz), n, kConsWide + 32);
+  p.g_proj = grid_for(k_projgr<R, H, S>, n, kThreads);
+  const int g_max = std::max({p.gcp.grid, p.freev.grid, p.dir.grid, p.apply.grid, p.post.grid,
+                              p.pgcp.grid, p.g_proj});
+  w.part = w.template alloc<double>((size_t)g_max * 256);
+  c.part = w.part;
+  p.g_elem = (int)std::min<long long>(((long long)n + 255) / 256, (long long)device_sms() * 8);
+
+  // history slots start at zero so that unused positions read as finite values
+  CK(cudaMemsetAsync(w.ws, 0, N * kSlots * sizeof(H), stream));
+  CK(cudaMemsetAsync(w.wy, 0, N * kSlots * sizeof(H), stream));
+  CK(cudaMemsetAsync(w.fbits, 0, words * sizeof(uint32_t), stream));
+  CK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned int), stream));
+
+  DevState<S>& hs = *w.hs;
+  std::memset(&hs, 0, sizeof(hs));
+  hs.n = n;
+  hs.m = m;
+  hs.subsm_proj = (ext && ext->subsm_projection) ? 1 : 0;
+  hs.boxed = 1;
+  hs.head = 1;
+  hs.theta = 1;
+  hs.iword = -1;
+  hs.big = (S)1.0e10;
+  for (int r = 1; r <= m; r++) hs.phys[r] = r - 1;
+  hs.spare = m;
+  hs.xr[0] = 0;
+  hs.xr[1] = 1;
+  hs.xr[2] = 2;
+  hs.gr[0] = 0;
+  hs.gr[1] = 1;
+}
+
 template <typename R, typename H, typename S>
 static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
                  const typename Api<R>::Opt* opt, typename Api<R>::Cb funcgrad,
@@ -303,101 +442,13 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
   int prev_no_spec = 0;
   try {
     const size_t N = (size_t)n;
-    for (int k = 0; k < 3; k++) w.X[k] = w.template alloc<R>(N);
-    for (int k = 0; k < 2; k++) w.G[k] = w.template alloc<R>(N);
-    w.dsub = w.template alloc<R>(N);
-    const size_t ld = ((N + kTile - 1) / kTile) * kTile;  // 16-byte aligned slots
-    w.ws = w.template alloc<H>(ld * kSlots);
-    w.wy = w.template alloc<H>(ld * kSlots);
-    w.code = w.template alloc<int8_t>(N);
-    const size_t words = (N + 31) / 32 + 1;
-    w.fbits = w.template alloc<uint32_t>(words);
-    w.st = w.template alloc<DevState<S>>(1);
-    w.ticket = w.template alloc<unsigned int>(1);
-    w.hs = static_cast<DevState<S>*>(pinned_mirror(sizeof(DevState<S>)));
-
-    // the staged passes copy l, u and nbd in 16-byte aligned tiles
-    const R* la = l;
-    const R* ua = u;
-    const int* nbda = nbd;
-    auto misaligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) != 0; };
-    if (misaligned(l) || misaligned(u) || misaligned(nbd)) {
-      R* lc = w.template alloc<R>(N);
-      R* uc = w.template alloc<R>(N);
-      int* nc = w.template alloc<int>(N);
-      CK(cudaMemcpyAsync(lc, l, N * sizeof(R), cudaMemcpyDeviceToDevice, stream));
-      CK(cudaMemcpyAsync(uc, u, N * sizeof(R), cudaMemcpyDeviceToDevice, stream));
-      CK(cudaMemcpyAsync(nc, nbd, N * sizeof(int), cudaMemcpyDeviceToDevice, stream));
-      la = lc;
-      ua = uc;
-      nbda = nc;
-    }
-
-    // every stream the staged passes copy with cp.async.bulk starts on a 16-byte boundary
-    for (const void* p : {(const void*)la, (const void*)ua, (const void*)nbda, (const void*)w.X[0],
-                          (const void*)w.X[1], (const void*)w.X[2], (const void*)w.G[0],
-                          (const void*)w.G[1], (const void*)w.dsub, (const void*)w.code,
-                          (const void*)w.fbits, (const void*)w.ws, (const void*)w.wy}) {
-      if (misaligned(p)) throw CudaFailure{cudaErrorMisalignedAddress, "workspace alignment", __LINE__};
-    }
-
     Ctx<R, H, S> c;
-    c.n = n;
-    c.l = la;
-    c.u = ua;
-    c.nbd = nbda;
-    c.ws = w.ws;
-    c.wy = w.wy;
-    c.ld = (long long)ld;
-    c.stages = 2;
-    c.code = w.code;
-    c.fbits = w.fbits;
-    c.dsub = w.dsub;
-    c.st = w.st;
-    c.ticket = w.ticket;
-    c.wl_t = nullptr;
-    c.wl_i = nullptr;
-    c.wl_n = nullptr;
-
-    const int hsz = (int)sizeof(H);
-    const PassCfg p_gcp = pass_cfg(k_gcp_scan<R, H, S, kConsWide>,
-                                   stage_capacity(StageBytes<R>::gcp, 0, m, hsz), n, kConsWide + 32);
-    const PassCfg p_freev =
-        pass_cfg(k_freev_formk<R, H, S, kConsWide>,
-                 stage_capacity(StageBytes<R>::freev, kTile / 8, m, hsz), n, kConsWide + 32);
-    const PassCfg p_dir = pass_cfg(k_subsm_dir<R, H, S, kConsWide>,
-                                   stage_capacity(StageBytes<R>::dir, 0, m, hsz), n, kConsWide + 32);
-    const PassCfg p_apply = pass_cfg(k_subsm_apply<R, H, S, kConsWide>,
-                                     stage_capacity(StageBytes<R>::apply, 0, 0, hsz), n, kConsWide + 32);
-    const PassCfg p_post = pass_cfg(k_post_eval<R, H, S, kConsWide>,
-                                    stage_capacity(StageBytes<R>::post, 0, m, hsz), n, kConsWide + 32);
-    const PassCfg p_pgcp = pass_cfg(k_post_gcp<R, H, S, kConsWide>,
-                                    stage_capacity(StageBytes<R>::post, 0, m, hsz), n, kConsWide + 32);
-    const int g_proj = grid_for(k_projgr<R, H, S>, n, kThreads);
-    const int g_max = std::max({p_gcp.grid, p_freev.grid, p_dir.grid, p_apply.grid, p_post.grid,
-                                p_pgcp.grid, g_proj});
-    w.part = w.template alloc<double>((size_t)g_max * 256);
-    c.part = w.part;
-    const int g_elem = (int)std::min<long long>(((long long)n + 255) / 256, (long long)device_sms() * 8);
-
-    // history slots start at zero so that unused positions read as finite values
-    CK(cudaMemsetAsync(w.ws, 0, N * kSlots * sizeof(H), stream));
-    CK(cudaMemsetAsync(w.wy, 0, N * kSlots * sizeof(H), stream));
-    CK(cudaMemsetAsync(w.fbits, 0, words * sizeof(uint32_t), stream));
-    CK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned int), stream));
-
+    Plan p;
+    prepare<R, H, S>(w, c, p, n, m, nbd, l, u, stream, ext, false);
+    const PassCfg &p_gcp = p.gcp, &p_freev = p.freev, &p_dir = p.dir, &p_apply = p.apply,
+                  &p_post = p.post, &p_pgcp = p.pgcp;
+    const int g_proj = p.g_proj, g_elem = p.g_elem;
     DevState<S>& hs = *w.hs;
-    std::memset(&hs, 0, sizeof(hs));
-    hs.n = n;
-    hs.m = m;
-    hs.subsm_proj = (ext && ext->subsm_projection) ? 1 : 0;
-    hs.boxed = 1;
-    hs.head = 1;
-    hs.theta = 1;
-    hs.iword = -1;
-    hs.big = (S)1.0e10;
-    for (int r = 1; r <= m; r++) hs.phys[r] = r - 1;
-    hs.spare = m;
     CK(cudaMemcpyAsync(w.st, &hs, sizeof(hs), cudaMemcpyHostToDevice, stream));
     const size_t header = offsetof(DevState<S>, big);
     auto pull = [&]() {
@@ -698,6 +749,236 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
   return LBFGSB_B200_OK;
 }
 
+template <typename R>
+struct DevObjective;
+template <>
+struct DevObjective<double> {
+  using Fn = lbfgsb_b200_device_objective_f64;
+};
+template <>
+struct DevObjective<float> {
+  using Fn = lbfgsb_b200_device_objective_f32;
+};
+
+// The calling thread's stream for device-driven solves (capture needs a stream other than
+// the legacy default stream) and the two events that order it after / before the caller's.
+struct RoundStream {
+  cudaStream_t s = nullptr;
+  cudaEvent_t in = nullptr, out = nullptr;
+  int dev = -1;
+  ~RoundStream() {
+    if (in) cudaEventDestroy(in);
+    if (out) cudaEventDestroy(out);
+    if (s) cudaStreamDestroy(s);
+  }
+};
+static RoundStream& round_stream() {
+  thread_local RoundStream rs;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (rs.dev != dev) {
+    if (rs.s) {
+      cudaEventDestroy(rs.in);
+      cudaEventDestroy(rs.out);
+      cudaStreamDestroy(rs.s);
+    }
+    rs.s = nullptr;
+    CK(cudaStreamCreateWithFlags(&rs.s, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&rs.in, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&rs.out, cudaEventDisableTiming));
+    rs.dev = dev;
+  }
+  return rs;
+}
+
+// The evaluation slot of one device-driven solve (device memory): the objective reads x at
+// *x, writes g to *g and f to f; active = 0 marks an evaluation whose result is not used.
+struct EvalSlots {
+  void* x;
+  void* g;
+  double f;
+  int active;
+  int pad;
+};
+
+// Owns a captured round graph.
+struct RoundGraph {
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t e = nullptr;
+  ~RoundGraph() {
+    if (e) cudaGraphExecDestroy(e);
+    if (g) cudaGraphDestroy(g);
+  }
+};
+
+// A solve whose objective keeps f on the device (no counterpart in the reference, whose
+// callback returns f on the host): the outer loop's decisions run on the device
+// (rounds.cuh), one round is captured into a CUDA graph and relaunched, and the host reads
+// the state once before the first iteration and then every few rounds.  The results equal
+// those of solve() with the same objective, bit for bit.
+template <typename R, typename H, typename S>
+static int solve_device(int n, R* x_user, const int* nbd, const R* l, const R* u,
+                        const typename Api<R>::Opt* opt, typename DevObjective<R>::Fn objective,
+                        void* user, cudaStream_t ustream, const lbfgsb_b200_ext* ext,
+                        typename Api<R>::Sum* summary) {
+  g_last_error.clear();
+  std::memset(&g_last_stats, 0, sizeof(g_last_stats));
+  if (!opt || !summary || !x_user || !nbd || !l || !u) return LBFGSB_B200_ERR_ARGUMENT;
+  if (opt->mode != LBFGSB_B200_MODE_CUDA) {
+    summary->info = -1;
+    return LBFGSB_B200_ERR_ARGUMENT;
+  }
+  const int m = std::min(opt->hessian_approximate_dimension, kMaxM);
+  if (n <= 0 || m <= 0 || m > n || opt->eps_f < 0 || opt->max_iteration < 0 ||
+      opt->eps_g < 0 || opt->eps_x < 0) {
+    summary->info = -1;
+    return LBFGSB_B200_OK;
+  }
+  if (!objective) {
+    summary->info = -1;
+    return LBFGSB_B200_ERR_ARGUMENT;
+  }
+  long long syncs = 0, rounds_launched = 0, launches = 0;
+  try {
+    RoundStream& rs = round_stream();
+    const cudaStream_t stream = rs.s;
+    CK(cudaEventRecord(rs.in, ustream));
+    CK(cudaStreamWaitEvent(stream, rs.in, 0));
+    Workspace<R, H, S> w;
+    w.s = stream;
+    const size_t N = (size_t)n;
+    Ctx<R, H, S> c;
+    Plan p;
+    prepare<R, H, S>(w, c, p, n, m, nbd, l, u, stream, ext, true);
+    EvalSlots* slot = w.template alloc<EvalSlots>(1);
+    c.ev_x = reinterpret_cast<R**>(&slot->x);
+    c.ev_g = reinterpret_cast<R**>(&slot->g);
+    c.ev_f = &slot->f;
+    c.ev_act = &slot->active;
+    c.gdummy = w.template alloc<R>(N);
+    DevState<S>& hs = *w.hs;
+    hs.phase = PH_ITER;
+    hs.eps_g = (S)opt->eps_g;
+    hs.eps_x = (S)opt->eps_x;
+    hs.eps_f = (S)opt->eps_f;
+    hs.max_iteration = opt->max_iteration;
+    hs.res_x = (S)summary->residual_x;  // left as given unless a test reaches them
+    hs.res_f = (S)summary->residual_f;
+    CK(cudaMemcpyAsync(w.st, &hs, sizeof(hs), cudaMemcpyHostToDevice, stream));
+    const size_t header = offsetof(DevState<S>, big);
+    auto pull = [&]() {
+      CK(cudaMemcpyAsync(w.hs, w.st, header, cudaMemcpyDeviceToHost, stream));
+      CK(cudaStreamSynchronize(stream));
+      syncs++;
+      if (w.hs->device_error) throw CudaFailure{cudaErrorLaunchTimeout, "staged-tile wait", __LINE__};
+    };
+    k_init<R, S><<<p.g_elem, 256, 0, stream>>>(n, x_user, w.X[0], nbd, l, u, w.st);
+    CK(cudaGetLastError());
+    launches++;
+    pull();
+    bool done = false;
+    if (hs.input_error) {
+      summary->info = -1;  // x is left as given (lbfgsbcpu.cpp:259-264)
+      done = true;
+    }
+    if (!done) {
+      // the first evaluation, at x0, and projgr there (lbfgsbcpu.cpp:266-276)
+      c.rounds = 1;
+      EvalSlots* hslot = static_cast<EvalSlots*>(pinned_mirror_slot(sizeof(EvalSlots)));
+      hslot->x = w.X[0];
+      hslot->g = w.G[0];
+      hslot->f = 0;
+      hslot->active = 1;
+      CK(cudaMemcpyAsync(slot, hslot, sizeof(EvalSlots), cudaMemcpyHostToDevice, stream));
+      objective(user, (const R* const*)c.ev_x, c.ev_g, c.ev_f, c.ev_act, (void*)stream);
+      CK(cudaGetLastError());
+      k_projgr<R, H, S><<<p.g_proj, kThreads, 0, stream>>>(c, nullptr, nullptr, S(0));
+      CK(cudaGetLastError());
+      launches++;
+      pull();
+      summary->residual_g = (R)hs.sbgnrm;
+      if (hs.sbgnrm <= (S)opt->eps_g) {
+        summary->info = 4;
+        done = true;
+      }
+    }
+    if (!done) {
+      const bool fused = hs.cnstnd != 0;
+      auto round = [&]() {
+        k_round_begin<R, H, S><<<1, 32, 0, stream>>>(c);
+        c.stages = p.gcp.stages;
+        k_gcp_scan<R, H, S, kConsWide><<<p.gcp.grid, p.gcp.threads, p.gcp.smem, stream>>>(c, nullptr, nullptr);
+        k_walk_gather<R, H, S><<<p.g_elem, kThreads, 0, stream>>>(c, nullptr, nullptr);
+        k_walk<R, H, S><<<1, kWalkThreads, 0, stream>>>(c, nullptr, nullptr);
+        c.stages = p.freev.stages;
+        k_freev_formk<R, H, S, kConsWide><<<p.freev.grid, p.freev.threads, p.freev.smem, stream>>>(c, nullptr, nullptr);
+        c.stages = p.dir.stages;
+        k_subsm_dir<R, H, S, kConsWide><<<p.dir.grid, p.dir.threads, p.dir.smem, stream>>>(c, nullptr, nullptr, nullptr);
+        c.stages = p.apply.stages;
+        k_subsm_apply<R, H, S, kConsWide><<<p.apply.grid, p.apply.threads, p.apply.smem, stream>>>(c, nullptr, nullptr, nullptr);
+        k_pre_eval<R, H, S><<<1, 32, 0, stream>>>(c);
+        k_trial_round<R, H, S><<<p.g_elem, 256, 0, stream>>>(c);
+        objective(user, (const R* const*)c.ev_x, c.ev_g, c.ev_f, c.ev_act, (void*)stream);
+        if (fused) {
+          c.stages = p.pgcp.stages;
+          k_post_gcp<R, H, S, kConsWide><<<p.pgcp.grid, p.pgcp.threads, p.pgcp.smem, stream>>>(
+              c, nullptr, nullptr, nullptr, nullptr, nullptr, S(0), 0);
+        } else {
+          c.stages = p.post.stages;
+          k_post_eval<R, H, S, kConsWide><<<p.post.grid, p.post.threads, p.post.smem, stream>>>(
+              c, nullptr, nullptr, nullptr, nullptr, nullptr, S(0), 0);
+        }
+        k_post_round<R, H, S><<<1, 32, 0, stream>>>(c);
+      };
+      constexpr int kRoundKernels = 12;
+      RoundGraph rg;
+      CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      round();
+      const cudaError_t launch_err = cudaGetLastError();
+      const cudaError_t cap_err = cudaStreamEndCapture(stream, &rg.g);
+      CK(launch_err);
+      CK(cap_err);
+      CK(cudaGraphInstantiate(&rg.e, rg.g, 0));
+      // rounds between two reads of the state: few at first, then about a quarter of the
+      // rounds so far (a finished solve idles through at most that many rounds)
+      int batch = 4;
+      while (true) {
+        for (int r = 0; r < batch; r++) CK(cudaGraphLaunch(rg.e, stream));
+        rounds_launched += batch;
+        pull();
+        if (hs.phase == PH_DONE) break;
+        batch = (int)std::min<long long>(64, std::max<long long>(4, rounds_launched / 4));
+      }
+      launches += rounds_launched * kRoundKernels;
+      summary->info = hs.info_final;
+      summary->num_iteration = hs.iter;
+      summary->residual_g = (R)hs.res_g;
+      summary->residual_x = (R)hs.res_x;
+      summary->residual_f = (R)hs.res_f;
+    }
+    if (!hs.input_error) {
+      CK(cudaMemcpyAsync(x_user, w.X[hs.xr[0]], N * sizeof(R), cudaMemcpyDeviceToDevice, stream));
+    }
+    CK(cudaEventRecord(rs.out, stream));
+    CK(cudaStreamWaitEvent(ustream, rs.out, 0));
+    w.release();  // the workspace returns to the pool on the solve's stream
+    CK(cudaStreamSynchronize(stream));
+    lbfgsb_b200_stats& st = g_last_stats;
+    st.kernels = 0;
+    st.total_launches = launches;
+    st.host_syncs = syncs;
+    st.evaluations = hs.nfgv + 1;
+    st.rounds = rounds_launched;
+  } catch (const CudaFailure& e) {
+    char buf[256];
+    std::snprintf(buf, sizeof(buf), "%s failed at driver.cu:%d: %s", e.call, e.line,
+                  cudaGetErrorString(e.err));
+    g_last_error = buf;
+    return LBFGSB_B200_ERR_CUDA;
+  }
+  return LBFGSB_B200_OK;
+}
+
 template <typename R, typename Opt>
 static void default_option(Opt* o, R meps, R mmax) {
   o->eps_f = o->eps_g = o->eps_x = (R)1e-15;
@@ -911,6 +1192,32 @@ int lbfgsb_b200_minimize_ext_f32(int n, float* x, const int* nbd, const float* l
                                                ext, summary);
   return solve<float, float, float>(n, x, nbd, l, u, option, funcgrad, after_iteration,
                                     customized_stopping, user, s, ext, summary);
+}
+
+int lbfgsb_b200_minimize_device_f64(int n, double* x, const int* nbd, const double* l,
+                                    const double* u, const lbfgsb_b200_option_f64* option,
+                                    lbfgsb_b200_device_objective_f64 objective, void* user,
+                                    void* stream, const lbfgsb_b200_ext* ext,
+                                    lbfgsb_b200_summary_f64* summary) {
+  return solve_device<double, double, double>(n, x, nbd, l, u, option, objective, user,
+                                              (cudaStream_t)stream, ext, summary);
+}
+
+int lbfgsb_b200_minimize_device_f32(int n, float* x, const int* nbd, const float* l,
+                                    const float* u, const lbfgsb_b200_option_f32* option,
+                                    lbfgsb_b200_device_objective_f32 objective, void* user,
+                                    void* stream, const lbfgsb_b200_ext* ext,
+                                    lbfgsb_b200_summary_f32* summary) {
+  const int form = ext ? ext->form : LBFGSB_B200_FORM_PLAIN;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (form == LBFGSB_B200_FORM_MIXED)
+    return solve_device<float, float, double>(n, x, nbd, l, u, option, objective, user, s, ext,
+                                              summary);
+  if (form == LBFGSB_B200_FORM_MIXED_BF16)
+    return solve_device<float, __nv_bfloat16, double>(n, x, nbd, l, u, option, objective, user,
+                                                      s, ext, summary);
+  return solve_device<float, float, float>(n, x, nbd, l, u, option, objective, user, s, ext,
+                                           summary);
 }
 
 int lbfgsb_b200_minimize_f64(int n, double* x, const int* nbd, const double* l,

@@ -39,6 +39,13 @@ __device__ __forceinline__ void rsincos(double v, double* s, double* c) { sincos
 __device__ __forceinline__ void rsincos(float v, float* s, float* c) { sincosf(v, s, c); }
 
 template <typename R, typename F>
+__device__ __forceinline__ void synth_body(int s, const R* __restrict__ x, const F* __restrict__ kap,
+                                           const F* __restrict__ w, const F* __restrict__ tt,
+                                           const F* __restrict__ b, R* __restrict__ g,
+                                           double* part, unsigned int* ticket, double f0,
+                                           double* fout, CtaPos cp);
+
+template <typename R, typename F>
 __global__ void __launch_bounds__(kThreads) k_synth(int s, const R* __restrict__ x,
                                                     const F* __restrict__ kap,
                                                     const F* __restrict__ w,
@@ -46,11 +53,35 @@ __global__ void __launch_bounds__(kThreads) k_synth(int s, const R* __restrict__
                                                     const F* __restrict__ b, R* __restrict__ g,
                                                     double* part, unsigned int* ticket,
                                                     double f0, double* fout) {
+  synth_body<R, F>(s, x, kap, w, tt, b, g, part, ticket, f0, fout, cta_here());
+}
+
+// The device-driven form: x and g are read from device memory (the solver's evaluation
+// slot), f is left in device memory, and nothing runs when the evaluation is not used.
+template <typename R, typename F>
+__global__ void __launch_bounds__(kThreads) k_synth_slot(int s, const R* const* xs,
+                                                         const F* __restrict__ kap,
+                                                         const F* __restrict__ w,
+                                                         const F* __restrict__ tt,
+                                                         const F* __restrict__ b, R* const* gs,
+                                                         const int* active, double* part,
+                                                         unsigned int* ticket, double f0,
+                                                         double* fout) {
+  if (!*active) return;
+  synth_body<R, F>(s, *xs, kap, w, tt, b, *gs, part, ticket, f0, fout, cta_here());
+}
+
+template <typename R, typename F>
+__device__ __forceinline__ void synth_body(int s, const R* __restrict__ x, const F* __restrict__ kap,
+                                           const F* __restrict__ w, const F* __restrict__ tt,
+                                           const F* __restrict__ b, R* __restrict__ g,
+                                           double* part, unsigned int* ticket, double f0,
+                                           double* fout, CtaPos cp) {
   const long long n = (long long)s * s;
   const R h = R(1) / (R)(s + 1), h2 = h * h;
   double acc = 0.0;
-  for (long long k = (long long)blockIdx.x * kThreads + threadIdx.x; k < n;
-       k += (long long)gridDim.x * kThreads) {
+  for (long long k = (long long)cp.rank * kThreads + threadIdx.x; k < n;
+       k += (long long)cp.count * kThreads) {
     const int i = (int)(k % s), j = (int)(k / s);
     const R xk = x[k];
     const R xe = (i + 1 < s) ? x[k + 1] : R(0);
@@ -75,11 +106,30 @@ __global__ void __launch_bounds__(kThreads) k_synth(int s, const R* __restrict__
   }
   double sarr[1] = {acc}, xd[1] = {0.0}, ld[1] = {0.0};
   MinPair md[1] = {MinPair{0.0, 0}};
-  cta_reduce_to_row<kThreads, 1, 0, 0, 0>(sarr, xd, md, ld, part, 1);
-  if (!last_cta(ticket)) return;
+  cta_reduce_to_row<kThreads, 1, 0, 0, 0>(sarr, xd, md, ld, part, 1, cp.rank);
+  if (!last_cta(ticket, cp.count)) return;
   __shared__ double red[1];
-  fold_rows<kThreads>(part, gridDim.x, 1, 1, 0, 0, red);
+  fold_rows<kThreads>(part, cp.count, 1, 1, 0, 0, red);
   if (threadIdx.x == 0) *fout = red[0] - f0;
+}
+
+template <typename R>
+static int synth_device(void* handle, const R* const* x, R* const* g, double* f,
+                        const int* active, void* stream) {
+  SynthCtx* c = static_cast<SynthCtx*>(handle);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (c->single) {
+    k_synth_slot<R, float><<<c->grid[sizeof(R) == 8 ? 0 : 1], kThreads, 0, s>>>(
+        c->s, x, (const float*)c->field[0], (const float*)c->field[1],
+        (const float*)c->field[2], (const float*)c->field[3], g, active, c->part, c->ticket,
+        c->f0, f);
+  } else {
+    k_synth_slot<R, double><<<c->grid[sizeof(R) == 8 ? 0 : 1], kThreads, 0, s>>>(
+        c->s, x, (const double*)c->field[0], (const double*)c->field[1],
+        (const double*)c->field[2], (const double*)c->field[3], g, active, c->part, c->ticket,
+        c->f0, f);
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 
 template <typename R>
@@ -186,6 +236,16 @@ int lbfgsb_b200_synth_funcgrad_f64(void* handle, double* x, double* f, double* g
 int lbfgsb_b200_synth_funcgrad_f32(void* handle, float* x, float* f, float* g, void* stream,
                                    const lbfgsb_b200_summary_f32*) {
   return synth_eval<float>(handle, x, f, g, stream);
+}
+
+int lbfgsb_b200_synth_device_f64(void* handle, const double* const* x, double* const* g,
+                                 double* f, const int* active, void* stream) {
+  return synth_device<double>(handle, x, g, f, active, stream);
+}
+
+int lbfgsb_b200_synth_device_f32(void* handle, const float* const* x, float* const* g,
+                                 double* f, const int* active, void* stream) {
+  return synth_device<float>(handle, x, g, f, active, stream);
 }
 
 }  // extern "C"

@@ -53,6 +53,19 @@ struct Ctx {
   double* wl_t;      // breakpoint list (walk)
   int* wl_i;
   unsigned int* wl_n;
+  // device-driven solves: rounds = 1 makes every pass gate itself on the round plan in the
+  // state and take its vectors from the buffers below by the roles st->xr / st->gr
+  int rounds;
+  R* X[3];
+  R* G[2];
+  R* gdummy;         // g of evaluations whose result is not used
+  // where the objective of a device-driven solve reads x (*ev_x) and writes g (*ev_g) and
+  // f (*ev_f); *ev_act = 0 marks an evaluation whose result is not used (device memory;
+  // a batch keeps each of them as one array over its instances)
+  R** ev_x;
+  R** ev_g;
+  double* ev_f;
+  int* ev_act;
 };
 
 // Physical slot pointers of ring positions 1..kMaxM counted from head.
@@ -315,9 +328,15 @@ __device__ void gcp_epilogue(DevState<S>* st, const double* red, int col, SmallW
 // ------------------------------------------------------------------------------------
 // A: the Cauchy-point scan.
 template <typename R, typename H, typename S, int CONS>
-__global__ void __launch_bounds__(CONS + 32) k_gcp_scan(Ctx<R, H, S> c, const R* __restrict__ x,
+__device__ __forceinline__ void gcp_scan_pass(const Ctx<R, H, S>& c, CtaPos cp, int stages,
+    const R* __restrict__ x,
                                                        const R* __restrict__ g) {
   DevState<S>* st = c.st;
+  if (c.rounds) {
+    if (!st->rp_scan) return;
+    x = c.X[st->xr[0]];
+    g = c.G[st->gr[0]];
+  }
   const int n = c.n, col = st->col;
   // sums: [0] sum neggi^2, [1..16] p (y part 1..8, s part 9..16), [17] nbreak,
   // [18] movable variables without breakpoint; max: [0] any such with g != 0;
@@ -349,8 +368,8 @@ __global__ void __launch_bounds__(CONS + 32) k_gcp_scan(Ctx<R, H, S> c, const R*
   const int cap = stage_capacity(StageBytes<R>::gcp, 0, st->m, (int)sizeof(H));
   dispatch_cols(col, [&](auto cols_tag) {
     constexpr bool kFull = decltype(cols_tag)::value == kMaxM;
-    run_tiles<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
-              &st->device_error, [&](const unsigned char* buf, long long t, int valid, int e) {
+    run_tiles<CONS>(ss, n, stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)stages * cap),
+              &st->device_error, cp, [&](const unsigned char* buf, long long t, int valid, int e) {
       if (e >= valid) return;
       const long long i = t * kTile + e;
       const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
@@ -384,14 +403,20 @@ __global__ void __launch_bounds__(CONS + 32) k_gcp_scan(Ctx<R, H, S> c, const R*
   });
   constexpr int W = NS + NX + 2 * NM;
   double lo[1] = {0.0};
-  cta_reduce_to_row<CONS + 32, NS, NX, NM, 0>(s, xm, mn, lo, c.part, W);
-  if (!last_cta(c.ticket)) return;
+  cta_reduce_to_row<CONS + 32, NS, NX, NM, 0>(s, xm, mn, lo, c.part, W, cp.rank);
+  if (!last_cta(c.ticket, cp.count)) return;
   __shared__ double red[W];
-  fold_rows<CONS + 32>(c.part, gridDim.x, W, NS, NX, NM, red);
+  fold_rows<CONS + 32>(c.part, cp.count, W, NS, NX, NM, red);
   __shared__ SmallWork<S> sw;
   epilogue_on_shared_warp<S>(st, [&](DevState<S>* st, int lane) {
     gcp_epilogue<S>(st, red, col, sw, lane);
   });
+}
+
+template <typename R, typename H, typename S, int CONS>
+__global__ void __launch_bounds__(CONS + 32) k_gcp_scan(Ctx<R, H, S> c,
+    const R* __restrict__ x, const R* __restrict__ g) {
+  gcp_scan_pass<R, H, S, CONS>(c, cta_here(), c.stages, x, g);
 }
 
 // ------------------------------------------------------------------------------------
@@ -419,9 +444,15 @@ __host__ __device__ inline void corr_map(int q, int& kind, int& a, int& b) {
 }
 
 template <typename R, typename H, typename S, int CONS>
-__global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const R* __restrict__ x,
+__device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos cp, int stages,
+    const R* __restrict__ x,
                                                           const R* __restrict__ g) {
   DevState<S>* st = c.st;
+  if (c.rounds) {
+    if (!st->rp_sub) return;
+    x = c.X[st->xr[0]];
+    g = c.G[st->gr[0]];
+  }
   if (st->gcp_state == GCP_WALK || st->internal_fail != 0) return;
   const int n = c.n, col = st->col, iter = st->iter;
   const bool uncon = st->uncon_branch != 0;
@@ -580,8 +611,8 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const
       }
     };
     const bool need_row = updatd && col > 0;
-    run_stages<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
-                     &st->device_error, [&](const unsigned char* buf, long long t, int valid,
+    run_stages<CONS>(ss, n, stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)stages * cap),
+                     &st->device_error, cp, [&](const unsigned char* buf, long long t, int valid,
                                             auto release) {
       if (role == 0) {
   #pragma unroll
@@ -621,7 +652,7 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const
       if (lane == 0 && role == 0) wsum[warp][2 * kMaxM + k] = v;
     }
     __syncthreads();
-    double* row = c.part + (size_t)blockIdx.x * W;
+    double* row = c.part + (size_t)cp.rank * W;
     for (int k = threadIdx.x; k < W; k += CONS + 32) {
       double a = 0.0;
       if (k < NS) {
@@ -632,9 +663,9 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const
       row[k] = a;
     }
   }
-  if (!last_cta(c.ticket)) return;
+  if (!last_cta(c.ticket, cp.count)) return;
   __shared__ double red[W];
-  fold_rows<CONS + 32>(c.part, gridDim.x, W, W, 0, 0, red);
+  fold_rows<CONS + 32>(c.part, cp.count, W, W, 0, 0, red);
   __shared__ SmallWork<S> sw;
   __shared__ S wn1_snap[4 * kMaxM * kMaxM];
   epilogue_on_shared_warp<S>(st, [&](DevState<S>* st, int lane) {
@@ -705,6 +736,12 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c, const
     wdtrsl1(st->wn, 2 * kMaxM, 2 * col, wv, lane);  // the same diagonal: no zero
     if (lane < 2 * col) st->wv[lane + 1] = wv[lane + 1];
   });
+}
+
+template <typename R, typename H, typename S, int CONS>
+__global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c,
+    const R* __restrict__ x, const R* __restrict__ g) {
+  freev_formk_pass<R, H, S, CONS>(c, cta_here(), c.stages, x, g);
 }
 
 // lnsrlb's per-variable start at the subspace point z (lbfgsbcpu.cpp:1263-1299): d = z - x,
@@ -793,9 +830,16 @@ struct DirElem {
 // ------------------------------------------------------------------------------------
 // C: subspace direction on the free set and the step to the first bound it meets.
 template <typename R, typename H, typename S, int CONS>
-__global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c, const R* __restrict__ x,
+__device__ __forceinline__ void subsm_dir_pass(const Ctx<R, H, S>& c, CtaPos cp, int stages,
+    const R* __restrict__ x,
                                                         const R* __restrict__ g, R* __restrict__ z) {
   DevState<S>* st = c.st;
+  if (c.rounds) {
+    if (!st->rp_sub) return;
+    x = c.X[st->xr[0]];
+    g = c.G[st->gr[0]];
+    z = c.X[st->xr[1]];
+  }
   if (st->gcp_state == GCP_WALK || st->internal_fail != 0 || !st->subsm_active) return;
   const int n = c.n, col = st->col;
   const bool uncon = st->uncon_branch != 0;
@@ -845,8 +889,8 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c, const R
     constexpr bool kFull = decltype(cols_tag)::value == kMaxM;
     // each thread reads its variable's inputs and history row into registers and the stage
     // is released before the arithmetic, so that the producer refills it sooner
-    run_tiles_split<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
-              &st->device_error, [&](const unsigned char* buf, long long t, int valid, int e) {
+    run_tiles_split<CONS>(ss, n, stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)stages * cap),
+              &st->device_error, cp, [&](const unsigned char* buf, long long t, int valid, int e) {
       DirElem<R, S> v{};
       if (e < valid) {
         v.code = stage_at<int8_t>(buf, o_code, e);
@@ -935,11 +979,11 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c, const R
   constexpr int W = 7;
   // (the pipeline ends with a block barrier, so every thread's flag store is visible)
   double xm[1] = {s_projected ? 1.0 : 0.0}, ldum[1] = {0.0};
-  cta_reduce_to_row<CONS + 32, 2, 1, 2, 0>(sl, xm, mn, ldum, c.part, W);
-  if (!last_cta(c.ticket)) return;
+  cta_reduce_to_row<CONS + 32, 2, 1, 2, 0>(sl, xm, mn, ldum, c.part, W, cp.rank);
+  if (!last_cta(c.ticket, cp.count)) return;
   __shared__ double red[W];
   __shared__ double rl[3];
-  fold_rows<CONS + 32>(c.part, gridDim.x, W, 2, 1, 2, red);
+  fold_rows<CONS + 32>(c.part, cp.count, W, 2, 1, 2, red);
   epilogue_on_shared<S>(st, [&](DevState<S>* st) {
     // the 3.0 step keeps the projected point when it gives a descent direction from x
     // (g'd <= 0 over the written z); otherwise, and always with the 2.1 step, the step is
@@ -967,12 +1011,25 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c, const R
   });
 }
 
+template <typename R, typename H, typename S, int CONS>
+__global__ void __launch_bounds__(CONS + 32) k_subsm_dir(Ctx<R, H, S> c,
+    const R* __restrict__ x, const R* __restrict__ g, R* __restrict__ z) {
+  subsm_dir_pass<R, H, S, CONS>(c, cta_here(), c.stages, x, g, z);
+}
+
 // ------------------------------------------------------------------------------------
 // D: apply the subspace step, form z and d = z - x, and start the line search.
 template <typename R, typename H, typename S, int CONS>
-__global__ void __launch_bounds__(CONS + 32) k_subsm_apply(Ctx<R, H, S> c, const R* __restrict__ x,
+__device__ __forceinline__ void subsm_apply_pass(const Ctx<R, H, S>& c, CtaPos cp, int stages,
+    const R* __restrict__ x,
                                                           const R* __restrict__ g, R* __restrict__ z) {
   DevState<S>* st = c.st;
+  if (c.rounds) {
+    if (!st->rp_sub) return;
+    x = c.X[st->xr[0]];
+    g = c.G[st->gr[0]];
+    z = c.X[st->xr[1]];
+  }
   if (st->gcp_state == GCP_WALK || st->internal_fail != 0 || st->spec_apply) return;
   const int n = c.n;
   const bool uncon = st->uncon_branch != 0;
@@ -1000,8 +1057,8 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_apply(Ctx<R, H, S> c, const
   const int o_code = ss.off[0], o_x = ss.off[1], o_g = ss.off[2], o_l = ss.off[3];
   const int o_u = ss.off[4], o_ds = ss.off[5], o_nb = ss.off[6];
   const int cap = stage_capacity(StageBytes<R>::apply, 0, 0, (int)sizeof(H));
-  run_tiles<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
-            &st->device_error, [&](const unsigned char* buf, long long t, int valid, int e) {
+  run_tiles<CONS>(ss, n, stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)stages * cap),
+            &st->device_error, cp, [&](const unsigned char* buf, long long t, int valid, int e) {
     if (e >= valid) return;
     const long long i = t * kTile + e;
     const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
@@ -1027,27 +1084,49 @@ __global__ void __launch_bounds__(CONS + 32) k_subsm_apply(Ctx<R, H, S> c, const
   });
   constexpr int W = 4;
   double xdum[1] = {0.0}, ldum[1] = {0.0};
-  cta_reduce_to_row<CONS + 32, 2, 0, 1, 0>(s, xdum, mn, ldum, c.part, W);
-  if (!last_cta(c.ticket)) return;
+  cta_reduce_to_row<CONS + 32, 2, 0, 1, 0>(s, xdum, mn, ldum, c.part, W, cp.rank);
+  if (!last_cta(c.ticket, cp.count)) return;
   __shared__ double red[W];
-  fold_rows<CONS + 32>(c.part, gridDim.x, W, 2, 0, 1, red);
+  fold_rows<CONS + 32>(c.part, cp.count, W, 2, 0, 1, red);
   epilogue_on_shared<S>(st, [&](DevState<S>* st) {
 
     lnsrlb_start<S>(st, red);
   });
 }
 
+template <typename R, typename H, typename S, int CONS>
+__global__ void __launch_bounds__(CONS + 32) k_subsm_apply(Ctx<R, H, S> c,
+    const R* __restrict__ x, const R* __restrict__ g, R* __restrict__ z) {
+  subsm_apply_pass<R, H, S, CONS>(c, cta_here(), c.stages, x, g, z);
+}
+
 // Trial point x = stp*d + t with d = z - t (lbfgsbcpu.cpp:1332-1334).
 template <typename R, typename S>
-__global__ void k_trial(int n, const R* __restrict__ t, const R* __restrict__ z, R* __restrict__ xt,
-                        const DevState<S>* st) {
+__device__ __forceinline__ void trial_point(int n, const R* __restrict__ t, const R* __restrict__ z,
+                                            R* __restrict__ xt, const DevState<S>* st, CtaPos cp) {
   const R stp = (R)st->stp;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
+  for (long long i = (long long)cp.rank * blockDim.x + threadIdx.x; i < n;
+       i += (long long)cp.count * blockDim.x) {
     const R ti = t[i];
     const R d = rsub(z[i], ti);
     xt[i] = radd(rmul(stp, d), ti);
   }
+}
+template <typename R, typename S>
+__global__ void k_trial(int n, const R* __restrict__ t, const R* __restrict__ z, R* __restrict__ xt,
+                        const DevState<S>* st) {
+  trial_point<R, S>(n, t, z, xt, st, cta_here());
+}
+// The trial point of a device-driven round, when the round evaluates at stp != 1.
+template <typename R, typename H, typename S>
+__device__ __forceinline__ void trial_round_pass(const Ctx<R, H, S>& c, CtaPos cp) {
+  const DevState<S>* st = c.st;
+  if (!st->ev_trial) return;
+  trial_point<R, S>(c.n, c.X[st->xr[0]], c.X[st->xr[1]], c.X[st->xr[2]], st, cp);
+}
+template <typename R, typename H, typename S>
+__global__ void k_trial_round(Ctx<R, H, S> c) {
+  trial_round_pass<R, H, S>(c, cta_here());
 }
 
 // The epilogue after a function evaluation: g'd and dcsrch (lbfgsbcpu.cpp:1312-1338); on
@@ -1150,13 +1229,24 @@ __device__ bool post_epilogue(DevState<S>* st, const double* red, S f, int force
 // E: after a function evaluation at xt (gradient gt; t and go are the point and the
 // gradient where the line search started).
 template <typename R, typename H, typename S, int CONS>
-__global__ void __launch_bounds__(CONS + 32) k_post_eval(Ctx<R, H, S> c, const R* __restrict__ t,
+__device__ __forceinline__ void post_eval_pass(const Ctx<R, H, S>& c, CtaPos cp, int stages,
+    const R* __restrict__ t,
                                                         const R* __restrict__ z,
                                                         const R* __restrict__ xt,
                                                         const R* __restrict__ gt,
                                                         const R* __restrict__ go, S f,
                                                         int force_accept) {
   DevState<S>* st = c.st;
+  if (c.rounds) {
+    if (!(st->ev_active || st->ev_force)) return;
+    t = c.X[st->xr[0]];
+    z = c.X[st->xr[1]];
+    xt = st->ev_is_z ? z : c.X[st->xr[2]];
+    gt = c.G[st->gr[1]];
+    go = c.G[st->gr[0]];
+    force_accept = st->ev_force;
+    f = st->ev_force ? st->f : (S)(R)*c.ev_f;
+  }
   const int n = c.n, col = st->col;
   const R stp = (R)st->stp;
   const bool unit = st->stp == S(1);
@@ -1193,8 +1283,8 @@ __global__ void __launch_bounds__(CONS + 32) k_post_eval(Ctx<R, H, S> c, const R
   const int cap = stage_capacity(StageBytes<R>::post, 0, st->m, (int)sizeof(H));
   dispatch_cols(col, [&](auto cols_tag) {
     constexpr bool kFull = decltype(cols_tag)::value == kMaxM;
-    run_tiles<CONS>(ss, n, c.stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap),
-              &st->device_error, [&](const unsigned char* buf, long long tt, int valid, int e) {
+    run_tiles<CONS>(ss, n, stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)stages * cap),
+              &st->device_error, cp, [&](const unsigned char* buf, long long tt, int valid, int e) {
       if (e >= valid) return;
       const long long i = tt * kTile + e;
       const R ti = stage_at<R>(buf, o_t, e), zi = stage_at<R>(buf, o_z, e);
@@ -1233,23 +1323,31 @@ __global__ void __launch_bounds__(CONS + 32) k_post_eval(Ctx<R, H, S> c, const R
   constexpr int W = NS + NX;
   MinPair mdum[1] = {MinPair{0.0, 0}};
   double ldum[1] = {0.0};
-  cta_reduce_to_row<CONS + 32, NS, NX, 0, 0>(s, xm, mdum, ldum, c.part, W);
-  if (!last_cta(c.ticket)) return;
+  cta_reduce_to_row<CONS + 32, NS, NX, 0, 0>(s, xm, mdum, ldum, c.part, W, cp.rank);
+  if (!last_cta(c.ticket, cp.count)) return;
   __shared__ double red[W];
-  fold_rows<CONS + 32>(c.part, gridDim.x, W, NS, NX, 0, red);
+  fold_rows<CONS + 32>(c.part, cp.count, W, NS, NX, 0, red);
   epilogue_on_shared_warp<S>(st, [&](DevState<S>* st, int lane) {
     post_epilogue<S>(st, red, f, force_accept, lane);
   });
 }
 
+template <typename R, typename H, typename S, int CONS>
+__global__ void __launch_bounds__(CONS + 32) k_post_eval(Ctx<R, H, S> c,
+    const R* __restrict__ t, const R* __restrict__ z, const R* __restrict__ xt,
+    const R* __restrict__ gt, const R* __restrict__ go, S f, int force_accept) {
+  post_eval_pass<R, H, S, CONS>(c, cta_here(), c.stages, t, z, xt, gt, go, f, force_accept);
+}
+
 // ------------------------------------------------------------------------------------
 // Set-up: errclb (871-905), lbfgsbactive (467-515) into the solver's x buffer.
 template <typename R, typename S>
-__global__ void k_init(int n, const R* __restrict__ x_in, R* __restrict__ x, const int* __restrict__ nbd,
-                       const R* __restrict__ l, const R* __restrict__ u, DevState<S>* st) {
+__device__ __forceinline__ void init_pass(int n, const R* __restrict__ x_in, R* __restrict__ x,
+                                          const int* __restrict__ nbd, const R* __restrict__ l,
+                                          const R* __restrict__ u, DevState<S>* st, CtaPos cp) {
   int err = 0, any_c = 0, not_boxed = 0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
+  for (long long i = (long long)cp.rank * blockDim.x + threadIdx.x; i < n;
+       i += (long long)cp.count * blockDim.x) {
     const int nb = nbd[i];
     const R li = l[i], ui = u[i];
     R xi = x_in[i];
@@ -1275,14 +1373,24 @@ __global__ void k_init(int n, const R* __restrict__ x_in, R* __restrict__ x, con
     if (not_boxed) atomicAnd(&st->boxed, 0);
   }
 }
+template <typename R, typename S>
+__global__ void k_init(int n, const R* __restrict__ x_in, R* __restrict__ x, const int* __restrict__ nbd,
+                       const R* __restrict__ l, const R* __restrict__ u, DevState<S>* st) {
+  init_pass<R, S>(n, x_in, x, nbd, l, u, st, cta_here());
+}
 
 // projgr at the start point (lbfgsbcpu.cpp:272-273); also records f.
 template <typename R, typename H, typename S>
-__global__ void __launch_bounds__(kThreads) k_projgr(Ctx<R, H, S> c, const R* __restrict__ x,
-                                                     const R* __restrict__ g, S f) {
+__device__ __forceinline__ void projgr_pass(const Ctx<R, H, S>& c, CtaPos cp, const R* __restrict__ x,
+                                            const R* __restrict__ g, S f) {
+  if (c.rounds) {
+    x = c.X[c.st->xr[0]];
+    g = c.G[c.st->gr[0]];
+    f = (S)(R)*c.ev_f;
+  }
   double xm[1] = {0.0};
-  for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < c.n;
-       i += (long long)gridDim.x * kThreads) {
+  for (long long i = (long long)cp.rank * kThreads + threadIdx.x; i < c.n;
+       i += (long long)cp.count * kThreads) {
     const R xi = x[i], gi = g[i];
     const int nb = c.nbd[i];
     R pg = gi;
@@ -1298,13 +1406,19 @@ __global__ void __launch_bounds__(kThreads) k_projgr(Ctx<R, H, S> c, const R* __
   }
   double sdum[1] = {0.0}, ldum[1] = {0.0};
   MinPair mdum[1] = {MinPair{0.0, 0}};
-  cta_reduce_to_row<kThreads, 0, 1, 0, 0>(sdum, xm, mdum, ldum, c.part, 1);
-  if (!last_cta(c.ticket)) return;
+  cta_reduce_to_row<kThreads, 0, 1, 0, 0>(sdum, xm, mdum, ldum, c.part, 1, cp.rank);
+  if (!last_cta(c.ticket, cp.count)) return;
   __shared__ double red[1];
-  fold_rows<kThreads>(c.part, gridDim.x, 1, 0, 1, 0, red);
+  fold_rows<kThreads>(c.part, cp.count, 1, 0, 1, 0, red);
   if (threadIdx.x != 0) return;
   c.st->sbgnrm = (S)red[0];
   c.st->f = f;
+  c.st->res_g = (S)red[0];
+}
+template <typename R, typename H, typename S>
+__global__ void __launch_bounds__(kThreads) k_projgr(Ctx<R, H, S> c, const R* __restrict__ x,
+                                                     const R* __restrict__ g, S f) {
+  projgr_pass<R, H, S>(c, cta_here(), x, g, f);
 }
 
 // The memory reset of the reference driver (col = 0, head = 1, theta = 1, iupdat = 0,
@@ -1364,7 +1478,8 @@ __device__ __forceinline__ double stored_value(double v) {
 // runs cauchy's epilogue on the reordered sums, and marks spec_gcp so that the host skips
 // the separate scan.  A rejected trial leaves codes that the next trial overwrites.
 template <typename R, typename H, typename S, int CONS>
-__global__ void __launch_bounds__(CONS + 32) k_post_gcp(Ctx<R, H, S> c, const R* __restrict__ t,
+__device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, int stages,
+    const R* __restrict__ t,
                                                        const R* __restrict__ z,
                                                        const R* __restrict__ xt,
                                                        const R* __restrict__ gt,
@@ -1372,6 +1487,16 @@ __global__ void __launch_bounds__(CONS + 32) k_post_gcp(Ctx<R, H, S> c, const R*
                                                        int force_accept) {
   static_assert(CONS == 512, "the role split assumes 16 consumer warps");
   DevState<S>* st = c.st;
+  if (c.rounds) {
+    if (!(st->ev_active || st->ev_force)) return;
+    t = c.X[st->xr[0]];
+    z = c.X[st->xr[1]];
+    xt = st->ev_is_z ? z : c.X[st->xr[2]];
+    gt = c.G[st->gr[1]];
+    go = c.G[st->gr[0]];
+    force_accept = st->ev_force;
+    f = st->ev_force ? st->f : (S)(R)*c.ev_f;
+  }
   const int n = c.n, col = st->col;
   const R stp = (R)st->stp;
   const bool unit = st->stp == S(1);
@@ -1490,8 +1615,8 @@ __global__ void __launch_bounds__(CONS + 32) k_post_gcp(Ctx<R, H, S> c, const R*
         }
       }
     };
-    run_stages<CONS>(ss, n, c.stages, dyn,
-                     reinterpret_cast<uint64_t*>(dyn + (size_t)c.stages * cap), &st->device_error,
+    run_stages<CONS>(ss, n, stages, dyn,
+                     reinterpret_cast<uint64_t*>(dyn + (size_t)stages * cap), &st->device_error, cp,
                      [&](const unsigned char* buf, long long tt, int valid, auto release) {
       if (role == 0) {
 #pragma unroll
@@ -1525,7 +1650,7 @@ __global__ void __launch_bounds__(CONS + 32) k_post_gcp(Ctx<R, H, S> c, const R*
       wsum[warp][NS + 3] = role == 1 ? (double)mv.i : (double)kNoIndex;
     }
     __syncthreads();
-    double* row = c.part + (size_t)blockIdx.x * W;
+    double* row = c.part + (size_t)cp.rank * W;
     for (int k = threadIdx.x; k < W; k += CONS + 32) {
       if (k < NS) {
         double a = 0.0;
@@ -1544,9 +1669,9 @@ __global__ void __launch_bounds__(CONS + 32) k_post_gcp(Ctx<R, H, S> c, const R*
       }
     }
   }
-  if (!last_cta(c.ticket)) return;
+  if (!last_cta(c.ticket, cp.count)) return;
   __shared__ double red[W];
-  fold_rows<CONS + 32>(c.part, gridDim.x, W, NS, 2, 1, red);
+  fold_rows<CONS + 32>(c.part, cp.count, W, NS, 2, 1, red);
   __shared__ SmallWork<S> sw;
   __shared__ double rp[NP + 1], rg[22];  // epilogue temporaries (shared, as all of them)
   epilogue_on_shared_warp<S>(st, [&](DevState<S>* st, int lane) {
@@ -1597,6 +1722,13 @@ __global__ void __launch_bounds__(CONS + 32) k_post_gcp(Ctx<R, H, S> c, const R*
     gcp_epilogue<S>(st, rg, ncol, sw, lane);
     if (lane == 0) st->spec_gcp = 1;
   });
+}
+
+template <typename R, typename H, typename S, int CONS>
+__global__ void __launch_bounds__(CONS + 32) k_post_gcp(Ctx<R, H, S> c,
+    const R* __restrict__ t, const R* __restrict__ z, const R* __restrict__ xt,
+    const R* __restrict__ gt, const R* __restrict__ go, S f, int force_accept) {
+  post_gcp_pass<R, H, S, CONS>(c, cta_here(), c.stages, t, z, xt, gt, go, f, force_accept);
 }
 
 }  // namespace lbfgsb_b200

@@ -1,7 +1,7 @@
 // reduce.cuh -- deterministic grid reductions for the streaming passes.
 //
 // Each CTA reduces its threads' accumulators (warp butterflies, then a fixed-order sum
-// over warps) into one row of `part` (gridDim.x rows).  The CTA that finishes last (an
+// over warps) into one row of `part` (one row per CTA of the instance, by rank).  The CTA that finishes last (an
 // atomic ticket after a fence) folds the rows in CTA order and runs the pass epilogue.
 // The order of every addition is fixed by the launch shape, so results are bitwise
 // reproducible from run to run.
@@ -43,14 +43,14 @@ struct RowLayout {
   static constexpr int kWidth = NS + NX + 2 * NM;
 };
 
-// CTA-level reduction of per-thread values into part[blockIdx.x * W + ...].  `lane_owned`
+// CTA-level reduction of per-thread values into part[rank * W + ...].  `lane_owned`
 // values (one distinct output per lane, NL per lane) are summed across warps only.
 template <int NT, int NS, int NX, int NM, int NL = 0>
 __device__ __forceinline__ void cta_reduce_to_row(const double (&s)[NS > 0 ? NS : 1],
                                                   const double (&x)[NX > 0 ? NX : 1],
                                                   const MinPair (&mn)[NM > 0 ? NM : 1],
                                                   const double (&lo)[NL > 0 ? NL : 1],
-                                                  double* part, int width) {
+                                                  double* part, int width, int rank) {
   constexpr int kWarps = NT / 32;
   constexpr int kVals = NS + NX + 2 * NM + 32 * NL;
   __shared__ double sm[kWarps][kVals > 0 ? kVals : 1];
@@ -76,7 +76,7 @@ __device__ __forceinline__ void cta_reduce_to_row(const double (&s)[NS > 0 ? NS 
 #pragma unroll
   for (int k = 0; k < NL; k++) sm[warp][NS + NX + 2 * NM + 32 * k + lane] = lo[k];
   __syncthreads();
-  double* row = part + (size_t)blockIdx.x * width;
+  double* row = part + (size_t)rank * width;
   for (int k = threadIdx.x; k < kVals; k += NT) {
     if (k >= NS && k < NS + NX) {
       double a = sm[0][k];
@@ -96,15 +96,15 @@ __device__ __forceinline__ void cta_reduce_to_row(const double (&s)[NS > 0 ? NS 
   }
 }
 
-// Ticket: returns true in exactly one CTA (the last to arrive), after all rows are
-// visible.  Resets the ticket for the next launch.
-__device__ __forceinline__ bool last_cta(unsigned int* ticket) {
+// Ticket: returns true in exactly one of the instance's `count` CTAs (the last to
+// arrive), after all rows are visible.  Resets the ticket for the next launch.
+__device__ __forceinline__ bool last_cta(unsigned int* ticket, int count) {
   __shared__ bool am_last;
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
     unsigned int t = atomicAdd(ticket, 1u);
-    am_last = (t == gridDim.x - 1);
+    am_last = (t == (unsigned int)count - 1u);
   }
   __syncthreads();
   if (am_last) {

@@ -14,6 +14,10 @@ namespace lbfgsb_b200 {
 
 // gcp_state
 enum : int { GCP_DONE = 0, GCP_WALK = 1, GCP_EARLY = 2, GCP_SKIPPED = 3 };
+// phase of a device-driven solve, what its next round does: start an iteration, evaluate
+// the line search's next trial point, accept the 20th backtrack without evaluating it (the
+// reference's exit from the search, lbfgsbcpu.cpp:352-358), or nothing (finished)
+enum : int { PH_ITER = 0, PH_LS = 1, PH_QUIRK = 2, PH_DONE = 3 };
 // ls_task: 1 = evaluate f, g at the trial point, 5 = the line search has converged
 // fail codes (internal_fail): nonzero requests the memory reset of the reference driver.
 
@@ -33,10 +37,23 @@ struct DevState {
   int spec_apply;     // 1: the direction pass also applied the (untruncated) step
   int dir_no_spec;    // 1 after a truncated step: the next direction pass does not try
   int subsm_proj;     // 1: the L-BFGS-B 3.0 subspace step (projection), 0: the 2.1 step
+  // device-driven solves (rounds.cuh): the round plan and the outer loop's decisions
+  int phase;          // PH_*
+  int reset_pending;  // the next iteration starts with the memory reset
+  int rp_scan, rp_sub;  // this round runs cauchy's scan / the walk and the subspace passes
+  int ev_active, ev_force, ev_is_z, ev_trial;  // this round's evaluation (see k_pre_eval)
+  int xr[3];          // roles of the x buffers: [0] the iterate, [1] z, [2] the trial point
+  int gr[2];          // roles of the g buffers: [0] at the iterate, [1] at the trial point
+  int info_final;     // summary.info once phase == PH_DONE
+  int max_iteration;  // option.max_iteration
+  int rounds;         // rounds run so far
+  int pad_rounds;
   unsigned long long free_hash, free_hash_acc, at_lower, at_upper;
   S theta, f, fold, gd, gdold, stp, dnrm, dtd, xstep, stpmx;
   S sbgnrm, tf, rr, dr, ddum_dr;
   S f1, f2, f2org, dtm, tsum, tj, bkmin, alpha, f1_0, f2_0;
+  S eps_g, eps_x, eps_f;        // the stopping tolerances (device-driven solves)
+  S res_g, res_x, res_f;        // summary.residual_* as the host loop would leave them
   // ---------------- large part ----------------
   S big;  // marks the end of the header
   int phys[kMaxM + 1];  // physical history slot of ring index r = 1..m

@@ -130,8 +130,8 @@ __device__ __forceinline__ void load_tile(const StreamSet& ss, long long t, long
 constexpr int kMaxStages = 8;
 
 // Warp-specialised tile pipeline.  The CTA has CONSUMERS + 32 threads: the last warp is
-// the producer, which issues the copies of the CTA's tiles (grid-stride over the n
-// elements) into a ring of `stages` stage buffers; the consumer threads run
+// the producer, which issues the copies of the CTA's tiles (tiles rank, rank + count, ...
+// of the instance's n elements) into a ring of `stages` stage buffers; the consumer threads run
 // body(buf, t, valid) once per tile.  full[s] completes when the bytes of the tile in
 // stage s have landed; empty[s] completes when every consumer warp has finished with it.
 // There is no CTA-wide barrier per tile, and the producer issues a freed stage's next
@@ -144,7 +144,7 @@ constexpr int kMaxStages = 8;
 template <int CONSUMERS, typename Body>
 __device__ __forceinline__ bool run_stages(const StreamSet& ss, long long n, int stages,
                                            unsigned char* ring, uint64_t* bars, int* err,
-                                           Body&& body) {
+                                           CtaPos cp, Body&& body) {
   constexpr int kConsumerWarps = CONSUMERS / 32;
   uint64_t* full = bars;
   uint64_t* empty = bars + stages;
@@ -163,7 +163,7 @@ __device__ __forceinline__ bool run_stages(const StreamSet& ss, long long n, int
   if (warp == kConsumerWarps) {
     // producer
     long long k = 0;
-    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, k++) {
+    for (long long t = cp.rank; t < ntiles; t += cp.count, k++) {
       const int s = (int)(k % stages);
       if (k >= stages) {
         const uint32_t parity = (uint32_t)(((k / stages) - 1) & 1);
@@ -180,7 +180,7 @@ __device__ __forceinline__ bool run_stages(const StreamSet& ss, long long n, int
   } else {
     // consumers
     long long k = 0;
-    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, k++) {
+    for (long long t = cp.rank; t < ntiles; t += cp.count, k++) {
       const int s = (int)(k % stages);
       const unsigned char* buf = ring + (size_t)s * ss.stage_bytes;
       const bool ok = __all_sync(0xffffffffu, mbar_wait(&full[s], (uint32_t)((k / stages) & 1)));
@@ -217,8 +217,8 @@ __device__ __forceinline__ bool run_stages(const StreamSet& ss, long long n, int
 template <int CONSUMERS, typename Body>
 __device__ __forceinline__ bool run_tiles(const StreamSet& ss, long long n, int stages,
                                           unsigned char* ring, uint64_t* bars, int* err,
-                                          Body&& body) {
-  return run_stages<CONSUMERS>(ss, n, stages, ring, bars, err,
+                                          CtaPos cp, Body&& body) {
+  return run_stages<CONSUMERS>(ss, n, stages, ring, bars, err, cp,
                                [&](const unsigned char* buf, long long t, int valid, auto release) {
 #pragma unroll
     for (int h = 0; h < kTile / CONSUMERS; h++)
@@ -232,9 +232,9 @@ __device__ __forceinline__ bool run_tiles(const StreamSet& ss, long long n, int 
 template <int CONSUMERS, typename Load, typename Compute>
 __device__ __forceinline__ bool run_tiles_split(const StreamSet& ss, long long n, int stages,
                                                 unsigned char* ring, uint64_t* bars, int* err,
-                                                Load&& load, Compute&& compute) {
+                                                CtaPos cp, Load&& load, Compute&& compute) {
   static_assert(kTile == CONSUMERS, "one element per consumer thread and tile");
-  return run_stages<CONSUMERS>(ss, n, stages, ring, bars, err,
+  return run_stages<CONSUMERS>(ss, n, stages, ring, bars, err, cp,
                                [&](const unsigned char* buf, long long t, int valid, auto release) {
     const int e = (int)threadIdx.x;
     const auto v = load(buf, t, valid, e);

@@ -22,12 +22,18 @@
 namespace lbfgsb_b200 {
 
 template <typename R, typename H, typename S>
-__global__ void __launch_bounds__(kThreads) k_walk_gather(Ctx<R, H, S> c, const R* __restrict__ x,
-                                                          const R* __restrict__ g) {
+__device__ __forceinline__ void walk_gather_pass(const Ctx<R, H, S>& c, CtaPos cp,
+                                                 const R* __restrict__ x, const R* __restrict__ g) {
+  if (c.rounds) {
+    const DevState<S>* st = c.st;
+    if (!st->rp_sub || st->gcp_state != GCP_WALK || st->internal_fail != 0) return;
+    x = c.X[st->xr[0]];
+    g = c.G[st->gr[0]];
+  }
   const int n = c.n;
   const int lane = threadIdx.x & 31;
-  for (long long base = (long long)blockIdx.x * kThreads; base < n;
-       base += (long long)gridDim.x * kThreads) {
+  for (long long base = (long long)cp.rank * kThreads; base < n;
+       base += (long long)cp.count * kThreads) {
     const long long i = base + threadIdx.x;
     bool has_bp = false;
     R t = 0;
@@ -43,6 +49,11 @@ __global__ void __launch_bounds__(kThreads) k_walk_gather(Ctx<R, H, S> c, const 
       c.wl_i[pos] = (int)i;
     }
   }
+}
+template <typename R, typename H, typename S>
+__global__ void __launch_bounds__(kThreads) k_walk_gather(Ctx<R, H, S> c, const R* __restrict__ x,
+                                                          const R* __restrict__ g) {
+  walk_gather_pass<R, H, S>(c, cta_here(), x, g);
 }
 
 constexpr int kWalkThreads = 512;
@@ -84,9 +95,14 @@ __device__ __forceinline__ void key_set_digit(Key96& k, int level, int d) {
 }
 
 template <typename R, typename H, typename S>
-__global__ void __launch_bounds__(kWalkThreads) k_walk(Ctx<R, H, S> c, const R* __restrict__ x,
-                                                       const R* __restrict__ g) {
+__device__ __forceinline__ void walk_pass(const Ctx<R, H, S>& c, const R* __restrict__ x,
+                                          const R* __restrict__ g) {
   DevState<S>* st = c.st;
+  if (c.rounds) {
+    if (!st->rp_sub || st->internal_fail != 0) return;
+    x = c.X[st->xr[0]];
+    g = c.G[st->gr[0]];
+  }
   if (st->gcp_state != GCP_WALK) return;
   const int n = c.n, col = st->col, col2 = 2 * col;
   const long long L = *c.wl_n;
@@ -317,6 +333,11 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(Ctx<R, H, S> c, const R* 
     }
   }
   st->gcp_state = GCP_DONE;
+}
+template <typename R, typename H, typename S>
+__global__ void __launch_bounds__(kWalkThreads) k_walk(Ctx<R, H, S> c, const R* __restrict__ x,
+                                                       const R* __restrict__ g) {
+  walk_pass<R, H, S>(c, x, g);
 }
 
 }  // namespace lbfgsb_b200

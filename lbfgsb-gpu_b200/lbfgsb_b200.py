@@ -71,7 +71,7 @@ class Stats(C.Structure):
                 ("launches", C.c_longlong * MAX_KERNELS), ("ms", C.c_double * MAX_KERNELS),
                 ("bytes", C.c_double * MAX_KERNELS), ("total_launches", C.c_longlong),
                 ("host_syncs", C.c_longlong), ("evaluations", C.c_longlong),
-                ("bytes_per_iteration_model", C.c_double)]
+                ("bytes_per_iteration_model", C.c_double), ("rounds", C.c_longlong)]
 
 
 CB64 = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
@@ -93,6 +93,8 @@ EXPORTS = [
     "lbfgsb_b200_minimize_batch_f64", "lbfgsb_b200_minimize_batch_f32",
     "lbfgsb_b200_workspace_bytes", "lbfgsb_b200_server_create", "lbfgsb_b200_server_submit_f32",
     "lbfgsb_b200_server_wait", "lbfgsb_b200_server_peak", "lbfgsb_b200_server_destroy",
+    "lbfgsb_b200_minimize_device_f64", "lbfgsb_b200_minimize_device_f32",
+    "lbfgsb_b200_synth_device_f64", "lbfgsb_b200_synth_device_f32",
 ]
 
 _lib = None
@@ -122,6 +124,11 @@ def load() -> C.CDLL:
         fn = getattr(lib, f"lbfgsb_b200_default_option_{sfx}")
         fn.restype = None
         fn.argtypes = [C.POINTER(opt)]
+        fn = getattr(lib, f"lbfgsb_b200_minimize_device_{sfx}")
+        fn.restype = C.c_int
+        fn.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                       C.POINTER(opt), C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Ext),
+                       C.POINTER(summ)]
     lib.lbfgsb_b200_last_stats.restype = C.c_int
     lib.lbfgsb_b200_last_stats.argtypes = [C.POINTER(Stats)]
     lib.lbfgsb_b200_last_error.restype = C.c_char_p
@@ -183,7 +190,7 @@ def last_stats() -> dict:
     st = Stats()
     load().lbfgsb_b200_last_stats(C.byref(st))
     out = {"kernels": {}, "total_launches": st.total_launches, "host_syncs": st.host_syncs,
-           "evaluations": st.evaluations,
+           "evaluations": st.evaluations, "rounds": st.rounds,
            "bytes_per_iteration_model": st.bytes_per_iteration_model}
     for k in range(st.kernels):
         name = bytes(st.name[k]).split(b"\0", 1)[0].decode()
@@ -295,6 +302,9 @@ class SynthObjective:
             lib.lbfgsb_b200_synth_set_offset(self.handle, float(prob["f_offset"]))
         self.f64 = C.cast(lib.lbfgsb_b200_synth_funcgrad_f64, C.c_void_p).value
         self.f32 = C.cast(lib.lbfgsb_b200_synth_funcgrad_f32, C.c_void_p).value
+        # the device-driven forms (lbfgsb_b200_device_objective_*)
+        self.d64 = C.cast(lib.lbfgsb_b200_synth_device_f64, C.c_void_p).value
+        self.d32 = C.cast(lib.lbfgsb_b200_synth_device_f32, C.c_void_p).value
 
     def close(self):
         if self.handle:
@@ -356,11 +366,13 @@ _TRACE_KEYS = [f for f, _ in TraceRecord._fields_]
 def solve(prob: dict, dtype=np.float64, x0=None, option=None, objective: str = "host",
           form: int = FORM_PLAIN, trace: bool = False, record: bool = True,
           custom_stop_at: int | None = None, profile: bool = False, stream=None,
-          subsm_projection: bool = False) -> GpuResult:
+          subsm_projection: bool = False, driven: str = "host") -> GpuResult:
     """One solve on the GPU through the C ABI.
 
     subsm_projection: the L-BFGS-B 3.0 subspace step (lbfgsb_b200_ext.subsm_projection)
     instead of the reference's 2.1 step.
+    driven="device": lbfgsb_b200_minimize_device with the device synthetic objective (the
+    outer loop on the device; objective must be "device", no trace or callbacks).
 
     objective="host": funcgrad copies x to the host and evaluates the CPU objective of
     oracle/objective.c (so f and g are bit-identical to what the oracle sees);
@@ -446,10 +458,18 @@ def solve(prob: dict, dtype=np.float64, x0=None, option=None, objective: str = "
     keep.append(cb_tr)
     ext = Ext(form, 1 if profile else 0, cb_tr, None, 1 if subsm_projection else 0)
     sfx = "f64" if is64 else "f32"
-    fn = getattr(lib, f"lbfgsb_b200_minimize_ext_{sfx}")
     torch.cuda.synchronize()
-    status = fn(n, x.data_ptr(), nbd.data_ptr(), l.data_ptr(), u.data_ptr(), C.byref(opt),
-                fg_ptr, after_ptr, stop_ptr, user, stream, C.byref(ext), C.byref(summ))
+    if driven == "device":
+        if objective != "device" or trace or custom_stop_at is not None:
+            raise ValueError("a device-driven solve takes the device objective and no callbacks")
+        so = keep[0]
+        fn = getattr(lib, f"lbfgsb_b200_minimize_device_{sfx}")
+        status = fn(n, x.data_ptr(), nbd.data_ptr(), l.data_ptr(), u.data_ptr(), C.byref(opt),
+                    so.d64 if is64 else so.d32, so.handle, stream, C.byref(ext), C.byref(summ))
+    else:
+        fn = getattr(lib, f"lbfgsb_b200_minimize_ext_{sfx}")
+        status = fn(n, x.data_ptr(), nbd.data_ptr(), l.data_ptr(), u.data_ptr(), C.byref(opt),
+                    fg_ptr, after_ptr, stop_ptr, user, stream, C.byref(ext), C.byref(summ))
     torch.cuda.synchronize()
     if status != 0:
         raise RuntimeError(f"lbfgsb_b200 status {status}: {lib.lbfgsb_b200_last_error()}")
