@@ -257,6 +257,51 @@ int lbfgsb_b200_minimize_device_f32(int n, float* x, const int* nbd, const float
                                     void* stream, const lbfgsb_b200_ext* ext,
                                     lbfgsb_b200_summary_f32* summary);
 
+/* ---- batched device-driven solves (no counterpart in the reference) -----------------
+ * `count` independent instances of possibly different sizes n[k] (device arrays x[k] in /
+ * out, nbd[k], l[k], u[k]; one option set; ids[k] the id the objective sees for instance k,
+ * or ids = NULL for 0..count-1) solved together: every pass of a round is one launch for
+ * all live instances (instance k gets its own contiguous range of CTAs, sized by its n from
+ * a tuned table), the rounds are captured into a CUDA graph, converged instances are
+ * retired and the launches shrink to the rest.  Each instance's workspace is one segment of
+ * the library's pool.  An instance's results do not depend on the other instances of the
+ * batch (it runs the same launches on its own reduction rows); status[k] is its return
+ * code.  ext->form, ext->subsm_projection apply; the other ext fields are ignored.
+ *
+ * The objective evaluates a list of instances at once, enqueued on `stream` with nothing
+ * synchronised (it is captured with the round): `count` entries, entry j being instance
+ * ids[j]; x[j] (device) holds the pointer to that instance's x, g[j] the pointer to its
+ * gradient, f[j] receives its f (double), and active[j] = 0 marks an entry whose result is
+ * not used this round.  ids, x, g, f and active are device arrays of `count` entries.
+ * first (device, count + 1 entries) is a suggested launch shape: entry j may use CTAs
+ * first[j] .. first[j+1]-1 of a launch of `ctas` CTAs of 256 threads (at most 64 each). */
+typedef int (*lbfgsb_b200_batch_objective_f64)(void* user, int count, const int* ids,
+                                               const int* first, int ctas,
+                                               const double* const* x, double* const* g,
+                                               double* f, const int* active, void* stream);
+typedef int (*lbfgsb_b200_batch_objective_f32)(void* user, int count, const int* ids,
+                                               const int* first, int ctas,
+                                               const float* const* x, float* const* g,
+                                               double* f, const int* active, void* stream);
+int lbfgsb_b200_minimize_batch_device_f64(int count, const int* ids, const int* n,
+                                          double* const* x, const int* const* nbd,
+                                          const double* const* l, const double* const* u,
+                                          const lbfgsb_b200_option_f64* option,
+                                          lbfgsb_b200_batch_objective_f64 objective, void* user,
+                                          void* stream, const lbfgsb_b200_ext* ext,
+                                          lbfgsb_b200_summary_f64* summary, int* status);
+int lbfgsb_b200_minimize_batch_device_f32(int count, const int* ids, const int* n,
+                                          float* const* x, const int* const* nbd,
+                                          const float* const* l, const float* const* u,
+                                          const lbfgsb_b200_option_f32* option,
+                                          lbfgsb_b200_batch_objective_f32 objective, void* user,
+                                          void* stream, const lbfgsb_b200_ext* ext,
+                                          lbfgsb_b200_summary_f32* summary, int* status);
+/* Override the tuned tiles per CTA of the batched passes for instances in size bucket
+ * `bucket` (0: n <= 4096, 1: <= 16384, 2: <= 65536, 3: <= 262144, 4: larger); 0 restores
+ * the tuned value.  For the autotuner. */
+int lbfgsb_b200_batch_tiles_per_cta(int bucket, int tiles);
+
 /* Statistics of the calling thread's last solve. */
 #define LBFGSB_B200_MAX_KERNELS 16
 typedef struct {
@@ -308,6 +353,25 @@ int lbfgsb_b200_synth_device_f64(void* handle, const double* const* x, double* c
                                  double* f, const int* active, void* stream);
 int lbfgsb_b200_synth_device_f32(void* handle, const float* const* x, float* const* g,
                                  double* f, const int* active, void* stream);
+
+/* A batch of synthetic problems generated on the device (test and benchmark glue): problem
+ * p is the grid problem of side sides[p] whose fields, nbd and bounds are those the host
+ * generator lbfgsb-gpu_b200/synth.py gives for seed seeds[p] (same counter-based draws,
+ * bit-identical).  Fields are stored in float (single_precision_fields) or double; l, u in
+ * the solver precision real_size (4 or 8).  _problem gives problem p's device arrays; the
+ * _f64 / _f32 functions are its batched objective (lbfgsb_b200_batch_objective_*), the id of
+ * an entry being the problem index p. */
+void* lbfgsb_b200_synth_batch_create(int count, const int* sides, const unsigned long long* seeds,
+                                     int single_precision_fields, int real_size);
+void lbfgsb_b200_synth_batch_destroy(void* handle);
+int lbfgsb_b200_synth_batch_problem(void* handle, int p, void** l, void** u, int** nbd,
+                                    void* fields[4]);
+int lbfgsb_b200_synth_batch_f64(void* handle, int count, const int* ids, const int* first,
+                                int ctas, const double* const* x, double* const* g, double* f,
+                                const int* active, void* stream);
+int lbfgsb_b200_synth_batch_f32(void* handle, int count, const int* ids, const int* first,
+                                int ctas, const float* const* x, float* const* g, double* f,
+                                const int* active, void* stream);
 
 /* ---- dsscfg objective (the reference example's objective, examples/dsscfg/dsscfg_cuda.cu)
  * The MINPACK-2 steady-state combustion problem on an nx x ny grid with parameter lambda,

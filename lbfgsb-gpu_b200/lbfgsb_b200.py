@@ -95,6 +95,10 @@ EXPORTS = [
     "lbfgsb_b200_server_wait", "lbfgsb_b200_server_peak", "lbfgsb_b200_server_destroy",
     "lbfgsb_b200_minimize_device_f64", "lbfgsb_b200_minimize_device_f32",
     "lbfgsb_b200_synth_device_f64", "lbfgsb_b200_synth_device_f32",
+    "lbfgsb_b200_minimize_batch_device_f64", "lbfgsb_b200_minimize_batch_device_f32",
+    "lbfgsb_b200_batch_tiles_per_cta", "lbfgsb_b200_synth_batch_create",
+    "lbfgsb_b200_synth_batch_destroy", "lbfgsb_b200_synth_batch_problem",
+    "lbfgsb_b200_synth_batch_f64", "lbfgsb_b200_synth_batch_f32",
 ]
 
 _lib = None
@@ -146,6 +150,22 @@ def load() -> C.CDLL:
         fn.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                        C.POINTER(opt), C.c_void_p, C.c_void_p, C.c_int, C.POINTER(summ),
                        C.c_void_p, C.c_void_p]
+    for sfx, opt, summ in (("f64", OptionF64, SummaryF64), ("f32", OptionF32, SummaryF32)):
+        fn = getattr(lib, f"lbfgsb_b200_minimize_batch_device_{sfx}")
+        fn.restype = C.c_int
+        fn.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                       C.c_void_p, C.POINTER(opt), C.c_void_p, C.c_void_p, C.c_void_p,
+                       C.POINTER(Ext), C.POINTER(summ), C.c_void_p]
+    lib.lbfgsb_b200_batch_tiles_per_cta.restype = C.c_int
+    lib.lbfgsb_b200_batch_tiles_per_cta.argtypes = [C.c_int, C.c_int]
+    lib.lbfgsb_b200_synth_batch_create.restype = C.c_void_p
+    lib.lbfgsb_b200_synth_batch_create.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int]
+    lib.lbfgsb_b200_synth_batch_destroy.restype = None
+    lib.lbfgsb_b200_synth_batch_destroy.argtypes = [C.c_void_p]
+    lib.lbfgsb_b200_synth_batch_problem.restype = C.c_int
+    lib.lbfgsb_b200_synth_batch_problem.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p),
+                                                    C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                                    C.c_void_p]
     lib.lbfgsb_b200_dsscfg_create.restype = C.c_void_p
     lib.lbfgsb_b200_dsscfg_create.argtypes = [C.c_int, C.c_int, C.c_double]
     lib.lbfgsb_b200_dsscfg_destroy.restype = None
@@ -339,6 +359,73 @@ def synth_value(prob: dict, x0=None) -> float:
     torch.cuda.synchronize()
     so.close()
     return float(f.value)
+
+
+class SynthBatch:
+    """A batch of synth.py problems generated on the device (lbfgsb_b200_synth_batch_*):
+    problem p has grid side sides[p] and seed seeds[p]; its l, u (in the solver precision)
+    and nbd stay on the device."""
+
+    def __init__(self, sides, seeds, single_precision_fields=True, dtype=np.float32):
+        lib = load()
+        self.count = len(sides)
+        self.sides = [int(v) for v in sides]
+        self.n = [v * v for v in self.sides]
+        self.dtype = np.dtype(dtype)
+        sd = (C.c_int * self.count)(*self.sides)
+        se = (C.c_ulonglong * self.count)(*[int(v) for v in seeds])
+        self.handle = lib.lbfgsb_b200_synth_batch_create(self.count, sd, se,
+                                                         1 if single_precision_fields else 0,
+                                                         self.dtype.itemsize)
+        if not self.handle:
+            raise RuntimeError("lbfgsb_b200_synth_batch_create failed")
+        self.objective = C.cast(lib.lbfgsb_b200_synth_batch_f64 if self.dtype == np.float64
+                                else lib.lbfgsb_b200_synth_batch_f32, C.c_void_p).value
+
+    def problem(self, p):
+        """(l, u, nbd, [kappa, w, t, b]) device pointers of problem p."""
+        lib = load()
+        l, u, nbd = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        fields = (C.c_void_p * 4)()
+        if lib.lbfgsb_b200_synth_batch_problem(self.handle, p, C.byref(l), C.byref(u),
+                                               C.byref(nbd), fields) != 0:
+            raise IndexError(p)
+        return l.value, u.value, nbd.value, [fields[k] for k in range(4)]
+
+    def close(self):
+        if self.handle:
+            load().lbfgsb_b200_synth_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def solve_batch_device(batch: "SynthBatch", xs, option, form: int = FORM_PLAIN,
+                       subsm_projection: bool = False, ids=None):
+    """lbfgsb_b200_minimize_batch_device over the problems `ids` (default all) of a
+    SynthBatch (the objective's ids are the batch's problem indices); xs: device tensors
+    (start points in, solutions out).  Returns (status, per-instance statuses, summaries,
+    stats)."""
+    lib = load()
+    ids = list(range(batch.count)) if ids is None else list(ids)
+    k = len(ids)
+    is64 = batch.dtype == np.float64
+    probs = [batch.problem(p) for p in ids]
+    n_arr = (C.c_int * k)(*[batch.n[p] for p in ids])
+    id_arr = (C.c_int * k)(*ids)
+    ptr = lambda v: (C.c_void_p * k)(*v)  # noqa: E731
+    summ = ((SummaryF64 if is64 else SummaryF32) * k)()
+    stat = (C.c_int * k)()
+    ext = Ext(form, 0, TRACE_CB(), None, 1 if subsm_projection else 0)
+    fn = lib.lbfgsb_b200_minimize_batch_device_f64 if is64 else lib.lbfgsb_b200_minimize_batch_device_f32
+    rc = fn(k, id_arr, n_arr, ptr([t.data_ptr() for t in xs]), ptr([p[2] for p in probs]),
+            ptr([p[0] for p in probs]), ptr([p[1] for p in probs]), C.byref(option),
+            batch.objective, batch.handle, None, C.byref(ext), summ, stat)
+    return rc, list(stat), list(summ), last_stats()
 
 
 def _digest(a: np.ndarray) -> str:
