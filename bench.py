@@ -436,150 +436,203 @@ def dsscfg_compare():
     return out
 
 
-def batched_compare(count: int = 256, workers: int = 16):
-    """A seeded sample of the batched workload (independent FP32 solves of the synthetic
-    bounded grid problem, each with its own seed, grid side log-uniform in [32, 512], m = 8,
-    eps_g = 1e-6, at most 500 iterations, device objectives): the same instances solved one
-    after another on one stream, then side by side by lbfgsb_b200_minimize_batch_f32 with
-    `workers` streams.  Reports solves/s of both, per-solve p50/p99 wall time in the batched
-    run, and whether both runs give identical results."""
+def _cpu_batch_worker(args):
+    """One reference CPU solve (oracle/_ref, lbfgsbcpu.cpp) of a batched-workload instance;
+    returns its wall seconds.  Runs in a spawned process."""
+    side, seed, eps_g, max_it = args
+    import sys as _sys
+    for _p in (REPO, os.path.join(REPO, "lbfgsb-gpu_b200")):
+        if _p not in _sys.path:
+            _sys.path.insert(0, _p)
+    import synth
+    from oracle import binding as OB
+    prob = dict(synth.synth_problem(int(side), seed=int(seed)), kind="synth")
+    o = OB.default_option(np.float32)
+    o.eps_g = eps_g
+    o.max_iteration = max_it
+    t0 = time.perf_counter()
+    OB.run_cpu("ref", prob, np.float32, option=o, record=False)
+    return time.perf_counter() - t0
+
+
+def batched_compare(count: int = 4096, seq_sample: int = 32, cpu_budget_s: float = 25.0):
+    """The batched workload: `count` independent FP32 solves of the synthetic bounded grid
+    problem, problem k with seed 100 + k and grid side log-uniform in [32, 512] (n 1,024 ..
+    262,144), m = 8, eps_g = 1e-6, at most 500 iterations.  Fields are generated on the
+    device (bit-identical to synth.py).  All of them are solved together by
+    lbfgsb_b200_minimize_batch_device_f32 (one launch per pass for every live instance);
+    the sequential baseline is the plain GPU form (lbfgsb_b200_minimize_f32, host-driven, the
+    reference's API) solving a sample of the same problems one after another (every
+    count/seq_sample-th problem), its rate taken as the sequential rate; the CPU baseline is
+    the reference's CPU path, one solve per host core, on the first problems for a bounded
+    time."""
     import torch
     import lbfgsb_b200 as LB
     import synth
+    lib = LB.load()
     rng = np.random.default_rng(3)
     sides = np.rint(np.exp(rng.uniform(np.log(32), np.log(512), count))).astype(int)
-    probs = [synth.synth_problem(int(s), seed=100 + k) for k, s in enumerate(sides)]
-    objs = [LB.SynthObjective(p, single_precision_fields=True) for p in probs]
-    dev = [dict(l=torch.from_numpy(p["l"].astype(np.float32)).cuda(),
-                u=torch.from_numpy(p["u"].astype(np.float32)).cuda(),
-                nbd=torch.from_numpy(p["nbd"]).cuda()) for p in probs]
+    seeds = [100 + k for k in range(count)]
+    bt = LB.SynthBatch(sides, seeds, single_precision_fields=True, dtype=np.float32)
     opt = LB.default_option(np.float32)
     opt.eps_g = 1e-6
     opt.max_iteration = 500
-    ns = [p["nbd"].size for p in probs]
-
-    def run(conc):
-        xs = [torch.zeros(n, dtype=torch.float32, device="cuda") for n in ns]
+    xs = [torch.zeros(int(n), dtype=torch.float32, device="cuda") for n in bt.n]
+    # warm the pool and the module on a few instances
+    LB.solve_batch_device(bt, xs[:8], opt, ids=list(range(8)))
+    for x in xs[:8]:
+        x.zero_()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    rc, stat, summ, st = LB.solve_batch_device(bt, xs, opt)
+    e1.record()
+    e1.synchronize()
+    if rc != 0:
+        raise RuntimeError(lib.lbfgsb_b200_last_error())
+    batched_s = e0.elapsed_time(e1) / 1000.0
+    its = np.array([sm.num_iteration for sm in summ])
+    infos = np.array([sm.info for sm in summ])
+    # sequential plain GPU solves of a sample of the same problems
+    sample = list(range(0, count, max(1, count // seq_sample)))[:seq_sample]
+    seq_s = 0.0
+    seq_its = []
+    for p in sample:
+        prob = synth.synth_problem(int(sides[p]), seed=seeds[p])
+        so = LB.SynthObjective(prob, single_precision_fields=True)
+        x = torch.zeros(int(bt.n[p]), dtype=torch.float32, device="cuda")
+        l = torch.from_numpy(prob["l"].astype(np.float32)).cuda()
+        u = torch.from_numpy(prob["u"].astype(np.float32)).cuda()
+        nbd = torch.from_numpy(prob["nbd"]).cuda()
+        sm = LB.SummaryF32()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        rc, stat, summ, secs = LB.solve_batch(ns, xs, [d["nbd"] for d in dev], [d["l"] for d in dev],
-                                              [d["u"] for d in dev], opt, objs[0].f32,
-                                              [o.handle for o in objs], concurrency=conc,
-                                              dtype=np.float32)
+        r = lib.lbfgsb_b200_minimize_f32(int(bt.n[p]), x.data_ptr(), nbd.data_ptr(), l.data_ptr(),
+                                         u.data_ptr(), C.byref(opt), so.f32, None, None, so.handle,
+                                         None, C.byref(sm))
         torch.cuda.synchronize()
-        wall = time.perf_counter() - t0
-        if rc != 0:
-            raise RuntimeError(LB.load().lbfgsb_b200_last_error())
-        return wall, xs, summ, secs
-
-    run(workers)  # warm the pool and the module for every size
-    wall1, x1, s1, _ = run(1)
-    wallb, xb, sb, secs = run(workers)
-    same = all(torch.equal(a, b) for a, b in zip(x1, xb)) and \
-        all((a.info, a.num_iteration) == (b.info, b.num_iteration) for a, b in zip(s1, sb))
-    for o in objs:
-        o.close()
-    its = np.array([s.num_iteration for s in sb])
-    return {"instances": count, "workers": workers, "n_total": int(sum(ns)),
-            "n_range": [int(min(ns)), int(max(ns))],
-            "sequential_solves_per_s": count / wall1, "batched_solves_per_s": count / wallb,
-            "speedup": wall1 / wallb,
-            "p50_solve_s": float(np.percentile(secs, 50)), "p99_solve_s": float(np.percentile(secs, 99)),
+        seq_s += time.perf_counter() - t0
+        seq_its.append(sm.num_iteration)
+        so.close()
+        if r != 0:
+            raise RuntimeError(lib.lbfgsb_b200_last_error())
+    seq_rate = len(sample) / seq_s
+    # reference CPU path, one solve per host core, on the first problems, bounded time
+    cpu = None
+    try:
+        from oracle import binding as OB
+        if OB.ref_available():
+            import multiprocessing as mp
+            cores = os.cpu_count() or 1
+            ctx = mp.get_context("spawn")
+            jobs = [(int(sides[p]), seeds[p], 1e-6, 500) for p in range(count)]
+            done = 0
+            t0 = time.perf_counter()
+            with ctx.Pool(cores) as pool:
+                for secs in pool.imap(_cpu_batch_worker, jobs[:cores * 4]):
+                    done += 1
+                    if time.perf_counter() - t0 > cpu_budget_s and done >= cores:
+                        break
+                pool.terminate()
+            wall = time.perf_counter() - t0
+            cpu = {"value": done / wall, "unit": "solves/s", "cores": cores, "kind": "reference",
+                   "sample": f"{done} of the same problems (the first ones), one reference "
+                             f"lbfgsbcpu.cpp solve per host core, {wall:.1f} s"}
+    except Exception as exc:  # noqa: BLE001 - the CPU baseline is reported, never required
+        cpu = {"unavailable": str(exc)[:200]}
+    bt.close()
+    return {"instances": count, "n_total": int(sum(bt.n)),
+            "n_range": [int(min(bt.n)), int(max(bt.n))],
+            "batched_solves_per_s": count / batched_s, "batched_seconds": batched_s,
+            "rounds": st["rounds"], "launches": st["total_launches"],
+            "host_syncs": st["host_syncs"],
             "iterations_mean": float(its.mean()), "iterations_max": int(its.max()),
-            "identical_results": bool(same),
-            "note": "a 256-instance sample of the 4096-instance workload; one worker stream per "
-                    "host thread, whole solves overlapped"}
+            "converged": int(np.sum(np.isin(infos, [1, 2, 4]))), "hit_max_iteration": int(np.sum(infos == 5)),
+            "sequential_plain_solves_per_s": seq_rate,
+            "sequential_sample": f"{len(sample)} of the problems (every {max(1, count // seq_sample)}th), "
+                                 "lbfgsb_b200_minimize_f32 one after another",
+            "sequential_iterations_mean": float(np.mean(seq_its)),
+            "speedup_vs_sequential": (count / batched_s) / seq_rate,
+            "cpu_baseline": cpu}
 
 
-def serving_compare(count: int = 64, rate: float = 2000.0, workers: int = 16):
-    """A bounded sample of the serving workload: `count` solve requests with Poisson
-    arrivals at `rate` per second, each a synthetic bounded grid problem with its own seed
-    and grid side log-uniform in [64, 2048] (n 4,096 .. 4,194,304), FP32 vectors with FP64
-    small-matrix steps, eps_g = 1e-6, at most 500 iterations, device objectives, admitted
-    against a 150 GB workspace budget by the library's server (lbfgsb_b200_server_*) on
-    `workers` streams; latency is submit to result.  The one-at-a-time baseline solves the
-    same requests alone, one after another, and its latencies are those of a first come,
-    first served single server with the same arrival times and the measured solve times."""
-    import ctypes as C
+def serving_compare(count: int = 400, rate: float = 2000.0, seq_sample: int = 16):
+    """A bounded sample of the serving workload: `count` solve requests with Poisson arrivals
+    at `rate` per second, request k a synthetic bounded grid problem with seed 500 + k and
+    grid side log-uniform in [64, 2048] (n 4,096 .. 4,194,304), FP32 vectors with FP64
+    small-matrix steps, eps_g = 1e-6, at most 500 iterations, admitted against a 150 GB HBM
+    budget by the continuous-batching server (lbfgsb_b200_batch_server_*); latency is submit
+    to result.  One-at-a-time baseline: the same solves one after another through the same
+    engine alone (a sample of every count/seq_sample-th request), replayed through a first
+    come, first served single server with the same arrivals."""
     import torch
     import lbfgsb_b200 as LB
-    import synth
     lib = LB.load()
     rng = np.random.default_rng(4)
     sides = np.rint(np.exp(rng.uniform(np.log(64), np.log(2048), count))).astype(int)
     gaps = rng.exponential(1.0 / rate, count)
     arrivals = np.cumsum(gaps) - gaps[0]
-    probs = [synth.synth_problem(int(s), seed=500 + k) for k, s in enumerate(sides)]
-    objs = [LB.SynthObjective(p, single_precision_fields=True) for p in probs]
-    dev = [dict(l=torch.from_numpy(p["l"].astype(np.float32)).cuda(),
-                u=torch.from_numpy(p["u"].astype(np.float32)).cuda(),
-                nbd=torch.from_numpy(p["nbd"]).cuda()) for p in probs]
-    ns = [p["nbd"].size for p in probs]
+    bt = LB.SynthBatch(sides, [500 + k for k in range(count)], single_precision_fields=True,
+                       dtype=np.float32)
     opt = LB.default_option(np.float32)
     opt.eps_g = 1e-6
     opt.max_iteration = 500
     form = LB.FORM_MIXED
-    ext = LB.Ext(form, 0, LB.TRACE_CB(), None)
-
-    def alone(k):
-        x = torch.zeros(ns[k], dtype=torch.float32, device="cuda")
-        summ = LB.SummaryF32()
+    xs = [torch.zeros(int(n), dtype=torch.float32, device="cuda") for n in bt.n]
+    # one-at-a-time solves of a sample (also warms the pool for the largest sizes)
+    sample = list(range(0, count, max(1, count // seq_sample)))[:seq_sample]
+    solo = {}
+    for p in sample:
+        x = torch.zeros(int(bt.n[p]), dtype=torch.float32, device="cuda")
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        st = lib.lbfgsb_b200_minimize_ext_f32(ns[k], x.data_ptr(), dev[k]["nbd"].data_ptr(),
-                                              dev[k]["l"].data_ptr(), dev[k]["u"].data_ptr(),
-                                              C.byref(opt), objs[k].f32, None, None,
-                                              objs[k].handle, None, C.byref(ext), C.byref(summ))
+        rc, stat, summ, _ = LB.solve_batch_device(bt, [x], opt, form=form, ids=[p])
         torch.cuda.synchronize()
-        if st != 0:
-            raise RuntimeError(lib.lbfgsb_b200_last_error().decode())
-        return time.perf_counter() - t0, x, summ
-
-    alone(int(np.argmax(ns)))  # grow the workspace pool once
-    solo = [alone(k) for k in range(count)]
-    finish, lat1 = 0.0, []
-    for a, (d, _, _) in zip(arrivals, solo):
-        finish = max(a, finish) + d
-        lat1.append(finish - a)
-    span1 = finish - arrivals[0]
-
-    sv = LB.Server(workers=workers, hbm_budget_bytes=150 * 10**9, form=form)
-    xs = [torch.zeros(n, dtype=torch.float32, device="cuda") for n in ns]
+        solo[p] = (time.perf_counter() - t0, x, summ[0])
+    mean_solo = float(np.mean([v[0] for v in solo.values()]))
+    sv = LB.BatchServer(bt, opt, hbm_budget_bytes=150 * 10**9, form=form, rounds_per_loop=4)
     torch.cuda.synchronize()
-    ids = []
+    tickets = []
     t0 = time.perf_counter()
     for k in range(count):
         delay = t0 + arrivals[k] - time.perf_counter()
         if delay > 0:
             time.sleep(delay)
-        rc, rid = sv.submit(ns[k], xs[k], dev[k]["nbd"], dev[k]["l"], dev[k]["u"], opt,
-                            objs[k].f32, objs[k].handle)
+        rc, t = sv.submit(k, xs[k])
         if rc != 0:
             raise RuntimeError(lib.lbfgsb_b200_last_error().decode())
-        ids.append(rid)
-    outs = [sv.wait(rid) for rid in ids]
+        tickets.append(t)
+    outs = [sv.wait(t) for t in tickets]
     span = time.perf_counter() - t0
-    peak_bytes, peak_running = sv.peak()
+    peak_bytes, peak_live = sv.peak()
     sv.close()
     torch.cuda.synchronize()
-    same = all(o[0] == 0 and torch.equal(xs[k], solo[k][1]) and
-               (o[1].info, o[1].num_iteration) == (solo[k][2].info, solo[k][2].num_iteration)
-               for k, o in enumerate(outs))
-    for o in objs:
-        o.close()
+    same = all(outs[p][0] == 0 and torch.equal(xs[p], solo[p][1]) and
+               (outs[p][1].info, outs[p][1].num_iteration) == (solo[p][2].info, solo[p][2].num_iteration)
+               for p in sample)
     lat = np.array([o[2] for o in outs])
     its = np.array([o[1].num_iteration for o in outs])
-    return {"requests": count, "offered_per_s": rate, "workers": workers,
-            "hbm_budget_gb": 150, "n_range": [int(min(ns)), int(max(ns))], "n_total": int(sum(ns)),
-            "solves_per_s": count / span, "p50_latency_s": float(np.percentile(lat, 50)),
+    # FCFS single server with the mean measured solo time per request
+    finish, lat1 = 0.0, []
+    for a in arrivals:
+        finish = max(a, finish) + mean_solo
+        lat1.append(finish - a)
+    bt.close()
+    return {"requests": count, "offered_per_s": rate, "arrival_span_s": float(arrivals[-1]),
+            "hbm_budget_gb": 150, "n_range": [int(min(bt.n)), int(max(bt.n))],
+            "n_total": int(sum(bt.n)), "solves_per_s": count / span,
+            "p50_latency_s": float(np.percentile(lat, 50)),
             "p99_latency_s": float(np.percentile(lat, 99)),
-            "one_at_a_time_solves_per_s": count / span1,
+            "peak_admitted": peak_live, "peak_workspace_gb": peak_bytes / 1e9,
+            "iterations_mean": float(its.mean()),
+            "one_at_a_time_solves_per_s": 1.0 / mean_solo,
             "one_at_a_time_p50_latency_s": float(np.percentile(lat1, 50)),
             "one_at_a_time_p99_latency_s": float(np.percentile(lat1, 99)),
-            "peak_admitted": peak_running, "peak_workspace_gb": peak_bytes / 1e9,
-            "iterations_mean": float(its.mean()), "identical_results": bool(same),
-            "note": f"a {count}-request sample of the 60 s stream at the same arrival rate "
-                    "(all arrive within a fraction of a second, so the queue builds up)"}
+            "one_at_a_time_sample": f"{len(sample)} requests solved alone (every "
+                                    f"{max(1, count // seq_sample)}th), mean {mean_solo:.3f} s",
+            "same_alone_and_in_mix": bool(same),
+            "note": f"{count} requests of the 60 s stream at the same arrival rate; the offered "
+                    "load exceeds the GPU's capacity, so the queue builds up"}
 
 
 def max_over_ranks(values, dist, device):

@@ -297,6 +297,37 @@ int lbfgsb_b200_minimize_batch_device_f32(int count, const int* ids, const int* 
                                           lbfgsb_b200_batch_objective_f32 objective, void* user,
                                           void* stream, const lbfgsb_b200_ext* ext,
                                           lbfgsb_b200_summary_f32* summary, int* status);
+/* Continuous-batching server for FP32 solves (no counterpart in the reference): one server
+ * thread keeps every admitted solve's state on the device and advances all of them together
+ * with the batched passes above.  Requests queue in arrival order and are admitted, first
+ * come first served, as soon as their workspace segment fits in `hbm_budget_bytes` beside
+ * the running solves; requests that arrive while others run join them at the next round,
+ * finished solves leave and free their memory for the queue.  `form` is the precision form
+ * of every request (LBFGSB_B200_FORM_MIXED: FP32 vectors with FP64 small-matrix steps),
+ * `option` their options, `objective` their batched objective (the request's `id` is the
+ * entry id it sees); the server runs `rounds_per_loop` rounds (0: 4) between admissions.
+ * submit queues a solve on the caller's device arrays (x in / out, nbd, l, u, valid until
+ * the request is waited on) and returns a ticket at once; a request larger than the whole
+ * budget is refused (LBFGSB_B200_ERR_ARGUMENT).  wait blocks until the ticket's solve has
+ * finished and gives its summary, its return code and the seconds from submit to result and
+ * from submit to admission; a result equals that of the same solve through
+ * lbfgsb_b200_minimize_batch_device_f32 alone.  destroy finishes every queued request
+ * first.  submit, wait and peak may be called from any threads. */
+typedef struct lbfgsb_b200_batch_server lbfgsb_b200_batch_server;
+int lbfgsb_b200_batch_server_create_f32(unsigned long long hbm_budget_bytes, int form,
+                                        const lbfgsb_b200_option_f32* option,
+                                        lbfgsb_b200_batch_objective_f32 objective, void* user,
+                                        int rounds_per_loop, lbfgsb_b200_batch_server** server);
+int lbfgsb_b200_batch_server_submit_f32(lbfgsb_b200_batch_server* server, int id, int n,
+                                        float* x, const int* nbd, const float* l,
+                                        const float* u, long long* ticket);
+int lbfgsb_b200_batch_server_wait(lbfgsb_b200_batch_server* server, long long ticket,
+                                  lbfgsb_b200_summary_f32* summary, int* status,
+                                  double* latency_s, double* queue_s);
+int lbfgsb_b200_batch_server_peak(lbfgsb_b200_batch_server* server,
+                                  unsigned long long* peak_bytes, int* peak_live);
+int lbfgsb_b200_batch_server_destroy(lbfgsb_b200_batch_server* server);
+
 /* Override the tuned tiles per CTA of the batched passes for instances in size bucket
  * `bucket` (0: n <= 4096, 1: <= 16384, 2: <= 65536, 3: <= 262144, 4: larger); 0 restores
  * the tuned value.  For the autotuner. */

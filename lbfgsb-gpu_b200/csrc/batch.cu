@@ -768,6 +768,129 @@ static int solve_batch_device(int count, const int* ids, const int* n, R* const*
   return first_bad;
 }
 
+// ---- continuous batching ----------------------------------------------------------------
+// A server thread owns a BatchRunner on its own stream.  Requests queue in arrival order and
+// are admitted, first come first served, as soon as their segment fits in the HBM budget
+// beside the live solves; every loop admits what fits, runs a few rounds of every live
+// solve (old and new together, one launch per pass) and retires the finished ones, whose
+// memory then admits the next requests.
+struct BatchServeRequest {
+  int id = 0, n = 0;
+  float* x = nullptr;
+  const int* nbd = nullptr;
+  const float* l = nullptr;
+  const float* u = nullptr;
+  size_t bytes = 0;
+  std::chrono::steady_clock::time_point arrive, start, finish;
+  lbfgsb_b200_summary_f32 summary{};
+  int status = -1;
+  bool done = false;
+};
+
+struct BatchServer {
+  int dev = 0, form = LBFGSB_B200_FORM_MIXED, rounds_per_loop = 4;
+  lbfgsb_b200_option_f32 opt{};
+  lbfgsb_b200_batch_objective_f32 objective = nullptr;
+  void* user = nullptr;
+  size_t budget = 0, in_use = 0, peak_bytes = 0;
+  int live = 0, peak_live = 0;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<BatchServeRequest> reqs;  // by ticket
+  std::deque<long long> queue;         // tickets waiting for admission, in arrival order
+  bool stop = false;
+  std::string error;
+  long long rounds = 0, launches = 0;
+  std::thread thread;
+};
+
+template <typename H, typename S>
+static void batch_serve_loop(BatchServer* sv) {
+  using Runner = BatchRunner<float, H, S>;
+  cudaStream_t s = nullptr;
+  try {
+    CK(cudaSetDevice(sv->dev));
+    CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    lbfgsb_b200_ext ext{};
+    ext.form = sv->form;
+    Runner run(s, sv->opt, &ext, sv->objective, sv->user);
+    std::vector<typename Runner::Inst> fresh, finished;
+    auto complete = [&](std::vector<typename Runner::Inst>& fin) {
+      if (fin.empty()) return;
+      CK(cudaStreamSynchronize(s));  // x is copied back
+      const auto now = std::chrono::steady_clock::now();
+      std::lock_guard<std::mutex> lock(sv->mu);
+      for (auto& in : fin) {
+        BatchServeRequest& r = *static_cast<BatchServeRequest*>(in.tag);
+        r.finish = now;
+        r.done = true;
+        sv->in_use -= r.bytes;
+        sv->live--;
+      }
+      fin.clear();
+      sv->cv_done.notify_all();
+    };
+    for (;;) {
+      fresh.clear();
+      {
+        std::unique_lock<std::mutex> lock(sv->mu);
+        if (run.live() == 0)
+          sv->cv_work.wait(lock, [&] { return sv->stop || !sv->queue.empty(); });
+        if (sv->stop && sv->queue.empty() && run.live() == 0) break;
+        const auto now = std::chrono::steady_clock::now();
+        while (!sv->queue.empty()) {
+          BatchServeRequest& r = sv->reqs[(size_t)sv->queue.front()];
+          if (sv->in_use + r.bytes > sv->budget) break;  // first come, first served
+          sv->queue.pop_front();
+          sv->in_use += r.bytes;
+          sv->peak_bytes = std::max(sv->peak_bytes, sv->in_use);
+          sv->peak_live = std::max(sv->peak_live, ++sv->live);
+          r.start = now;
+          typename Runner::Inst in;
+          in.id = r.id;
+          in.n = r.n;
+          in.x_user = r.x;
+          in.nbd = r.nbd;
+          in.l = r.l;
+          in.u = r.u;
+          in.summary = &r.summary;
+          in.status = &r.status;
+          in.tag = &r;
+          fresh.push_back(in);
+        }
+      }
+      if (!fresh.empty()) {
+        run.admit(fresh, &finished);
+        complete(finished);
+      }
+      if (run.live() > 0) {
+        run.run(sv->rounds_per_loop);
+        run.poll(&finished);
+        complete(finished);
+      }
+    }
+    std::lock_guard<std::mutex> lock(sv->mu);
+    sv->rounds = run.rounds();
+    sv->launches = run.launches();
+  } catch (const CudaFailure& e) {
+    char buf[256];
+    std::snprintf(buf, sizeof(buf), "%s failed at batch.cu:%d: %s", e.call, e.line,
+                  cudaGetErrorString(e.err));
+    std::lock_guard<std::mutex> lock(sv->mu);
+    sv->error = buf;
+    // every request not finished fails
+    for (auto& r : sv->reqs)
+      if (!r.done) {
+        r.status = LBFGSB_B200_ERR_CUDA;
+        r.done = true;
+        r.finish = std::chrono::steady_clock::now();
+      }
+    sv->queue.clear();
+    sv->cv_done.notify_all();
+  }
+  if (s) cudaStreamDestroy(s);
+}
+
 }  // namespace lbfgsb_b200
 
 using namespace lbfgsb_b200;
@@ -804,6 +927,127 @@ int lbfgsb_b200_minimize_batch_device_f32(int count, const int* ids, const int* 
                                                             status);
   return solve_batch_device<float, float, float>(count, ids, n, x, nbd, l, u, option, objective,
                                                  user, s, ext, summary, status);
+}
+
+int lbfgsb_b200_batch_server_create_f32(unsigned long long hbm_budget_bytes, int form,
+                                        const lbfgsb_b200_option_f32* option,
+                                        lbfgsb_b200_batch_objective_f32 objective, void* user,
+                                        int rounds_per_loop, lbfgsb_b200_batch_server** out) {
+  g_last_error.clear();
+  if (!out || !option || !objective || form < LBFGSB_B200_FORM_PLAIN ||
+      form > LBFGSB_B200_FORM_MIXED_BF16 || option->mode != LBFGSB_B200_MODE_CUDA) {
+    g_last_error = "batch_server_create: bad argument";
+    return LBFGSB_B200_ERR_ARGUMENT;
+  }
+  *out = nullptr;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    g_last_error = cudaGetErrorString(e);
+    return LBFGSB_B200_ERR_CUDA;
+  }
+  auto* sv = new BatchServer;
+  sv->dev = dev;
+  sv->form = form;
+  sv->opt = *option;
+  sv->objective = objective;
+  sv->user = user;
+  sv->budget = (size_t)hbm_budget_bytes;
+  sv->rounds_per_loop = rounds_per_loop > 0 ? rounds_per_loop : 4;
+  if (form == LBFGSB_B200_FORM_MIXED)
+    sv->thread = std::thread(batch_serve_loop<float, double>, sv);
+  else if (form == LBFGSB_B200_FORM_MIXED_BF16)
+    sv->thread = std::thread(batch_serve_loop<__nv_bfloat16, double>, sv);
+  else
+    sv->thread = std::thread(batch_serve_loop<float, float>, sv);
+  *out = reinterpret_cast<lbfgsb_b200_batch_server*>(sv);
+  return LBFGSB_B200_OK;
+}
+
+int lbfgsb_b200_batch_server_submit_f32(lbfgsb_b200_batch_server* server, int id, int n, float* x,
+                                        const int* nbd, const float* l, const float* u,
+                                        long long* ticket) {
+  g_last_error.clear();
+  auto* sv = reinterpret_cast<BatchServer*>(server);
+  if (!sv || n <= 0 || !x || !nbd || !l || !u || !ticket) {
+    g_last_error = "batch_server_submit: null argument or n <= 0";
+    return LBFGSB_B200_ERR_ARGUMENT;
+  }
+  const int m = std::min(sv->opt.hessian_approximate_dimension, kMaxM);
+  const size_t hist = sv->form == LBFGSB_B200_FORM_MIXED_BF16 ? 2 : 4;
+  const size_t bytes = hist == 2 ? BatchRunner<float, __nv_bfloat16, double>::segment_bytes(n, m, 148)
+                                 : BatchRunner<float, float, double>::segment_bytes(n, m, 148);
+  if (bytes > sv->budget) {
+    g_last_error = "batch_server_submit: the solve's workspace (" + std::to_string(bytes) +
+                   " bytes) exceeds the server's HBM budget (" + std::to_string(sv->budget) + ")";
+    return LBFGSB_B200_ERR_ARGUMENT;
+  }
+  std::lock_guard<std::mutex> lock(sv->mu);
+  if (sv->stop || !sv->error.empty()) {
+    g_last_error = sv->error.empty() ? "batch_server_submit: the server is shutting down" : sv->error;
+    return LBFGSB_B200_ERR_ARGUMENT;
+  }
+  sv->reqs.emplace_back();
+  BatchServeRequest& r = sv->reqs.back();
+  r.id = id;
+  r.n = n;
+  r.x = x;
+  r.nbd = nbd;
+  r.l = l;
+  r.u = u;
+  r.bytes = bytes;
+  r.arrive = std::chrono::steady_clock::now();
+  *ticket = (long long)sv->reqs.size() - 1;
+  sv->queue.push_back(*ticket);
+  sv->cv_work.notify_all();
+  return LBFGSB_B200_OK;
+}
+
+int lbfgsb_b200_batch_server_wait(lbfgsb_b200_batch_server* server, long long ticket,
+                                  lbfgsb_b200_summary_f32* summary, int* status,
+                                  double* latency_s, double* queue_s) {
+  g_last_error.clear();
+  auto* sv = reinterpret_cast<BatchServer*>(server);
+  if (!sv || ticket < 0) {
+    g_last_error = "batch_server_wait: bad argument";
+    return LBFGSB_B200_ERR_ARGUMENT;
+  }
+  std::unique_lock<std::mutex> lock(sv->mu);
+  if ((size_t)ticket >= sv->reqs.size()) {
+    g_last_error = "batch_server_wait: unknown ticket";
+    return LBFGSB_B200_ERR_ARGUMENT;
+  }
+  sv->cv_done.wait(lock, [&] { return sv->reqs[(size_t)ticket].done; });
+  const BatchServeRequest& r = sv->reqs[(size_t)ticket];
+  if (summary) *summary = r.summary;
+  if (status) *status = r.status;
+  if (latency_s) *latency_s = std::chrono::duration<double>(r.finish - r.arrive).count();
+  if (queue_s) *queue_s = std::chrono::duration<double>(r.start - r.arrive).count();
+  if (r.status != LBFGSB_B200_OK) g_last_error = sv->error;
+  return LBFGSB_B200_OK;
+}
+
+int lbfgsb_b200_batch_server_peak(lbfgsb_b200_batch_server* server, unsigned long long* peak_bytes,
+                                  int* peak_live) {
+  auto* sv = reinterpret_cast<BatchServer*>(server);
+  if (!sv) return LBFGSB_B200_ERR_ARGUMENT;
+  std::lock_guard<std::mutex> lock(sv->mu);
+  if (peak_bytes) *peak_bytes = (unsigned long long)sv->peak_bytes;
+  if (peak_live) *peak_live = sv->peak_live;
+  return LBFGSB_B200_OK;
+}
+
+int lbfgsb_b200_batch_server_destroy(lbfgsb_b200_batch_server* server) {
+  auto* sv = reinterpret_cast<BatchServer*>(server);
+  if (!sv) return LBFGSB_B200_ERR_ARGUMENT;
+  {
+    std::lock_guard<std::mutex> lock(sv->mu);
+    sv->stop = true;
+  }
+  sv->cv_work.notify_all();
+  if (sv->thread.joinable()) sv->thread.join();
+  delete sv;
+  return LBFGSB_B200_OK;
 }
 
 int lbfgsb_b200_batch_tiles_per_cta(int bucket, int tiles) {

@@ -99,6 +99,9 @@ EXPORTS = [
     "lbfgsb_b200_batch_tiles_per_cta", "lbfgsb_b200_synth_batch_create",
     "lbfgsb_b200_synth_batch_destroy", "lbfgsb_b200_synth_batch_problem",
     "lbfgsb_b200_synth_batch_f64", "lbfgsb_b200_synth_batch_f32",
+    "lbfgsb_b200_batch_server_create_f32", "lbfgsb_b200_batch_server_submit_f32",
+    "lbfgsb_b200_batch_server_wait", "lbfgsb_b200_batch_server_peak",
+    "lbfgsb_b200_batch_server_destroy",
 ]
 
 _lib = None
@@ -166,6 +169,21 @@ def load() -> C.CDLL:
     lib.lbfgsb_b200_synth_batch_problem.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p),
                                                     C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                                     C.c_void_p]
+    lib.lbfgsb_b200_batch_server_create_f32.restype = C.c_int
+    lib.lbfgsb_b200_batch_server_create_f32.argtypes = [C.c_ulonglong, C.c_int, C.POINTER(OptionF32),
+                                                        C.c_void_p, C.c_void_p, C.c_int,
+                                                        C.POINTER(C.c_void_p)]
+    lib.lbfgsb_b200_batch_server_submit_f32.restype = C.c_int
+    lib.lbfgsb_b200_batch_server_submit_f32.argtypes = [C.c_void_p, C.c_int, C.c_int] + \
+        [C.c_void_p] * 4 + [C.POINTER(C.c_longlong)]
+    lib.lbfgsb_b200_batch_server_wait.restype = C.c_int
+    lib.lbfgsb_b200_batch_server_wait.argtypes = [C.c_void_p, C.c_longlong, C.POINTER(SummaryF32),
+                                                  C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                                  C.POINTER(C.c_double)]
+    lib.lbfgsb_b200_batch_server_peak.restype = C.c_int
+    lib.lbfgsb_b200_batch_server_peak.argtypes = [C.c_void_p, C.POINTER(C.c_ulonglong), C.POINTER(C.c_int)]
+    lib.lbfgsb_b200_batch_server_destroy.restype = C.c_int
+    lib.lbfgsb_b200_batch_server_destroy.argtypes = [C.c_void_p]
     lib.lbfgsb_b200_dsscfg_create.restype = C.c_void_p
     lib.lbfgsb_b200_dsscfg_create.argtypes = [C.c_int, C.c_int, C.c_double]
     lib.lbfgsb_b200_dsscfg_destroy.restype = None
@@ -426,6 +444,56 @@ def solve_batch_device(batch: "SynthBatch", xs, option, form: int = FORM_PLAIN,
             ptr([p[0] for p in probs]), ptr([p[1] for p in probs]), C.byref(option),
             batch.objective, batch.handle, None, C.byref(ext), summ, stat)
     return rc, list(stat), list(summ), last_stats()
+
+
+class BatchServer:
+    """The continuous-batching server (lbfgsb_b200_batch_server_*) over a SynthBatch's
+    batched objective: FP32 solves admitted in arrival order within an HBM budget and
+    advanced together on the device."""
+
+    def __init__(self, batch: "SynthBatch", option, hbm_budget_bytes=150 * 10**9,
+                 form=FORM_MIXED, rounds_per_loop=4):
+        self.lib = load()
+        self.batch = batch
+        h = C.c_void_p()
+        rc = self.lib.lbfgsb_b200_batch_server_create_f32(hbm_budget_bytes, form, C.byref(option),
+                                                          batch.objective, batch.handle,
+                                                          rounds_per_loop, C.byref(h))
+        if rc != 0:
+            raise RuntimeError(self.lib.lbfgsb_b200_last_error().decode())
+        self.handle = h
+
+    def submit(self, p, x):
+        """Queue problem p of the batch with start point / result tensor x; returns
+        (status, ticket)."""
+        l, u, nbd, _ = self.batch.problem(p)
+        t = C.c_longlong(-1)
+        rc = self.lib.lbfgsb_b200_batch_server_submit_f32(self.handle, p, self.batch.n[p],
+                                                          x.data_ptr(), nbd, l, u, C.byref(t))
+        return rc, t.value
+
+    def wait(self, ticket):
+        """(status, summary, seconds from submit to result, seconds to admission)."""
+        summ = SummaryF32()
+        st = C.c_int(-1)
+        lat = C.c_double()
+        q = C.c_double()
+        rc = self.lib.lbfgsb_b200_batch_server_wait(self.handle, ticket, C.byref(summ),
+                                                    C.byref(st), C.byref(lat), C.byref(q))
+        if rc != 0:
+            raise RuntimeError(self.lib.lbfgsb_b200_last_error().decode())
+        return st.value, summ, lat.value, q.value
+
+    def peak(self):
+        b = C.c_ulonglong()
+        r = C.c_int()
+        self.lib.lbfgsb_b200_batch_server_peak(self.handle, C.byref(b), C.byref(r))
+        return b.value, r.value
+
+    def close(self):
+        if self.handle:
+            self.lib.lbfgsb_b200_batch_server_destroy(self.handle)
+            self.handle = None
 
 
 def _digest(a: np.ndarray) -> str:
