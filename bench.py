@@ -218,6 +218,41 @@ class Runner:
             raise RuntimeError(f"solve stopped early: {summ.num_iteration} iterations, info {summ.info}")
         return ev["start"].elapsed_time(ev["end"])
 
+    def solve_device(self, iters):
+        """The same solve through lbfgsb_b200_minimize_device (the outer loop on the device,
+        the objective's f left in device memory)."""
+        import torch
+        self.x.zero_()
+        summ = self.summ_t()
+        ext = self.LB.Ext(self.form, 0, self.LB.TRACE_CB(), None)
+        fn = self.lib.lbfgsb_b200_minimize_device_f64 if self.is64 else self.lib.lbfgsb_b200_minimize_device_f32
+        st = fn(self.n, self.x.data_ptr(), self.nbd.data_ptr(), self.l.data_ptr(), self.u.data_ptr(),
+                C.byref(self.option(iters)), self.so.d64 if self.is64 else self.so.d32, self.so.handle,
+                None, C.byref(ext), C.byref(summ))
+        torch.cuda.synchronize()
+        if st != 0:
+            raise RuntimeError(f"status {st}: {self.lib.lbfgsb_b200_last_error()}")
+        return summ, self.LB.last_stats()
+
+    def timed_device(self, W, K):
+        """ms of K device-driven iterations: a solve of W + K iterations less one of W, each
+        timed with CUDA events around the call (the set-up of the two solves cancels)."""
+        import torch
+        out = []
+        for iters in (W, W + K):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            summ, st = self.solve_device(iters)
+            e1.record()
+            e1.synchronize()
+            if summ.num_iteration != iters:
+                raise RuntimeError(f"device-driven solve stopped early: {summ.num_iteration}")
+            out.append((e0.elapsed_time(e1), st))
+        st = dict(out[1][1])
+        st["timed_launches"] = out[1][1]["total_launches"] - out[0][1]["total_launches"]
+        return out[1][0] - out[0][0], st
+
     def close(self):
         self.so.close()
 
@@ -276,6 +311,10 @@ def run_ours(args, rank: int, world: int, dist):
     # ---- per-kernel device times of the K steady-state iterations (profiled runs) ----
     kern, evals_k, launches_k, model_bytes = run.steady_kernels(W, K)
 
+    # ---- the same iterations device-driven (lbfgsb_b200_minimize_device) ----
+    run.solve_device(2)
+    ms_dev, st_dev = run.timed_device(W, K)
+
     # ---- e2e through the C ABI from pinned host buffers ----
     hx = torch.zeros(n, dtype=tdt).pin_memory()
     hl = torch.from_numpy(prob["l"].astype(dt)).pin_memory()
@@ -309,8 +348,10 @@ def run_ours(args, rank: int, world: int, dist):
     run.close()
 
     # ---- gather over ranks (max time) ----
-    ms, e2e_ms = max_over_ranks([ms, e2e_ms], dist, dev)
-    return {"ms": ms, "kern": kern, "launches_k": launches_k, "evals_k": evals_k,
+    ms, e2e_ms, ms_dev = max_over_ranks([ms, e2e_ms, ms_dev], dist, dev)
+    return {"ms_dev": ms_dev, "dev_rounds": st_dev["rounds"], "dev_syncs": st_dev["host_syncs"],
+            "dev_launches": st_dev["total_launches"], "dev_timed_launches": st_dev["timed_launches"],
+            "ms": ms, "kern": kern, "launches_k": launches_k, "evals_k": evals_k,
             "clocks": sampler.summary(), "e2e_ms": e2e_ms, "e2e_iters": summ2.num_iteration,
             "h2d": h2d, "d2h": d2h, "n": n, "model_bytes_iter": model_bytes}
 
@@ -372,6 +413,30 @@ def forms_compare(hbm, hbm_kind, sides=(4096, 2048), W=5, K=20, err_iters=300):
                    "per-iteration decrease; errors compare the iterates after the same number "
                    "of iterations from the same start (not converged solves)")
     return out
+
+
+def walk_timing(side: int = 1024, bound: float = 7.5e-8):
+    """The breakpoint walk at scale: the synthetic problem on a side x side grid with bounds
+    +-bound, so tight that the first Cauchy steps pass most breakpoints; FP64, the device
+    objective, the first three iterations profiled.  Reports the cooperative walk's launches
+    and time, and the breakpoints listed and passed by the first iteration's walk."""
+    import lbfgsb_b200 as LB
+    prob = make_problem(side)
+    prob["l"] = prob["l"] * bound
+    prob["u"] = prob["u"] * bound
+    o = LB.default_option(np.float64)
+    o.eps_f = o.eps_g = o.eps_x = 0.0
+    o.max_iteration = 2
+    LB.solve(prob, np.float64, option=o, objective="device", record=False)
+    r = LB.solve(prob, np.float64, option=o, objective="device", record=False, profile=True,
+                 trace=True)
+    k = r.stats["kernels"].get("k_walk_coop", {"launches": 0, "ms": 0.0})
+    t0 = r.trace[0]
+    return {"n": side * side, "bound": bound, "walk_launches": k["launches"],
+            "walk_ms_total": k["ms"], "walk_ms_per_launch": k["ms"] / max(1, k["launches"]),
+            "breakpoints_listed_iter1": t0["nbreak"], "segments_walked_iter1": t0["nint"],
+            "ns_per_segment": 1e6 * k["ms"] / max(1, sum(t["nint"] for t in r.trace)),
+            "iterations": r.num_iteration}
 
 
 def dsscfg_compare():
@@ -761,7 +826,16 @@ def main():
     if rank != 0:
         return
     K = args.steps
-    value = job_throughput(world, K, r["ms"])
+    # the headline is the faster of the two drivers of the same iterations (same kernels):
+    # host-driven through the reference's callback API, or device-driven
+    v_host = job_throughput(world, K, r["ms"])
+    v_dev = job_throughput(world, K, r["ms_dev"])
+    use_dev = v_dev > v_host
+    value = v_dev if use_dev else v_host
+    ms_step = (r["ms_dev"] if use_dev else r["ms"]) / K
+    config["driver"] = ("device-driven: lbfgsb_b200_minimize_device, rounds captured in a CUDA graph"
+                        if use_dev else
+                        "host-driven: lbfgsb_b200_minimize_ext, the reference's callback API")
     hbm, hbm_kind = peaks()
     kern = r["kern"]
     roof, per_kernel = roofline_of(kern, r["n"], hbm, hbm_kind, ncu_traffic())
@@ -777,21 +851,28 @@ def main():
     batched = None
     serving = None
     forms = None
+    walk = None
     if not args.no_cpu_baseline and world == 1:
         forms = forms_compare(hbm, hbm_kind)
+        walk = walk_timing()
         dss = dsscfg_compare()
         batched = batched_compare()
         serving = serving_compare()
     e2e_iters = max(1, r["e2e_iters"])
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
-        "warmup": args.warmup, "ms_per_step": r["ms"] / K, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
         "config": config,
         "e2e": {"value": job_throughput(world, e2e_iters, r["e2e_ms"]), "unit": UNIT,
                 "h2d_bytes_per_step": r["h2d"] / e2e_iters,
                 "d2h_bytes_per_step": r["d2h"] / e2e_iters},
-        "gpu_launches": r["launches_k"],
+        "gpu_launches": (r["dev_timed_launches"] if use_dev else r["launches_k"]),
+        "host_driven": {"value": v_host, "ms_per_step": r["ms"] / K, "launches": r["launches_k"]},
+        "device_driven": {"value": v_dev, "ms_per_step": r["ms_dev"] / K,
+                          "rounds_whole_solve": r["dev_rounds"], "host_syncs_whole_solve": r["dev_syncs"],
+                          "launches_whole_solve": r["dev_launches"],
+                          "timing": "a solve of W+K iterations less one of W, CUDA events around each call"},
         "roofline": roof,
         "cpu_baseline": cpu,
         "clocks": r["clocks"],
@@ -800,6 +881,7 @@ def main():
         "hbm_GBps_model": r["model_bytes_iter"] / (solver_ms / K / 1000.0) / 1e9 if solver_ms else None,
         "kernels": per_kernel,
         "forms": forms,
+        "walk": walk,
         "dsscfg": dss,
         "serving": serving,
         "batched": batched,

@@ -99,6 +99,7 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
     const PassCfg &p_gcp = p.gcp, &p_freev = p.freev, &p_dir = p.dir, &p_apply = p.apply,
                   &p_post = p.post, &p_pgcp = p.pgcp;
     const int g_proj = p.g_proj, g_elem = p.g_elem;
+    const int g_walk = walk_coop_grid<R, H, S>();
     DevState<S>& hs = *w.hs;
     CK(cudaMemcpyAsync(w.st, &hs, sizeof(hs), cudaMemcpyHostToDevice, stream));
     const size_t header = offsetof(DevState<S>, big);
@@ -193,19 +194,10 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
         subspace();
         count_dir();
         if (hs.gcp_state == GCP_WALK && hs.internal_fail == 0) {
-          if (!c.wl_t) {
-            w.wl_t = w.template alloc<double>(N);
-            w.wl_i = w.template alloc<int>(N);
-            w.wl_n = w.template alloc<unsigned int>(1);
-            c.wl_t = w.wl_t;
-            c.wl_i = w.wl_i;
-            c.wl_n = w.wl_n;
-          }
+          if (!c.wl_t) walk_buffers(w, c, N);
           CK(cudaMemsetAsync(w.wl_n, 0, sizeof(unsigned int), stream));
-          L.run(KID_WALK_GATHER, [&] {
-            k_walk_gather<R, H, S><<<g_elem, kThreads, 0, stream>>>(c, xcur, gcur);
-          });
-          L.run(KID_WALK, [&] { k_walk<R, H, S><<<1, kWalkThreads, 0, stream>>>(c, xcur, gcur); });
+          CK(cudaMemsetAsync(&c.wsc->bar, 0, sizeof(unsigned int), stream));
+          L.run(KID_WALK, [&] { launch_walk_coop<R, H, S>(c, xcur, gcur, g_walk, stream); });
           subspace();
           count_dir();
         }
@@ -383,7 +375,7 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
     st.bytes[KID_POST] = nn * (6 * Rb + 4 + hist + 2 * Hb);
     st.bytes[KID_POSTGCP] = nn * (6 * Rb + 4 + hist + 2 * Hb + 1);
     st.bytes[KID_TRIAL] = nn * 3 * Rb;
-    st.bytes[KID_WALK_GATHER] = nn * (4 * Rb + 4);
+    st.bytes[KID_WALK] = nn * (4 * Rb + 4);  // the listing pass of the cooperative walk
     st.bytes[KID_PROJGR] = nn * (4 * Rb + 4);
     st.bytes[KID_INIT] = nn * (4 * Rb + 4);
     st.bytes_per_iteration_model =
@@ -493,12 +485,12 @@ static int solve_device(int n, R* x_user, const int* nbd, const R* l, const R* u
     }
     if (!done) {
       const bool fused = hs.cnstnd != 0;
+      const int g_walk = walk_coop_grid<R, H, S>();
       auto round = [&]() {
         k_round_begin<R, H, S><<<1, 32, 0, stream>>>(c);
         c.stages = p.gcp.stages;
         k_gcp_scan<R, H, S, kConsWide><<<p.gcp.grid, p.gcp.threads, p.gcp.smem, stream>>>(c, nullptr, nullptr);
-        k_walk_gather<R, H, S><<<p.g_elem, kThreads, 0, stream>>>(c, nullptr, nullptr);
-        k_walk<R, H, S><<<1, kWalkThreads, 0, stream>>>(c, nullptr, nullptr);
+        launch_walk_coop<R, H, S>(c, (const R*)nullptr, (const R*)nullptr, g_walk, stream);
         c.stages = p.freev.stages;
         k_freev_formk<R, H, S, kConsWide><<<p.freev.grid, p.freev.threads, p.freev.smem, stream>>>(c, nullptr, nullptr);
         c.stages = p.dir.stages;
@@ -519,7 +511,7 @@ static int solve_device(int n, R* x_user, const int* nbd, const R* l, const R* u
         }
         k_post_round<R, H, S><<<1, 32, 0, stream>>>(c);
       };
-      constexpr int kRoundKernels = 12;
+      constexpr int kRoundKernels = 11;
       RoundGraph rg;
       CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
       round();

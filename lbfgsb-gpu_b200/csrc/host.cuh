@@ -52,7 +52,7 @@ enum KernelId {
 };
 static const char* kKernelNames[KID_COUNT] = {
     "k_init",      "k_projgr",    "k_begin_iteration", "k_gcp_scan",
-    "k_walk_gather", "k_walk",    "k_freev_formk",     "k_subsm_dir",
+    "k_walk_gather", "k_walk_coop", "k_freev_formk",   "k_subsm_dir",
     "k_subsm_apply", "k_trial",   "k_post_eval",       "k_post_gcp"};
 
 template <typename R>
@@ -243,6 +243,47 @@ static int grid_for(K kernel, int n, int threads) {
   return (int)std::max<long long>(1, std::min(want, cap));
 }
 
+// The breakpoint-walk buffers of one solve: the list of (t, i) and the cooperative walk's
+// scratch.
+template <typename R, typename H, typename S>
+static void walk_buffers(Workspace<R, H, S>& w, Ctx<R, H, S>& c, size_t N) {
+  w.wl_t = w.template alloc<double>(N);
+  w.wl_i = w.template alloc<int>(N);
+  w.wl_n = w.template alloc<unsigned int>(1);
+  c.wl_t = w.wl_t;
+  c.wl_i = w.wl_i;
+  c.wl_n = w.wl_n;
+  c.wsc = w.template alloc<WalkScratch>(1);
+}
+
+// Grid of the cooperative walk: CTAs that are all resident at once (one per SM at most).
+template <typename R, typename H, typename S>
+static int walk_coop_grid() {
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_coop<R, H, S>, kWalkThreads, 0));
+  if (per_sm < 1) throw CudaFailure{cudaErrorCooperativeLaunchTooLarge, "k_walk_coop occupancy", __LINE__};
+  return device_sms();
+}
+
+// The cooperative walk: listing, selection and walk in one launch whose CTAs are
+// guaranteed to be resident together (its grid barrier relies on that).  *wl_n and the
+// barrier must be zero (the host clears them, or a device-driven round's k_round_begin).
+template <typename R, typename H, typename S>
+static void launch_walk_coop(const Ctx<R, H, S>& c, const R* x, const R* g, int grid,
+                             cudaStream_t stream) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kWalkThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  CK(cudaLaunchKernelEx(&cfg, k_walk_coop<R, H, S>, c, x, g));
+}
+
 // Launch shapes of one solve's passes.
 struct Plan {
   PassCfg gcp, freev, dir, apply, post, pgcp;
@@ -321,14 +362,8 @@ static void prepare(Workspace<R, H, S>& w, Ctx<R, H, S>& c, Plan& p, int n, int 
   c.ev_g = nullptr;
   c.ev_f = nullptr;
   c.ev_act = nullptr;
-  if (walk) {
-    w.wl_t = w.template alloc<double>(N);
-    w.wl_i = w.template alloc<int>(N);
-    w.wl_n = w.template alloc<unsigned int>(1);
-    c.wl_t = w.wl_t;
-    c.wl_i = w.wl_i;
-    c.wl_n = w.wl_n;
-  }
+  c.wsc = nullptr;
+  if (walk) walk_buffers(w, c, N);
 
   const int hsz = (int)sizeof(H);
   p.gcp = pass_cfg(k_gcp_scan<R, H, S, kConsWide>,

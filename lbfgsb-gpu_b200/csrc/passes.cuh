@@ -34,6 +34,22 @@
 
 namespace lbfgsb_b200 {
 
+// Scratch of the cooperative breakpoint walk (walk.cuh, k_walk_coop): its grid barrier,
+// the radix-select histograms (three, used in rotation), and the selected chunk.
+constexpr int kWalkChunk = 1024;  // breakpoints selected and sorted at a time
+struct WalkScratch {
+  unsigned int bar;      // grid-barrier arrivals; zero before each launch
+  unsigned int chunk_n;  // keys of the selected chunk
+  int done;              // the walk has ended
+  int cnt;               // keys in the chunk just walked
+  unsigned long long last_hi;  // largest key walked so far
+  unsigned int last_lo;
+  unsigned int pad;
+  unsigned int hist[3][256];
+  unsigned long long chunk_hi[kWalkChunk];
+  unsigned int chunk_lo[kWalkChunk];
+};
+
 template <typename R, typename H, typename S>
 struct Ctx {
   int n;
@@ -53,6 +69,7 @@ struct Ctx {
   double* wl_t;      // breakpoint list (walk)
   int* wl_i;
   unsigned int* wl_n;
+  WalkScratch* wsc;  // the cooperative walk's scratch (single-instance solves)
   // device-driven solves: rounds = 1 makes every pass gate itself on the round plan in the
   // state and take its vectors from the buffers below by the roles st->xr / st->gr
   int rounds;

@@ -5,7 +5,7 @@
 //
 //   k_round_begin   the loop top (279-284): the memory reset when one is pending, the
 //                   branch flags, and the round plan (scan? subspace passes?)
-//   k_gcp_scan, k_walk_gather, k_walk, k_freev_formk, k_subsm_dir, k_subsm_apply
+//   k_gcp_scan, k_walk_coop, k_freev_formk, k_subsm_dir, k_subsm_apply
 //                   each returns at once unless the plan (and the state) asks for it
 //   k_pre_eval      the checks between the subspace step and the line search (the memory
 //                   reset after a failed step, 297-341; the g'd >= 0 exit, 359-387), and
@@ -38,6 +38,7 @@ __device__ __forceinline__ void round_begin(const Ctx<R, H, S>& c) {
   st->rp_scan = 0;
   st->rp_sub = 0;
   if (c.wl_n) *c.wl_n = 0;  // the breakpoint list of this round's walk, if any
+  if (c.wsc) c.wsc->bar = 0;  // and the cooperative walk's grid barrier
   if (st->phase != PH_ITER) return;
   // the post-evaluation pass may already have started this iteration and run its Cauchy
   // scan (spec_gcp); otherwise, and after a reset, the loop top runs here

@@ -2,15 +2,19 @@
 // culbfgsb/lbfgsbcpu.cpp:725-816 after the first breakpoint test).
 //
 // The reference keeps the breakpoints in a heap (hpsolb, 1175-1233) and pops them one at
-// a time.  Here, only when the scan found that the first breakpoint is passed:
-//   k_walk_gather  lists every breakpoint (t_i, i) (one grid-wide pass; same arithmetic
-//                  as the scan, so the same t_i);
-//   k_walk         one CTA repeatedly selects the next chunk of the smallest remaining
-//                  breakpoints (radix select on the 96-bit key (bits of t, i) over the
-//                  list), sorts the chunk in shared memory, computes each candidate's
-//                  row of W, M*wbp and wbp'M wbp in parallel, and walks the chunk in key
-//                  order on one thread with the reference's recurrence for f', f'', c, p.
-// Breakpoints with equal t are passed in increasing variable index (the heap's order
+// a time.  Here, only when the scan found that the first breakpoint is passed, the
+// breakpoints (t_i, i) are listed (same arithmetic as the scan, so the same t_i) and walked
+// in chunks of the smallest remaining keys (96-bit key: the bits of t, then i):
+//   select   a radix select over the list, 8 bits a level, that stops as soon as the
+//            buckets below the boundary hold a large enough chunk (usually after one or
+//            two levels), and the extraction of that chunk;
+//   walk     the chunk is sorted in shared memory (bitonic), each candidate's row of W,
+//            M*wbp and wbp'M wbp are formed in parallel, and one thread walks the chunk in
+//            key order with the reference's recurrence for f', f'', c and p.
+// Two forms: k_walk_coop (single-instance solves) lists and selects with the whole grid, a
+// cooperative launch with a bounded grid barrier, and walks in CTA 0; k_walk (one CTA per
+// instance, used by batched solves, with k_walk_gather before it) does everything in one
+// CTA.  Breakpoints with equal t are passed in increasing variable index (the heap's order
 // among exact ties is an artefact of its layout).
 #pragma once
 
@@ -21,19 +25,14 @@
 
 namespace lbfgsb_b200 {
 
+// Appends the breakpoints of the CTA's share of the variables to (wl_t, wl_i).
 template <typename R, typename H, typename S>
-__device__ __forceinline__ void walk_gather_pass(const Ctx<R, H, S>& c, CtaPos cp,
-                                                 const R* __restrict__ x, const R* __restrict__ g) {
-  if (c.rounds) {
-    const DevState<S>* st = c.st;
-    if (!st->rp_sub || st->gcp_state != GCP_WALK || st->internal_fail != 0) return;
-    x = c.X[st->xr[0]];
-    g = c.G[st->gr[0]];
-  }
+__device__ __forceinline__ void gather_breakpoints(const Ctx<R, H, S>& c, CtaPos cp, int nthreads,
+                                                   const R* __restrict__ x, const R* __restrict__ g) {
   const int n = c.n;
   const int lane = threadIdx.x & 31;
-  for (long long base = (long long)cp.rank * kThreads; base < n;
-       base += (long long)cp.count * kThreads) {
+  for (long long base = (long long)cp.rank * nthreads; base < n;
+       base += (long long)cp.count * nthreads) {
     const long long i = base + threadIdx.x;
     bool has_bp = false;
     R t = 0;
@@ -50,6 +49,18 @@ __device__ __forceinline__ void walk_gather_pass(const Ctx<R, H, S>& c, CtaPos c
     }
   }
 }
+
+template <typename R, typename H, typename S>
+__device__ __forceinline__ void walk_gather_pass(const Ctx<R, H, S>& c, CtaPos cp,
+                                                 const R* __restrict__ x, const R* __restrict__ g) {
+  if (c.rounds) {
+    const DevState<S>* st = c.st;
+    if (!st->rp_sub || st->gcp_state != GCP_WALK || st->internal_fail != 0) return;
+    x = c.X[st->xr[0]];
+    g = c.G[st->gr[0]];
+  }
+  gather_breakpoints<R, H, S>(c, cp, kThreads, x, g);
+}
 template <typename R, typename H, typename S>
 __global__ void __launch_bounds__(kThreads) k_walk_gather(Ctx<R, H, S> c, const R* __restrict__ x,
                                                           const R* __restrict__ g) {
@@ -57,7 +68,8 @@ __global__ void __launch_bounds__(kThreads) k_walk_gather(Ctx<R, H, S> c, const 
 }
 
 constexpr int kWalkThreads = 512;
-constexpr int kChunk = 1024;  // breakpoints selected and sorted per round
+constexpr int kChunk = kWalkChunk;
+constexpr int kChunkMin = kChunk / 4;  // the smallest chunk the select may stop at
 constexpr int kBatch = 64;    // candidates prepared in parallel per walking step
 
 struct Key96 {
@@ -93,7 +105,212 @@ __device__ __forceinline__ void key_set_digit(Key96& k, int level, int d) {
     k.lo = (k.lo & ~(255u << sh)) | ((unsigned int)d << sh);
   }
 }
+// the key just below k (k > 0)
+__device__ __forceinline__ Key96 key_prev(Key96 k) {
+  if (k.lo > 0) return Key96{k.hi, k.lo - 1};
+  return Key96{k.hi - 1, ~0u};
+}
 
+// One level of the radix select, from the level's histogram (the same in every thread that
+// runs it): the boundary digit d, the keys below it, and whether the select may stop here
+// with the chunk "every candidate below bucket d" (at least kChunkMin keys in all).  taken:
+// keys already below the prefix from earlier levels; kk: keys still wanted.
+__device__ __forceinline__ void select_level(const unsigned int* hist, long long taken,
+                                             long long kk, int& d, long long& cum, bool& stop) {
+  cum = 0;
+  d = 255;
+  for (int b = 0; b < 256; b++) {
+    if (cum + hist[b] >= kk) {
+      d = b;
+      break;
+    }
+    cum += hist[b];
+  }
+  stop = taken + cum >= kChunkMin;
+}
+
+// Thread 0's running walk (lbfgsbcpu.cpp:725-809) across chunks.
+template <typename S>
+struct WalkCarry {
+  S f1, f2, f2org, dtm, tsum, tj;
+  int nleft, nint;
+  bool all_fixed;
+};
+
+template <typename S>
+struct WalkSmem {
+  unsigned long long k_hi[kChunk];
+  unsigned int k_lo[kChunk];
+  unsigned int hist[256];
+  int count, done, info;
+  Key96 prefix, last;
+  long long kk, taken;
+  S wbp[kBatch][2 * kMaxM + 1];
+  S v[kBatch][2 * kMaxM + 1];
+  S wmw[kBatch], dibp[kBatch], zibp[kBatch];
+  S work[kBatch][kMaxM + 1];
+};
+
+// Sort the cnt keys in sm.k_hi / k_lo and walk them (all threads of the CTA).  Sets sm.done:
+// 1 the walk ended, 2 a step of M*wbp failed (the driver resets the memory).
+template <typename R, typename H, typename S>
+__device__ void walk_chunk(const Ctx<R, H, S>& c, const R* __restrict__ x, const R* __restrict__ g,
+                           const H* const (&Y)[kMaxM], const H* const (&Sl)[kMaxM], WalkSmem<S>& sm,
+                           int cnt, WalkCarry<S>& w) {
+  DevState<S>* st = c.st;
+  const int n = c.n, col = st->col, col2 = 2 * col, nbreak = st->nbreak, bnded = st->bnded;
+  const S theta = st->theta;
+  // ---- bitonic sort of the chunk by (hi, lo), padded with maximal keys ----
+  for (int e = cnt + threadIdx.x; e < kChunk; e += blockDim.x) {
+    sm.k_hi[e] = ~0ull;
+    sm.k_lo[e] = ~0u;
+  }
+  __syncthreads();
+  for (int size = 2; size <= kChunk; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int e = threadIdx.x; e < kChunk; e += blockDim.x) {
+        const int p = e ^ stride;
+        if (p > e) {
+          const bool up = (e & size) == 0;
+          const Key96 a{sm.k_hi[e], sm.k_lo[e]}, b{sm.k_hi[p], sm.k_lo[p]};
+          if (key_less(b, a) == up) {
+            sm.k_hi[e] = b.hi;
+            sm.k_lo[e] = b.lo;
+            sm.k_hi[p] = a.hi;
+            sm.k_lo[p] = a.lo;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // ---- walk the chunk in batches ----
+  for (int b0 = 0; b0 < cnt; b0 += kBatch) {
+    const int nb = (cnt - b0) < kBatch ? (cnt - b0) : kBatch;
+    if (threadIdx.x < nb) {
+      const int k = b0 + threadIdx.x;
+      const int i = (int)sm.k_lo[k];
+      const R xi = x[i], gi = g[i];
+      const R dibp = -gi;
+      const R zibp = (dibp > R(0)) ? rsub(c.u[i], xi) : rsub(c.l[i], xi);
+      sm.dibp[threadIdx.x] = (S)dibp;
+      sm.zibp[threadIdx.x] = (S)zibp;
+      S* wbp = sm.wbp[threadIdx.x];
+      for (int j = 0; j < col; j++) {
+        wbp[1 + j] = (S)HistTraits<H>::load(Y[j] + i);
+        wbp[1 + col + j] = theta * (S)HistTraits<H>::load(Sl[j] + i);
+      }
+      if (col > 0) {
+        int info = 0;
+        sbmv(st->sy, st->wt, col, wbp, sm.v[threadIdx.x], &info, sm.work[threadIdx.x]);
+        if (info != 0) atomicExch(&sm.info, info);
+        sm.wmw[threadIdx.x] = sdot(&wbp[1], 1, &sm.v[threadIdx.x][1], 1, col2);
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      if (sm.info != 0) {
+        st->internal_fail = sm.info;
+        sm.done = 2;
+      }
+      for (int q = 0; q < nb && sm.done == 0; q++) {
+        const int k = b0 + q;
+        const S tk = (S)__longlong_as_double((long long)sm.k_hi[k]);
+        const int ibp = (int)sm.k_lo[k];
+        const S tj0 = w.tj;
+        w.tj = tk;
+        const S dt = w.tj - tj0;
+        if (w.dtm < dt) {
+          sm.done = 1;
+          break;
+        }
+        w.tsum = w.tsum + dt;
+        w.nleft = w.nleft - 1;
+        const S dibp = sm.dibp[q];
+        c.code[ibp] = (int8_t)(dibp > S(0) ? IW_WALK_UPP : IW_WALK_LOW);
+        if (w.nleft == 0 && nbreak == n) {
+          w.dtm = dt;
+          for (int j = 1; j <= col2; j++) st->c[j] += w.dtm * st->p[j];
+          w.all_fixed = true;
+          sm.done = 1;
+          break;
+        }
+        w.nint = w.nint + 1;
+        const S dibp2 = dibp * dibp;
+        w.f1 = w.f1 + dt * w.f2 + dibp2 - theta * dibp * sm.zibp[q];
+        w.f2 = w.f2 - theta * dibp2;
+        if (col > 0) {
+          for (int j = 1; j <= col2; j++) st->c[j] += dt * st->p[j];
+          const S wmc = sdot(&st->c[1], 1, &sm.v[q][1], 1, col2);
+          const S wmp = sdot(&st->p[1], 1, &sm.v[q][1], 1, col2);
+          const S wmw = sm.wmw[q];
+          for (int j = 1; j <= col2; j++) st->p[j] += (-dibp) * sm.wbp[q][j];
+          w.f1 = w.f1 + dibp * wmc;
+          w.f2 = w.f2 + (S)2.0 * dibp * wmp - dibp2 * wmw;
+        }
+        w.f2 = smax((S)(5e-16 * (double)w.f2org), w.f2);
+        if (w.nleft > 0) {
+          w.dtm = -w.f1 / w.f2;
+          continue;
+        }
+        if (bnded) {
+          w.f1 = 0;
+          w.f2 = 0;
+          w.dtm = 0;
+        } else {
+          w.dtm = -w.f1 / w.f2;
+        }
+        sm.done = 1;
+        break;
+      }
+    }
+    __syncthreads();
+    if (sm.done) break;
+  }
+}
+
+// The walk's start from the state and its end into it (thread 0).
+template <typename S>
+__device__ __forceinline__ WalkCarry<S> walk_start(const DevState<S>* st) {
+  WalkCarry<S> w;
+  w.f1 = st->f1;
+  w.f2 = st->f2;
+  w.f2org = st->f2org;
+  w.dtm = st->dtm;
+  w.tsum = st->tsum;
+  w.tj = st->tj;
+  w.nleft = st->nleft;
+  w.nint = st->nint;
+  w.all_fixed = false;
+  return w;
+}
+template <typename S>
+__device__ __forceinline__ void walk_end(DevState<S>* st, WalkCarry<S>& w, S* work) {
+  const int col = st->col, col2 = 2 * col;
+  if (!w.all_fixed) {
+    if (w.dtm <= S(0)) w.dtm = 0;
+    w.tsum = w.tsum + w.dtm;
+    for (int j = 1; j <= col2; j++) st->c[j] += w.dtm * st->p[j];
+  }
+  st->f1 = w.f1;
+  st->f2 = w.f2;
+  st->dtm = w.dtm;
+  st->tsum = w.tsum;
+  st->tj = w.tj;
+  st->nleft = w.nleft;
+  st->nint = w.nint;
+  if (col > 0) {
+    int info = 0;
+    sbmv(st->sy, st->wt, col, st->c, st->mc, &info, work);
+    if (info != 0) {
+      st->internal_fail = -8;
+      return;
+    }
+  }
+  st->gcp_state = GCP_DONE;
+}
+
+// The whole walk in one CTA (batched solves: one CTA per instance, after k_walk_gather).
 template <typename R, typename H, typename S>
 __device__ __forceinline__ void walk_pass(const Ctx<R, H, S>& c, const R* __restrict__ x,
                                           const R* __restrict__ g) {
@@ -104,240 +321,254 @@ __device__ __forceinline__ void walk_pass(const Ctx<R, H, S>& c, const R* __rest
     g = c.G[st->gr[0]];
   }
   if (st->gcp_state != GCP_WALK) return;
-  const int n = c.n, col = st->col, col2 = 2 * col;
   const long long L = *c.wl_n;
-  const S theta = st->theta;
   const H *Y[kMaxM], *Sl[kMaxM];
   ring_ptrs(st, c.wy, c.ld, Y);
   ring_ptrs(st, c.ws, c.ld, Sl);
-
-  __shared__ unsigned long long k_hi[kChunk];
-  __shared__ unsigned int k_lo[kChunk];
-  __shared__ unsigned int hist[256];
-  __shared__ int sh_count, sh_done;
-  __shared__ Key96 sh_prefix, sh_last;
-  __shared__ long long sh_kk;
-  __shared__ S b_wbp[kBatch][2 * kMaxM + 1];
-  __shared__ S b_v[kBatch][2 * kMaxM + 1];
-  __shared__ S b_wmw[kBatch], b_dibp[kBatch], b_zibp[kBatch];
-  __shared__ S b_work[kBatch][kMaxM + 1];
-  __shared__ int b_info;
-
-  // walk state (thread 0 only)
-  S f1 = st->f1, f2 = st->f2, f2org = st->f2org, dtm = st->dtm, tsum = st->tsum, tj = st->tj;
-  int nleft = st->nleft, nint = st->nint;
-  const int nbreak = st->nbreak, bnded = st->bnded;
-  bool all_fixed = false;
-
+  __shared__ WalkSmem<S> sm;
+  WalkCarry<S> w{};
   if (threadIdx.x == 0) {
-    sh_done = 0;
-    sh_last = Key96{0ull, 0u};
-    b_info = 0;
+    w = walk_start(st);
+    sm.done = 0;
+    sm.last = Key96{0ull, 0u};
+    sm.info = 0;
   }
   __syncthreads();
   bool first_round = true;
   long long consumed = 0;
   while (true) {
-    // ---- select the next chunk: the kChunk smallest keys greater than sh_last ----
+    // ---- select the next chunk: the smallest keys greater than sm.last ----
     const long long remaining = L - consumed;
     Key96 thr;
     thr.hi = ~0ull;
     thr.lo = ~0u;
     if (remaining > kChunk) {
       if (threadIdx.x == 0) {
-        sh_prefix = Key96{0ull, 0u};
-        sh_kk = kChunk;
+        sm.prefix = Key96{0ull, 0u};
+        sm.kk = kChunk;
+        sm.taken = 0;
+        sm.done = 0;
       }
       __syncthreads();
       for (int level = 0; level < 12; level++) {
-        for (int b = threadIdx.x; b < 256; b += kWalkThreads) hist[b] = 0;
+        for (int b = threadIdx.x; b < 256; b += blockDim.x) sm.hist[b] = 0;
         __syncthreads();
-        const Key96 pre = sh_prefix, last = sh_last;
-        for (long long e = threadIdx.x; e < L; e += kWalkThreads) {
+        const Key96 pre = sm.prefix, last = sm.last;
+        for (long long e = threadIdx.x; e < L; e += blockDim.x) {
           const Key96 k = make_key(c.wl_t[e], c.wl_i[e]);
           if (!first_round && !key_less(last, k)) continue;
           if (!key_prefix_eq(k, pre, level)) continue;
-          atomicAdd(&hist[key_digit(k, level)], 1u);
+          atomicAdd(&sm.hist[key_digit(k, level)], 1u);
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-          long long cum = 0, kk = sh_kk;
-          int d = 255;
-          for (int b = 0; b < 256; b++) {
-            if (cum + hist[b] >= kk) {
-              d = b;
-              break;
-            }
-            cum += hist[b];
-          }
-          sh_kk = kk - cum;
-          Key96 p = sh_prefix;
+          int d;
+          long long cum;
+          bool stop;
+          select_level(sm.hist, sm.taken, sm.kk, d, cum, stop);
+          Key96 p = sm.prefix;
           key_set_digit(p, level, d);
-          sh_prefix = p;
+          if (stop) {
+            // every candidate below bucket d: the prefix with digit d and zeros after it
+            sm.prefix = key_prev(p);
+            sm.done = 1;  // used here as "select finished early"
+          } else {
+            sm.prefix = p;
+            sm.kk = sm.kk - cum;
+            sm.taken = sm.taken + cum;
+          }
         }
         __syncthreads();
+        if (sm.done) break;
       }
-      thr = sh_prefix;
+      thr = sm.prefix;
+      __syncthreads();
+      if (threadIdx.x == 0) sm.done = 0;
     }
-    // ---- extract keys in (sh_last, thr] into shared memory ----
-    if (threadIdx.x == 0) sh_count = 0;
+    // ---- extract keys in (sm.last, thr] into shared memory ----
+    if (threadIdx.x == 0) sm.count = 0;
     __syncthreads();
     {
-      const Key96 last = sh_last;
-      for (long long e = threadIdx.x; e < L; e += kWalkThreads) {
+      const Key96 last = sm.last;
+      for (long long e = threadIdx.x; e < L; e += blockDim.x) {
         const Key96 k = make_key(c.wl_t[e], c.wl_i[e]);
         if (!first_round && !key_less(last, k)) continue;
         if (key_less(thr, k)) continue;
-        const int pos = atomicAdd(&sh_count, 1);
+        const int pos = atomicAdd(&sm.count, 1);
         if (pos < kChunk) {
-          k_hi[pos] = k.hi;
-          k_lo[pos] = k.lo;
+          sm.k_hi[pos] = k.hi;
+          sm.k_lo[pos] = k.lo;
         }
       }
     }
     __syncthreads();
-    const int cnt = sh_count < kChunk ? sh_count : kChunk;
-    // ---- bitonic sort of the chunk by (hi, lo), padded with maximal keys ----
-    for (int e = cnt + threadIdx.x; e < kChunk; e += kWalkThreads) {
-      k_hi[e] = ~0ull;
-      k_lo[e] = ~0u;
-    }
-    __syncthreads();
-    for (int size = 2; size <= kChunk; size <<= 1) {
-      for (int stride = size >> 1; stride > 0; stride >>= 1) {
-        for (int e = threadIdx.x; e < kChunk; e += kWalkThreads) {
-          const int p = e ^ stride;
-          if (p > e) {
-            const bool up = (e & size) == 0;
-            const Key96 a{k_hi[e], k_lo[e]}, b{k_hi[p], k_lo[p]};
-            if (key_less(b, a) == up) {
-              k_hi[e] = b.hi;
-              k_lo[e] = b.lo;
-              k_hi[p] = a.hi;
-              k_lo[p] = a.lo;
-            }
-          }
-        }
-        __syncthreads();
-      }
-    }
-    // ---- walk the chunk in batches ----
-    for (int b0 = 0; b0 < cnt; b0 += kBatch) {
-      const int nb = (cnt - b0) < kBatch ? (cnt - b0) : kBatch;
-      if (threadIdx.x < nb) {
-        const int k = b0 + threadIdx.x;
-        const int i = (int)k_lo[k];
-        const R xi = x[i], gi = g[i];
-        const R dibp = -gi;
-        const R zibp = (dibp > R(0)) ? rsub(c.u[i], xi) : rsub(c.l[i], xi);
-        b_dibp[threadIdx.x] = (S)dibp;
-        b_zibp[threadIdx.x] = (S)zibp;
-        S* wbp = b_wbp[threadIdx.x];
-        for (int j = 0; j < col; j++) {
-          wbp[1 + j] = (S)HistTraits<H>::load(Y[j] + i);
-          wbp[1 + col + j] = theta * (S)HistTraits<H>::load(Sl[j] + i);
-        }
-        if (col > 0) {
-          int info = 0;
-          sbmv(st->sy, st->wt, col, wbp, b_v[threadIdx.x], &info, b_work[threadIdx.x]);
-          if (info != 0) atomicExch(&b_info, info);
-          b_wmw[threadIdx.x] = sdot(&wbp[1], 1, &b_v[threadIdx.x][1], 1, col2);
-        }
-      }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        if (b_info != 0) {
-          st->internal_fail = b_info;
-          sh_done = 2;
-        }
-        for (int q = 0; q < nb && sh_done == 0; q++) {
-          const int k = b0 + q;
-          const S tk = (S)__longlong_as_double((long long)k_hi[k]);
-          const int ibp = (int)k_lo[k];
-          const S tj0 = tj;
-          tj = tk;
-          const S dt = tj - tj0;
-          if (dtm < dt) {
-            sh_done = 1;
-            break;
-          }
-          tsum = tsum + dt;
-          nleft = nleft - 1;
-          const S dibp = b_dibp[q];
-          c.code[ibp] = (int8_t)(dibp > S(0) ? IW_WALK_UPP : IW_WALK_LOW);
-          if (nleft == 0 && nbreak == n) {
-            dtm = dt;
-            for (int j = 1; j <= col2; j++) st->c[j] += dtm * st->p[j];
-            all_fixed = true;
-            sh_done = 1;
-            break;
-          }
-          nint = nint + 1;
-          const S dibp2 = dibp * dibp;
-          f1 = f1 + dt * f2 + dibp2 - theta * dibp * b_zibp[q];
-          f2 = f2 - theta * dibp2;
-          if (col > 0) {
-            for (int j = 1; j <= col2; j++) st->c[j] += dt * st->p[j];
-            const S wmc = sdot(&st->c[1], 1, &b_v[q][1], 1, col2);
-            const S wmp = sdot(&st->p[1], 1, &b_v[q][1], 1, col2);
-            const S wmw = b_wmw[q];
-            for (int j = 1; j <= col2; j++) st->p[j] += (-dibp) * b_wbp[q][j];
-            f1 = f1 + dibp * wmc;
-            f2 = f2 + (S)2.0 * dibp * wmp - dibp2 * wmw;
-          }
-          f2 = smax((S)(5e-16 * (double)f2org), f2);
-          if (nleft > 0) {
-            dtm = -f1 / f2;
-            continue;
-          }
-          if (bnded) {
-            f1 = 0;
-            f2 = 0;
-            dtm = 0;
-          } else {
-            dtm = -f1 / f2;
-          }
-          sh_done = 1;
-          break;
-        }
-      }
-      __syncthreads();
-      if (sh_done) break;
-    }
+    const int cnt = sm.count < kChunk ? sm.count : kChunk;
+    walk_chunk<R, H, S>(c, x, g, Y, Sl, sm, cnt, w);
     consumed += cnt;
-    if (sh_done || consumed >= L || cnt == 0) break;
-    if (threadIdx.x == 0) sh_last = Key96{k_hi[cnt - 1], k_lo[cnt - 1]};
+    if (sm.done || consumed >= L || cnt == 0) break;
+    if (threadIdx.x == 0) sm.last = Key96{sm.k_hi[cnt - 1], sm.k_lo[cnt - 1]};
     first_round = false;
     __syncthreads();
   }
   if (threadIdx.x != 0) return;
-  if (sh_done == 2) return;  // a failed M*wbp: the driver resets the memory
-  if (!all_fixed) {
-    if (dtm <= S(0)) dtm = 0;
-    tsum = tsum + dtm;
-    for (int j = 1; j <= col2; j++) st->c[j] += dtm * st->p[j];
-  }
-  st->f1 = f1;
-  st->f2 = f2;
-  st->dtm = dtm;
-  st->tsum = tsum;
-  st->tj = tj;
-  st->nleft = nleft;
-  st->nint = nint;
-  if (col > 0) {
-    int info = 0;
-    sbmv(st->sy, st->wt, col, st->c, st->mc, &info, b_work[0]);
-    if (info != 0) {
-      st->internal_fail = -8;
-      return;
-    }
-  }
-  st->gcp_state = GCP_DONE;
+  if (sm.done == 2) return;  // a failed M*wbp: the driver resets the memory
+  walk_end(st, w, sm.work[0]);
 }
 template <typename R, typename H, typename S>
 __global__ void __launch_bounds__(kWalkThreads) k_walk(Ctx<R, H, S> c, const R* __restrict__ x,
                                                        const R* __restrict__ g) {
   walk_pass<R, H, S>(c, x, g);
+}
+
+// ---- the cooperative walk of single-instance solves ------------------------------------
+
+// Bounded grid barrier of a cooperative launch: every CTA adds one arrival to *bar and
+// waits until all of this barrier's arrivals are in (target counts up by gridDim.x per
+// barrier; *bar is zero at launch).  Returns false in every CTA whose wait gave up.
+__device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int& target) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    target += gridDim.x;
+    __threadfence();
+    atomicAdd(bar, 1u);
+    long long k = 0;
+    while (*(volatile unsigned int*)bar < target && k < 4 * kWaitPolls) k++;
+    s_ok = k < 4 * kWaitPolls ? 1 : 0;
+    __threadfence();
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Lists the breakpoints with the whole grid, selects each chunk with the whole grid
+// (histograms in global memory, the same digit decided redundantly by every CTA) and walks
+// it in CTA 0.  wsc->bar and *wl_n are zero at launch.
+template <typename R, typename H, typename S>
+__global__ void __launch_bounds__(kWalkThreads) k_walk_coop(Ctx<R, H, S> c, const R* __restrict__ x,
+                                                            const R* __restrict__ g) {
+  DevState<S>* st = c.st;
+  if (c.rounds) {
+    if (!st->rp_sub || st->internal_fail != 0) return;
+    x = c.X[st->xr[0]];
+    g = c.G[st->gr[0]];
+  }
+  if (st->gcp_state != GCP_WALK) return;
+  WalkScratch* ws = c.wsc;
+  unsigned int target = 0;
+  auto fail = [&]() {
+    if (threadIdx.x == 0) atomicExch(&st->device_error, 1);
+  };
+  __shared__ WalkSmem<S> sm;
+  const bool lead = blockIdx.x == 0;
+  if (lead) {
+    for (int b = threadIdx.x; b < 256; b += blockDim.x) ws->hist[0][b] = 0;
+    if (threadIdx.x == 0) ws->chunk_n = 0;
+  }
+  gather_breakpoints<R, H, S>(c, cta_here(), blockDim.x, x, g);
+  if (!grid_barrier(&ws->bar, target)) return fail();
+  const long long L = (long long)*(volatile unsigned int*)c.wl_n;
+  const H *Y[kMaxM], *Sl[kMaxM];
+  WalkCarry<S> w{};
+  if (lead) {
+    ring_ptrs(st, c.wy, c.ld, Y);
+    ring_ptrs(st, c.ws, c.ld, Sl);
+    if (threadIdx.x == 0) {
+      w = walk_start(st);
+      sm.done = 0;
+      sm.info = 0;
+    }
+  }
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long e0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  bool first_round = true;
+  Key96 last{0ull, 0u};
+  long long consumed = 0;
+  int hb = 0;  // the histogram buffer of the next level (rotating over three)
+  __shared__ unsigned int s_hist[256];
+  while (true) {
+    const long long remaining = L - consumed;
+    Key96 thr{~0ull, ~0u};
+    if (remaining > kChunk) {
+      Key96 prefix{0ull, 0u};
+      long long kk = kChunk, taken = 0;
+      for (int level = 0; level < 12; level++) {
+        unsigned int* h = ws->hist[hb];
+        // the buffer after this one was last read two levels ago, before the previous
+        // barrier: clear it for the next level
+        if (lead)
+          for (int b = threadIdx.x; b < 256; b += blockDim.x) ws->hist[(hb + 1) % 3][b] = 0;
+        for (int b = threadIdx.x; b < 256; b += blockDim.x) s_hist[b] = 0;
+        __syncthreads();
+        for (long long e = e0; e < L; e += stride) {
+          const Key96 k = make_key(c.wl_t[e], c.wl_i[e]);
+          if (!first_round && !key_less(last, k)) continue;
+          if (!key_prefix_eq(k, prefix, level)) continue;
+          atomicAdd(&s_hist[key_digit(k, level)], 1u);
+        }
+        __syncthreads();
+        for (int b = threadIdx.x; b < 256; b += blockDim.x)
+          if (s_hist[b]) atomicAdd(&h[b], s_hist[b]);
+        if (!grid_barrier(&ws->bar, target)) return fail();
+        for (int b = threadIdx.x; b < 256; b += blockDim.x) s_hist[b] = __ldcg(&h[b]);
+        __syncthreads();
+        hb = (hb + 1) % 3;
+        int d;
+        long long cum;
+        bool stop;
+        select_level(s_hist, taken, kk, d, cum, stop);
+        key_set_digit(prefix, level, d);
+        if (stop) {
+          prefix = key_prev(prefix);
+          break;
+        }
+        kk -= cum;
+        taken += cum;
+      }
+      thr = prefix;
+    }
+    // extract the chunk: keys in (last, thr]
+    for (long long e = e0; e < L; e += stride) {
+      const Key96 k = make_key(c.wl_t[e], c.wl_i[e]);
+      if (!first_round && !key_less(last, k)) continue;
+      if (key_less(thr, k)) continue;
+      const unsigned int pos = atomicAdd(&ws->chunk_n, 1u);
+      if (pos < (unsigned int)kChunk) {
+        ws->chunk_hi[pos] = k.hi;
+        ws->chunk_lo[pos] = k.lo;
+      }
+    }
+    if (!grid_barrier(&ws->bar, target)) return fail();
+    if (lead) {
+      const unsigned int n_sel = __ldcg(&ws->chunk_n);
+      const int cnt = n_sel < (unsigned int)kChunk ? (int)n_sel : kChunk;
+      for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+        sm.k_hi[e] = __ldcg(&ws->chunk_hi[e]);
+        sm.k_lo[e] = __ldcg(&ws->chunk_lo[e]);
+      }
+      __syncthreads();
+      walk_chunk<R, H, S>(c, x, g, Y, Sl, sm, cnt, w);
+      if (threadIdx.x == 0) {
+        ws->chunk_n = 0;
+        ws->cnt = cnt;
+        ws->done = sm.done;
+        if (cnt > 0) {
+          ws->last_hi = sm.k_hi[cnt - 1];
+          ws->last_lo = sm.k_lo[cnt - 1];
+        }
+      }
+    }
+    if (!grid_barrier(&ws->bar, target)) return fail();
+    const int cnt = *(volatile int*)&ws->cnt;
+    const int done = *(volatile int*)&ws->done;
+    consumed += cnt;
+    if (done || consumed >= L || cnt == 0) break;
+    last = Key96{*(volatile unsigned long long*)&ws->last_hi, *(volatile unsigned int*)&ws->last_lo};
+    first_round = false;
+  }
+  if (!lead || threadIdx.x != 0) return;
+  if (sm.done == 2) return;  // a failed M*wbp: the driver resets the memory
+  walk_end(st, w, sm.work[0]);
 }
 
 }  // namespace lbfgsb_b200
