@@ -314,6 +314,10 @@ int lbfgsb_b200_minimize_batch_device_f32(int count, const int* ids, const int* 
  * lbfgsb_b200_minimize_batch_device_f32 alone.  destroy finishes every queued request
  * first.  submit, wait and peak may be called from any threads. */
 typedef struct lbfgsb_b200_batch_server lbfgsb_b200_batch_server;
+/* The HBM bytes a request of n elements is admitted against (its workspace segment) in a
+ * server of precision form `form` with m = option.hessian_approximate_dimension; host
+ * arithmetic only, 0 for a bad argument. */
+unsigned long long lbfgsb_b200_batch_request_bytes(int n, int form, int m);
 int lbfgsb_b200_batch_server_create_f32(unsigned long long hbm_budget_bytes, int form,
                                         const lbfgsb_b200_option_f32* option,
                                         lbfgsb_b200_batch_objective_f32 objective, void* user,

@@ -897,6 +897,8 @@ using namespace lbfgsb_b200;
 
 extern "C" {
 
+unsigned long long lbfgsb_b200_batch_request_bytes(int n, int form, int m);
+
 int lbfgsb_b200_minimize_batch_device_f64(int count, const int* ids, const int* n,
                                           double* const* x, const int* const* nbd,
                                           const double* const* l, const double* const* u,
@@ -973,10 +975,8 @@ int lbfgsb_b200_batch_server_submit_f32(lbfgsb_b200_batch_server* server, int id
     g_last_error = "batch_server_submit: null argument or n <= 0";
     return LBFGSB_B200_ERR_ARGUMENT;
   }
-  const int m = std::min(sv->opt.hessian_approximate_dimension, kMaxM);
-  const size_t hist = sv->form == LBFGSB_B200_FORM_MIXED_BF16 ? 2 : 4;
-  const size_t bytes = hist == 2 ? BatchRunner<float, __nv_bfloat16, double>::segment_bytes(n, m, 148)
-                                 : BatchRunner<float, float, double>::segment_bytes(n, m, 148);
+  const size_t bytes =
+      (size_t)lbfgsb_b200_batch_request_bytes(n, sv->form, sv->opt.hessian_approximate_dimension);
   if (bytes > sv->budget) {
     g_last_error = "batch_server_submit: the solve's workspace (" + std::to_string(bytes) +
                    " bytes) exceeds the server's HBM budget (" + std::to_string(sv->budget) + ")";
@@ -1048,6 +1048,14 @@ int lbfgsb_b200_batch_server_destroy(lbfgsb_b200_batch_server* server) {
   if (sv->thread.joinable()) sv->thread.join();
   delete sv;
   return LBFGSB_B200_OK;
+}
+
+unsigned long long lbfgsb_b200_batch_request_bytes(int n, int form, int m) {
+  if (n <= 0 || m <= 0) return 0;
+  m = std::min(m, kMaxM);
+  return form == LBFGSB_B200_FORM_MIXED_BF16
+             ? BatchRunner<float, __nv_bfloat16, double>::segment_bytes(n, m, 148)
+             : BatchRunner<float, float, double>::segment_bytes(n, m, 148);
 }
 
 int lbfgsb_b200_batch_tiles_per_cta(int bucket, int tiles) {

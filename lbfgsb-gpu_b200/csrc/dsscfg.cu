@@ -70,7 +70,8 @@ __global__ void __launch_bounds__(kThreads) k_dsscfg(int nx, int ny, R lam, cons
   }
   double sarr[2] = {fquad, fexp}, xd[1] = {0.0}, ld[1] = {0.0};
   MinPair md[1] = {MinPair{0.0, 0}};
-  cta_reduce_to_row<kThreads, 2, 0, 0, 0>(sarr, xd, md, ld, part, 2, (int)blockIdx.x);
+  cta_reduce_to_row<kThreads, 2, 0, 0, 0>(sarr, xd, md, ld, part, 2, (int)blockIdx.x,
+                                          (int)gridDim.x);
   if (!last_cta(ticket, (int)gridDim.x)) return;
   __shared__ double red[2];
   fold_rows<kThreads>(part, gridDim.x, 2, 2, 0, 0, red);

@@ -107,7 +107,7 @@ __device__ __forceinline__ void synth_body(int s, const R* __restrict__ x, const
   }
   double sarr[1] = {acc}, xd[1] = {0.0}, ld[1] = {0.0};
   MinPair md[1] = {MinPair{0.0, 0}};
-  cta_reduce_to_row<kThreads, 1, 0, 0, 0>(sarr, xd, md, ld, part, 1, cp.rank);
+  cta_reduce_to_row<kThreads, 1, 0, 0, 0>(sarr, xd, md, ld, part, 1, cp.rank, cp.count);
   if (!last_cta(ticket, cp.count)) return;
   __shared__ double red[1];
   fold_rows<kThreads>(part, cp.count, 1, 1, 0, 0, red);

@@ -420,7 +420,7 @@ __device__ __forceinline__ void gcp_scan_pass(const Ctx<R, H, S>& c, CtaPos cp, 
   });
   constexpr int W = NS + NX + 2 * NM;
   double lo[1] = {0.0};
-  cta_reduce_to_row<CONS + 32, NS, NX, NM, 0>(s, xm, mn, lo, c.part, W, cp.rank);
+  cta_reduce_to_row<CONS + 32, NS, NX, NM, 0>(s, xm, mn, lo, c.part, W, cp.rank, cp.count);
   if (!last_cta(c.ticket, cp.count)) return;
   __shared__ double red[W];
   fold_rows<CONS + 32>(c.part, cp.count, W, NS, NX, NM, red);
@@ -669,7 +669,7 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
       if (lane == 0 && role == 0) wsum[warp][2 * kMaxM + k] = v;
     }
     __syncthreads();
-    double* row = c.part + (size_t)cp.rank * W;
+    double* row = c.part + cp.rank;  // entry k at row[k * cp.count] (reduce.cuh)
     for (int k = threadIdx.x; k < W; k += CONS + 32) {
       double a = 0.0;
       if (k < NS) {
@@ -677,7 +677,7 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
       } else {
         for (int w = 0; w < kRole0Warps; w++) a += corr_sm[w][k - NS];
       }
-      row[k] = a;
+      row[(size_t)k * cp.count] = a;
     }
   }
   if (!last_cta(c.ticket, cp.count)) return;
@@ -996,7 +996,7 @@ __device__ __forceinline__ void subsm_dir_pass(const Ctx<R, H, S>& c, CtaPos cp,
   constexpr int W = 7;
   // (the pipeline ends with a block barrier, so every thread's flag store is visible)
   double xm[1] = {s_projected ? 1.0 : 0.0}, ldum[1] = {0.0};
-  cta_reduce_to_row<CONS + 32, 2, 1, 2, 0>(sl, xm, mn, ldum, c.part, W, cp.rank);
+  cta_reduce_to_row<CONS + 32, 2, 1, 2, 0>(sl, xm, mn, ldum, c.part, W, cp.rank, cp.count);
   if (!last_cta(c.ticket, cp.count)) return;
   __shared__ double red[W];
   __shared__ double rl[3];
@@ -1101,7 +1101,7 @@ __device__ __forceinline__ void subsm_apply_pass(const Ctx<R, H, S>& c, CtaPos c
   });
   constexpr int W = 4;
   double xdum[1] = {0.0}, ldum[1] = {0.0};
-  cta_reduce_to_row<CONS + 32, 2, 0, 1, 0>(s, xdum, mn, ldum, c.part, W, cp.rank);
+  cta_reduce_to_row<CONS + 32, 2, 0, 1, 0>(s, xdum, mn, ldum, c.part, W, cp.rank, cp.count);
   if (!last_cta(c.ticket, cp.count)) return;
   __shared__ double red[W];
   fold_rows<CONS + 32>(c.part, cp.count, W, 2, 0, 1, red);
@@ -1340,7 +1340,7 @@ __device__ __forceinline__ void post_eval_pass(const Ctx<R, H, S>& c, CtaPos cp,
   constexpr int W = NS + NX;
   MinPair mdum[1] = {MinPair{0.0, 0}};
   double ldum[1] = {0.0};
-  cta_reduce_to_row<CONS + 32, NS, NX, 0, 0>(s, xm, mdum, ldum, c.part, W, cp.rank);
+  cta_reduce_to_row<CONS + 32, NS, NX, 0, 0>(s, xm, mdum, ldum, c.part, W, cp.rank, cp.count);
   if (!last_cta(c.ticket, cp.count)) return;
   __shared__ double red[W];
   fold_rows<CONS + 32>(c.part, cp.count, W, NS, NX, 0, red);
@@ -1423,7 +1423,7 @@ __device__ __forceinline__ void projgr_pass(const Ctx<R, H, S>& c, CtaPos cp, co
   }
   double sdum[1] = {0.0}, ldum[1] = {0.0};
   MinPair mdum[1] = {MinPair{0.0, 0}};
-  cta_reduce_to_row<kThreads, 0, 1, 0, 0>(sdum, xm, mdum, ldum, c.part, 1, cp.rank);
+  cta_reduce_to_row<kThreads, 0, 1, 0, 0>(sdum, xm, mdum, ldum, c.part, 1, cp.rank, cp.count);
   if (!last_cta(c.ticket, cp.count)) return;
   __shared__ double red[1];
   fold_rows<kThreads>(c.part, cp.count, 1, 0, 1, 0, red);
@@ -1667,22 +1667,22 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
       wsum[warp][NS + 3] = role == 1 ? (double)mv.i : (double)kNoIndex;
     }
     __syncthreads();
-    double* row = c.part + (size_t)cp.rank * W;
+    double* row = c.part + cp.rank;  // entry k at row[k * cp.count] (reduce.cuh)
     for (int k = threadIdx.x; k < W; k += CONS + 32) {
       if (k < NS) {
         double a = 0.0;
         for (int w = 0; w < kAllWarps; w++) a += wsum[w][k];
-        row[k] = a;
+        row[(size_t)k * cp.count] = a;
       } else if (k < NS + 2) {
         double a = 0.0;
         for (int w = 0; w < kAllWarps; w++) a = wsum[w][k] > a ? wsum[w][k] : a;
-        row[k] = a;
+        row[(size_t)k * cp.count] = a;
       } else if (k == NS + 2) {
         MinPair a = MinPair{INFINITY, kNoIndex};
         for (int w = 0; w < kAllWarps; w++)
           a = minpair(a, MinPair{wsum[w][k], (long long)wsum[w][k + 1]});
-        row[k] = a.v;
-        row[k + 1] = (double)a.i;
+        row[(size_t)k * cp.count] = a.v;
+        row[(size_t)(k + 1) * cp.count] = (double)a.i;
       }
     }
   }

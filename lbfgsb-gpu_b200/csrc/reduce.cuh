@@ -1,7 +1,9 @@
 // reduce.cuh -- deterministic grid reductions for the streaming passes.
 //
 // Each CTA reduces its threads' accumulators (warp butterflies, then a fixed-order sum
-// over warps) into one row of `part` (one row per CTA of the instance, by rank).  The CTA that finishes last (an
+// over warps) into one row of `part` (one row per CTA of the instance, by rank).  `part` is
+// stored column by column (entry k of row r at part[k * rows + r]), so that the last CTA
+// reads each column with coalesced loads when it folds the rows.  The CTA that finishes last (an
 // atomic ticket after a fence) folds the rows in CTA order and runs the pass epilogue.
 // The order of every addition is fixed by the launch shape, so results are bitwise
 // reproducible from run to run.
@@ -43,14 +45,15 @@ struct RowLayout {
   static constexpr int kWidth = NS + NX + 2 * NM;
 };
 
-// CTA-level reduction of per-thread values into part[rank * W + ...].  `lane_owned`
+// CTA-level reduction of per-thread values into row `rank` of the `count` rows of part.  `lane_owned`
 // values (one distinct output per lane, NL per lane) are summed across warps only.
 template <int NT, int NS, int NX, int NM, int NL = 0>
 __device__ __forceinline__ void cta_reduce_to_row(const double (&s)[NS > 0 ? NS : 1],
                                                   const double (&x)[NX > 0 ? NX : 1],
                                                   const MinPair (&mn)[NM > 0 ? NM : 1],
                                                   const double (&lo)[NL > 0 ? NL : 1],
-                                                  double* part, int width, int rank) {
+                                                  double* part, int width, int rank,
+                                                  int count) {
   constexpr int kWarps = NT / 32;
   constexpr int kVals = NS + NX + 2 * NM + 32 * NL;
   __shared__ double sm[kWarps][kVals > 0 ? kVals : 1];
@@ -76,22 +79,23 @@ __device__ __forceinline__ void cta_reduce_to_row(const double (&s)[NS > 0 ? NS 
 #pragma unroll
   for (int k = 0; k < NL; k++) sm[warp][NS + NX + 2 * NM + 32 * k + lane] = lo[k];
   __syncthreads();
-  double* row = part + (size_t)rank * width;
+  (void)width;
+  double* row = part + rank;  // entry k at row[k * count]
   for (int k = threadIdx.x; k < kVals; k += NT) {
     if (k >= NS && k < NS + NX) {
       double a = sm[0][k];
       for (int w = 1; w < kWarps; w++) a = (sm[w][k] > a) ? sm[w][k] : a;
-      row[k] = a;
+      row[(size_t)k * count] = a;
     } else if (k >= NS + NX && k < NS + NX + 2 * NM) {
       if (((k - NS - NX) & 1) != 0) continue;
       MinPair a = {sm[0][k], (long long)sm[0][k + 1]};
       for (int w = 1; w < kWarps; w++) a = minpair(a, MinPair{sm[w][k], (long long)sm[w][k + 1]});
-      row[k] = a.v;
-      row[k + 1] = (double)a.i;
+      row[(size_t)k * count] = a.v;
+      row[(size_t)(k + 1) * count] = (double)a.i;
     } else {
       double a = 0;
       for (int w = 0; w < kWarps; w++) a += sm[w][k];
-      row[k] = a;
+      row[(size_t)k * count] = a;
     }
   }
 }
@@ -146,17 +150,17 @@ __device__ __forceinline__ void fold_rows(const double* part, int rows, int widt
       mp[u] = MinPair{INFINITY, kNoIndex};
     }
     for (int r = lane; r < rows; r += 32) {
-      const double* row = part + (size_t)r * width;
+      const double* row = part + r;  // entry k at row[k * rows]
 #pragma unroll
       for (int u = 0; u < kFoldCols; u++) {
         const int k = k0 + u * kWarps;
         if (kind[u] == 0) {
-          acc[u] += row[k];
+          acc[u] += row[(size_t)k * rows];
         } else if (kind[u] == 1) {
-          const double v = row[k];
+          const double v = row[(size_t)k * rows];
           acc[u] = (v > acc[u]) ? v : acc[u];
         } else if (kind[u] == 2) {
-          mp[u] = minpair(mp[u], MinPair{row[k], (long long)row[k + 1]});
+          mp[u] = minpair(mp[u], MinPair{row[(size_t)k * rows], (long long)row[(size_t)(k + 1) * rows]});
         }
       }
     }

@@ -101,7 +101,7 @@ EXPORTS = [
     "lbfgsb_b200_synth_batch_f64", "lbfgsb_b200_synth_batch_f32",
     "lbfgsb_b200_batch_server_create_f32", "lbfgsb_b200_batch_server_submit_f32",
     "lbfgsb_b200_batch_server_wait", "lbfgsb_b200_batch_server_peak",
-    "lbfgsb_b200_batch_server_destroy",
+    "lbfgsb_b200_batch_server_destroy", "lbfgsb_b200_batch_request_bytes",
 ]
 
 _lib = None
@@ -182,6 +182,8 @@ def load() -> C.CDLL:
                                                   C.POINTER(C.c_double)]
     lib.lbfgsb_b200_batch_server_peak.restype = C.c_int
     lib.lbfgsb_b200_batch_server_peak.argtypes = [C.c_void_p, C.POINTER(C.c_ulonglong), C.POINTER(C.c_int)]
+    lib.lbfgsb_b200_batch_request_bytes.restype = C.c_ulonglong
+    lib.lbfgsb_b200_batch_request_bytes.argtypes = [C.c_int, C.c_int, C.c_int]
     lib.lbfgsb_b200_batch_server_destroy.restype = C.c_int
     lib.lbfgsb_b200_batch_server_destroy.argtypes = [C.c_void_p]
     lib.lbfgsb_b200_dsscfg_create.restype = C.c_void_p

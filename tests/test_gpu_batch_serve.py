@@ -48,17 +48,19 @@ def _alone(LB, bt, p, form):
 def test_served_results_equal_solves_alone(LB, budget_solves):
     import torch
     form = LB.FORM_MIXED
-    bt = LB.SynthBatch(SIDES, SEEDS, single_precision_fields=True, dtype=np.float32)
+    sides = SIDES if budget_solves is None else [48] * 6
+    bt = LB.SynthBatch(sides, SEEDS[:len(sides)], single_precision_fields=True, dtype=np.float32)
     budget = 150 * 10**9
     if budget_solves == 1:
-        # room for the largest request only: admitted one at a time
-        n_max = max(bt.n)
-        budget = int(LB.load().lbfgsb_b200_workspace_bytes(n_max, 4, form) * 1.2)
+        # room for one request at a time: admitted one after another
+        one = LB.load().lbfgsb_b200_batch_request_bytes(bt.n[0], form, 8)
+        assert one > 0
+        budget = int(one * 1.5)
     sv = LB.BatchServer(bt, _opt(LB), hbm_budget_bytes=budget, form=form, rounds_per_loop=2)
     xs = [torch.zeros(n, dtype=torch.float32, device="cuda") for n in bt.n]
     torch.cuda.synchronize()
     tickets = []
-    for p in range(len(SIDES)):
+    for p in range(len(sides)):
         rc, t = sv.submit(p, xs[p])
         assert rc == 0
         tickets.append(t)
@@ -67,6 +69,7 @@ def test_served_results_equal_solves_alone(LB, budget_solves):
     peak_bytes, peak_live = sv.peak()
     sv.close()
     torch.cuda.synchronize()
+    assert peak_bytes <= budget
     if budget_solves == 1:
         assert peak_live == 1
     else:
