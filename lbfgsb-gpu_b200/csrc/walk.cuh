@@ -517,6 +517,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_coop(Ctx<R, H, S> c, cons
         long long cum;
         bool stop;
         select_level(s_hist, taken, kk, d, cum, stop);
+        __syncthreads();  // every thread has read s_hist before the next level clears it
         key_set_digit(prefix, level, d);
         if (stop) {
           prefix = key_prev(prefix);
