@@ -438,7 +438,13 @@ int lbfgsb_b200_copy(void* dst, const void* src, size_t bytes, int kind);
  * (streams not ordered with each other) race, so issue them in order.  The scratch's
  * arrival ticket must be zero when a call starts; it is zero at load and each call leaves
  * it zero.  The first call on a device looks up the scratch address
- * (cudaGetSymbolAddress); make that first call outside any stream capture. */
+ * (cudaGetSymbolAddress); make that first call outside any stream capture.  The address is
+ * kept for the life of the process: it assumes the device's context is not torn down and
+ * created again (cudaDeviceReset) in between.  A call whose grid does not finish (a fault
+ * in the caller's arrays) leaves the ticket set; the context is then unusable anyway, and
+ * later calls report the sticky error.  Unlike the reference's sequential max, a NaN in g
+ * does not propagate into the norm (the reduction keeps the larger of two values, and a NaN
+ * compares false); the reference's propagates only a NaN in the last element. */
 int lbfgsb_b200_projgr_noalloc_f64(int n, const double* x, const double* g, const int* nbd,
                                    const double* l, const double* u, double* sbgnrm,
                                    void* stream);

@@ -31,7 +31,7 @@ BUCKETS = [
     {"name": "n<=262144", "sides": (257, 512), "count": 96},
     {"name": "n>262144", "sides": (513, 1024), "count": 24},
 ]
-CANDIDATES = [1, 2, 4, 8, 16, 32]
+CANDIDATES = [4, 8, 16, 32, 64, 128, 1024]
 ITERATIONS = 30
 
 

@@ -62,14 +62,23 @@ struct FixedDiv64 {
     y = __ddiv_rn(1.0, b_);
   }
   __device__ __forceinline__ double operator()(double a) const {
+    if (!in_range(a)) return __ddiv_rn(a, b);
+    return markstein(a);
+  }
+  // the two halves of operator(), for callers that form several quotients branch-free and
+  // redo the (rare) out-of-range ones with the full division
+  __device__ __forceinline__ bool in_range(double a) const {
     const double aa = fabs(a);
-    if (!(fast && aa >= 0x1p-600 && aa <= 0x1p600)) return __ddiv_rn(a, b);
+    return fast && aa >= 0x1p-600 && aa <= 0x1p600;
+  }
+  __device__ __forceinline__ double markstein(double a) const {
     double q = __dmul_rn(a, y);
     double r = __fma_rn(-q, b, a);
     q = __fma_rn(r, y, q);
     r = __fma_rn(-q, b, a);
     return __fma_rn(r, y, q);
   }
+  __device__ __forceinline__ double full(double a) const { return __ddiv_rn(a, b); }
 };
 struct FixedDiv32 {
   float b, y;
@@ -80,14 +89,21 @@ struct FixedDiv32 {
     y = __fdiv_rn(1.0f, b_);
   }
   __device__ __forceinline__ float operator()(float a) const {
+    if (!in_range(a)) return __fdiv_rn(a, b);
+    return markstein(a);
+  }
+  __device__ __forceinline__ bool in_range(float a) const {
     const float aa = fabsf(a);
-    if (!(fast && aa >= 0x1p-60f && aa <= 0x1p60f)) return __fdiv_rn(a, b);
+    return fast && aa >= 0x1p-60f && aa <= 0x1p60f;
+  }
+  __device__ __forceinline__ float markstein(float a) const {
     float q = __fmul_rn(a, y);
     float r = __fmaf_rn(-q, b, a);
     q = __fmaf_rn(r, y, q);
     r = __fmaf_rn(-q, b, a);
     return __fmaf_rn(r, y, q);
   }
+  __device__ __forceinline__ float full(float a) const { return __fdiv_rn(a, b); }
 };
 // Filter for arg-min reductions of quotients num/den (breakpoints, steps to a bound):
 // true when num/den certainly exceeds `best`, so that the correctly rounded quotient need

@@ -476,7 +476,7 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
   const bool track = !uncon && iter > 0 && st->cnstnd;
   const bool updatd = st->updatd != 0;
   const S theta = st->theta, tsum = st->tsum;
-  __shared__ S a1[kMaxM + 1], a2[kMaxM];  // cmprlb's coefficients (uniform over the grid)
+  __shared__ __align__(16) S a1[kMaxM + 1], a2[kMaxM];  // cmprlb's coefficients (uniform)
   if (threadIdx.x < kMaxM) {
     const int j = threadIdx.x;
     a1[j] = (j < col) ? st->mc[1 + j] : S(0);
@@ -861,7 +861,7 @@ __device__ __forceinline__ void subsm_dir_pass(const Ctx<R, H, S>& c, CtaPos cp,
   const int n = c.n, col = st->col;
   const bool uncon = st->uncon_branch != 0;
   const S theta = st->theta, tsum = st->tsum;
-  __shared__ S a1[kMaxM + 1], a2[kMaxM], w1[kMaxM], w2[kMaxM];  // uniform coefficients
+  __shared__ __align__(16) S a1[kMaxM + 1], a2[kMaxM], w1[kMaxM], w2[kMaxM];  // uniform
   if (threadIdx.x < kMaxM) {
     const int j = threadIdx.x;
     a1[j] = (j < col) ? st->mc[1 + j] : S(0);
@@ -945,9 +945,30 @@ __device__ __forceinline__ void subsm_dir_pass(const Ctx<R, H, S>& c, CtaPos cp,
       // ... + wy*wv(jy)/theta + ws*wv(js), then d/theta (1472-1483): the divisions by the
       // pass-constant theta use its reciprocal with Markstein's correction (FixedDiv), which
       // rounds exactly like the division
+      // the quotients do not depend on d: they are formed side by side without branches,
+      // the rare out-of-range ones redone with the full division, then summed in order
+      S q[kMaxM];
+      bool ok = true;
+  #pragma unroll
+      for (int j = 0; j < kMaxM; j++) {
+        if (kFull || j < col) {
+          const S a = yv[j] * w1[j];
+          q[j] = divt.markstein(a);
+          ok = ok && divt.in_range(a);
+        }
+      }
+      if (!ok) {
+  #pragma unroll
+        for (int j = 0; j < kMaxM; j++) {
+          if (kFull || j < col) {
+            const S a = yv[j] * w1[j];
+            if (!divt.in_range(a)) q[j] = divt.full(a);
+          }
+        }
+      }
   #pragma unroll
       for (int j = 0; j < kMaxM; j++)
-        if (kFull || j < col) d = d + divt(yv[j] * w1[j]) + sv[j] * w2[j];
+        if (kFull || j < col) d = d + q[j] + sv[j] * w2[j];
       d = divt(d);
       const R dr = (R)d;
       c.dsub[i] = dr;

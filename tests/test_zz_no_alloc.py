@@ -5,8 +5,10 @@ lbfgsb_b200_minimize_f64 (a caller that must not allocate) it is called on every
 and each value must equal, bit for bit, the summary.residual_g that the next callback sees
 (the reference calls after_iteration before that iteration's projgr,
 culbfgsb/lbfgsbcpu.cpp:388-395).  Called directly, two calls in a row on different sizes
-must match a numpy restatement of projgr exactly.  Sizes beyond the static scratch are
-rejected before any CUDA call.
+must match a numpy restatement of projgr exactly, and at the largest size the scratch
+holds (n = 2^25, 8192 CTAs) a batch of calls must leave the device's free memory and the
+caching allocator's reserve unchanged.  Sizes beyond the static scratch are rejected before
+any CUDA call.
 """
 import ctypes as C
 
@@ -128,3 +130,30 @@ def test_matches_solver_residual_g_inside_callbacks(LB):
         assert seen[k][0] == seen[k + 1][1], f"iterate {k + 1}"
     assert seen[-1][0] == summ.residual_g
     assert seen[0][0] > 0.0
+
+
+@pytest.mark.gpu
+def test_largest_size_allocates_nothing(LB):
+    torch = _cuda()
+    lib = LB.load()
+    n = MAX_N
+    rng = np.random.default_rng(9)
+    x = rng.standard_normal(n)
+    g = rng.standard_normal(n)
+    l = x - np.abs(rng.standard_normal(n)) * (rng.random(n) < 0.5)
+    u = x + np.abs(rng.standard_normal(n)) * (rng.random(n) < 0.5)
+    nbd = rng.integers(0, 4, n).astype(np.int32)
+    want = projgr_np(x, g, nbd, l, u)
+    dev = [torch.from_numpy(a).cuda() for a in (x, g, nbd, l, u)]
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    ptrs = [t.data_ptr() for t in dev]
+    assert lib.lbfgsb_b200_projgr_noalloc_f64(n, *ptrs, out.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    reserved0 = torch.cuda.memory_reserved()
+    for _ in range(10):
+        assert lib.lbfgsb_b200_projgr_noalloc_f64(n, *ptrs, out.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0 and torch.cuda.memory_reserved() == reserved0
+    assert float(out.cpu()[0]) == want
