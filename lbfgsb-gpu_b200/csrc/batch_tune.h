@@ -5,5 +5,5 @@
 
 namespace lbfgsb_b200 {
 constexpr int kTuneBuckets = 5;
-constexpr int kTunedTilesPerCta[kTuneBuckets] = {2, 4, 8, 8, 8};
+constexpr int kTunedTilesPerCta[kTuneBuckets] = {128, 1024, 64, 128, 32};
 }  // namespace lbfgsb_b200
