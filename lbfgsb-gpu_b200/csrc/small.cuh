@@ -99,9 +99,10 @@ __host__ __device__ inline void sdtrsl(const S* t, int ld, int n, S* b, int job,
 // v and p are 1-based (index 1..2col); work holds kMaxM + 1 scalars.
 //
 // On the device every temporary of these routines lives in shared (or global) memory
-// passed in by the caller: with runtime-indexed thread-local arrays the epilogue kernels
-// were observed to read a stale element (p[1] returning p[col+1]) on sm_100a, so no
-// routine here declares a local array.
+// passed in by the caller, next to the state copy the epilogues work on: a runtime-indexed
+// thread-local array would be placed in local memory (the pass kernels run at 96 registers
+// a thread), and keeping all operands in one place lets the warp-shared forms of
+// warp_small.cuh exchange them between lanes.  No routine here declares a local array.
 template <typename S>
 __host__ __device__ inline void sbmv(const S* sy, const S* wt, int col, const S* v, S* p,
                                      int* info, S* work) {
