@@ -20,6 +20,7 @@ template <>
 struct HistTraits<float> {
   __device__ __forceinline__ static float load(const float* p) { return __ldg(p); }
   __device__ __forceinline__ static float from(double v) { return (float)v; }
+  __device__ __forceinline__ static float from(float v) { return v; }
 };
 template <>
 struct HistTraits<__nv_bfloat16> {
@@ -29,6 +30,7 @@ struct HistTraits<__nv_bfloat16> {
   __device__ __forceinline__ static __nv_bfloat16 from(double v) {
     return __float2bfloat16_rn((float)v);
   }
+  __device__ __forceinline__ static __nv_bfloat16 from(float v) { return __float2bfloat16_rn(v); }
 };
 
 // Elementwise arithmetic that must round exactly like the reference's scalar C++ code:
@@ -106,33 +108,60 @@ struct FixedDiv32 {
   __device__ __forceinline__ float full(float a) const { return __fdiv_rn(a, b); }
 };
 // Filter for arg-min reductions of quotients num/den (breakpoints, steps to a bound):
-// true when num/den certainly exceeds `best`, so that the correctly rounded quotient need
-// not be formed.  The estimate is num * y with y the hardware reciprocal refined by one
-// Newton step (relative error about 2^-44 in double, one float ulp in float), and the
-// test keeps a margin of 2^-20, far above it: a quotient within that margin of `best`,
-// or any operand outside [2^-100, 2^100] (where the flushed reciprocal could mislead), is
-// never filtered, and NaN estimates compare false.  A filtered candidate is strictly
-// larger than `best`, so it can change neither the minimum nor its (lowest) index.
-__device__ __forceinline__ double rcp_estimate(double b) {
-  double y;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
-  return y;
+// true when the correctly rounded num/den certainly exceeds the running minimum `best`, so
+// that it need not be formed.  thr = quotient_bound<T>(best) is the least value of the
+// quotients' type T above best; the exact quotient above thr rounds to thr or more, so
+// above best.  num/den > thr is tested as num > thr*den (den > 0) or num < thr*den
+// (den < 0), the product rounded toward the side that keeps the candidate (up, or down),
+// so that no candidate whose rounded quotient could equal or undercut best is skipped.  A
+// NaN operand or den = 0 compares false (kept).  One multiplication, no reciprocal.  A
+// filtered candidate is strictly larger than the minimum, so it can change neither the
+// minimum nor its (lowest) index.
+__device__ __forceinline__ double next_up(double v) {  // least double above v (NaN, +inf: v)
+  if (!(v < INFINITY)) return v;
+  if (v == 0.0) return __longlong_as_double(1LL);
+  const long long b = __double_as_longlong(v);
+  return __longlong_as_double(v > 0.0 ? b + 1 : b - 1);
 }
-__device__ __forceinline__ float rcp_estimate(float b) {
-  float y;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(b));
-  return y;
+__device__ __forceinline__ float next_up(float v) {
+  if (!(v < INFINITY)) return v;
+  if (v == 0.0f) return __int_as_float(1);
+  const int b = __float_as_int(v);
+  return __int_as_float(v > 0.0f ? b + 1 : b - 1);
 }
 template <typename T>
-__device__ __forceinline__ bool quotient_exceeds(T num, T den, double best) {
-  const T ad = den < T(0) ? -den : den;
-  if (!(ad >= T(0x1p-100) && ad <= T(0x1p100))) return false;
-  T y = rcp_estimate(den);
-  const T e = fma(-den, y, T(1));
-  y = fma(y, e, y);
-  const double q = (double)(num * y);
-  return q > best + fabs(best) * 0x1p-20;
+__device__ __forceinline__ T quotient_bound(double best);
+template <>
+__device__ __forceinline__ double quotient_bound<double>(double best) {
+  return next_up(best);
 }
+template <>
+__device__ __forceinline__ float quotient_bound<float>(double best) {
+  const float f = __double2float_ru(best);
+  return (double)f > best ? f : next_up(f);
+}
+__device__ __forceinline__ bool quotient_exceeds(double num, double den, double thr) {
+  if (den > 0.0) return num > __dmul_ru(thr, den);
+  if (den < 0.0) return num < __dmul_rd(thr, den);
+  return false;
+}
+__device__ __forceinline__ bool quotient_exceeds(float num, float den, float thr) {
+  if (den > 0.0f) return num > __fmul_ru(thr, den);
+  if (den < 0.0f) return num < __fmul_rd(thr, den);
+  return false;
+}
+
+// Per-thread accumulators of the streaming sums: float in the plain FP32 form (S = float;
+// each thread sums a few hundred terms, the CTA and grid levels sum in double), double
+// otherwise.
+template <typename S>
+struct AccOf {
+  using type = double;
+};
+template <>
+struct AccOf<float> {
+  using type = float;
+};
 
 template <typename S>
 struct FixedDiv;

@@ -145,14 +145,22 @@ template <typename T>
 __device__ __forceinline__ T stage_at(const unsigned char* buf, int off, int e) {
   return reinterpret_cast<const T*>(buf + off)[e];
 }
-template <typename H>
-__device__ __forceinline__ double hist_at(const unsigned char* buf, int off, int e) {
+// A history element of the stage as the accumulator type A.
+template <typename H, typename A = double>
+__device__ __forceinline__ A hist_at(const unsigned char* buf, int off, int e) {
   const H v = reinterpret_cast<const H*>(buf + off)[e];
   if constexpr (sizeof(H) == 2) {
-    return (double)__bfloat162float(v);
+    return (A)__bfloat162float(v);
   } else {
-    return (double)v;
+    return (A)v;
   }
+}
+
+// The per-thread sums as doubles, for the CTA and grid levels of a reduction.
+template <typename A, int N>
+__device__ __forceinline__ void sums_to_double(const A (&a)[N], double (&d)[N]) {
+#pragma unroll
+  for (int k = 0; k < N; k++) d[k] = (double)a[k];
 }
 
 // The history loops run over the col live columns.  In the steady state col == kMaxM and
@@ -195,7 +203,7 @@ __device__ __forceinline__ int classify_q(R x, R g, R l, R u, int nb, bool& has_
     if (neggi <= R(0)) code = IW_LOW;
   } else if (xupper) {
     if (neggi >= R(0)) code = IW_UPP;
-  } else if (fabs((double)neggi) <= 0.0) {
+  } else if (fabs(neggi) <= R(0)) {
     code = IW_ZERO;
   }
   if (code == IW_FREE) {
@@ -359,12 +367,13 @@ __device__ __forceinline__ void gcp_scan_pass(const Ctx<R, H, S>& c, CtaPos cp, 
   // [18] movable variables without breakpoint; max: [0] any such with g != 0;
   // min pair: smallest breakpoint
   constexpr int NS = 19, NX = 1, NM = 1;
-  double s[NS], xm[NX];
-  MinPair mn[NM];
+  using A = typename AccOf<S>::type;
+  A s[NS];
+  double xm[NX];
+  QuotMin<R> bp;  // the smallest breakpoint
 #pragma unroll
-  for (int k = 0; k < NS; k++) s[k] = 0.0;
+  for (int k = 0; k < NS; k++) s[k] = A(0);
   xm[0] = 0.0;
-  mn[0] = MinPair{INFINITY, kNoIndex};
 
   extern __shared__ __align__(128) unsigned char dyn[];
   __shared__ StreamSet ss;
@@ -397,30 +406,31 @@ __device__ __forceinline__ void gcp_scan_pass(const Ctx<R, H, S>& c, CtaPos cp, 
       const int code = classify_q(xi, gi, li, ui, nb, has_bp, tnum, tden);
       c.code[i] = (int8_t)code;
       if (code == IW_FREE || code == IW_UNB) {
-        const double neggi = -(double)gi;
+        const A neggi = -(A)gi;
         s[0] = fma(neggi, neggi, s[0]);
   #pragma unroll
         for (int j = 0; j < kMaxM; j++) {
           if (kFull || j < col) {
-            s[1 + j] = fma(hist_at<H>(buf, hy + j * hb, e), neggi, s[1 + j]);
-            s[9 + j] = fma(hist_at<H>(buf, hs + j * hb, e), neggi, s[9 + j]);
+            s[1 + j] = fma(hist_at<H, A>(buf, hy + j * hb, e), neggi, s[1 + j]);
+            s[9 + j] = fma(hist_at<H, A>(buf, hs + j * hb, e), neggi, s[9 + j]);
           }
         }
         if (has_bp) {
-          s[17] += 1.0;
+          s[17] += A(1);
           // the smallest breakpoint: only candidates that can reach it are divided exactly
-          if (!quotient_exceeds(tnum, tden, mn[0].v))
-            mn[0] = minpair(mn[0], MinPair{(double)rdiv(tnum, tden), i});
+          bp.offer_quotient(tnum, tden, i);
         } else {
-          s[18] += 1.0;
-          if (neggi != 0.0) xm[0] = 1.0;
+          s[18] += A(1);
+          if (neggi != A(0)) xm[0] = 1.0;
         }
       }
     });
   });
   constexpr int W = NS + NX + 2 * NM;
-  double lo[1] = {0.0};
-  cta_reduce_to_row<CONS + 32, NS, NX, NM, 0>(s, xm, mn, lo, c.part, W, cp.rank, cp.count);
+  double lo[1] = {0.0}, sd[NS];
+  MinPair mn[NM] = {bp.mp};
+  sums_to_double(s, sd);
+  cta_reduce_to_row<CONS + 32, NS, NX, NM, 0>(sd, xm, mn, lo, c.part, W, cp.rank, cp.count);
   if (!last_cta(c.ticket, cp.count)) return;
   __shared__ double red[W];
   fold_rows<CONS + 32>(c.part, cp.count, W, NS, NX, NM, red);
@@ -501,9 +511,10 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
                  : warp < kRole0Warps + 2 * kRole12Warps ? 2 : 3;  // 3: the producer
   const int rt = role == 0 ? (int)threadIdx.x
                : (int)threadIdx.x - 32 * (kRole0Warps + (role - 1) * kRole12Warps);
-  double acc[2 * kMaxM];
+  using A = typename AccOf<S>::type;
+  A acc[2 * kMaxM];
 #pragma unroll
-  for (int k = 0; k < 2 * kMaxM; k++) acc[k] = 0.0;
+  for (int k = 0; k < 2 * kMaxM; k++) acc[k] = A(0);
   int cnt[5] = {0, 0, 0, 0, 0};
   unsigned long long hash = 0;
   __shared__ double corr_sm[kRole0Warps][32 * kLaneOwned];
@@ -571,8 +582,8 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
   #pragma unroll
           for (int j = 0; j < kMaxM; j++) {
             if (kFull || j < col) {
-              acc[j] = fma(hist_at<H>(buf, hy + j * hb, e), (double)r, acc[j]);
-              acc[8 + j] = fma(hist_at<H>(buf, hs + j * hb, e), (double)r, acc[8 + j]);
+              acc[j] = fma(hist_at<H, A>(buf, hy + j * hb, e), (A)r, acc[j]);
+              acc[8 + j] = fma(hist_at<H, A>(buf, hs + j * hb, e), (A)r, acc[8 + j]);
             }
           }
         } else {
@@ -616,14 +627,14 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
       const int code = stage_at<int8_t>(buf, o_code, e);
       const bool fnow = uncon || iw_free(code);
       if (fnow != (role == 1)) return;
-      const double a = hist_at<H>(buf, (role == 1 ? hy : hs) + newest * hb, e);
+      const A a = hist_at<H, A>(buf, (role == 1 ? hy : hs) + newest * hb, e);
       const int o1 = role == 1 ? hy : hs;
   #pragma unroll
       for (int j = 0; j < kMaxM; j++) {
         if (kFull || j < col) {
-          acc[j] = fma(a, hist_at<H>(buf, o1 + j * hb, e), acc[j]);
-          acc[8 + j] = role == 1 ? fma(hist_at<H>(buf, hs + j * hb, e), a, acc[8 + j])
-                                 : fma(a, hist_at<H>(buf, hy + j * hb, e), acc[8 + j]);
+          acc[j] = fma(a, hist_at<H, A>(buf, o1 + j * hb, e), acc[j]);
+          acc[8 + j] = role == 1 ? fma(hist_at<H, A>(buf, hs + j * hb, e), a, acc[8 + j])
+                                 : fma(a, hist_at<H, A>(buf, hy + j * hb, e), acc[8 + j]);
         }
       }
     };
@@ -660,7 +671,7 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
     const int off = role == 0 ? 0 : role == 1 ? NA : NA + NB;
 #pragma unroll
     for (int k = 0; k < 2 * kMaxM; k++) {
-      const double v = warp_sum(acc[k]);
+      const double v = warp_sum((double)acc[k]);
       if (lane == 0 && role < 3) wsum[warp][off + k] = v;
     }
 #pragma unroll
@@ -764,13 +775,13 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c,
 // lnsrlb's per-variable start at the subspace point z (lbfgsbcpu.cpp:1263-1299): d = z - x,
 // d'd, g'd, and the step along d to the first bound (stpmx), filtered as for stpmx = 1e10;
 // candidates that cannot reach the running minimum skip the exact division.
-template <typename R>
+template <typename R, typename A>
 __device__ __forceinline__ void lnsrlb_elem(R zi, R xi, R gi, R li, R ui, int nb, bool want_stpmx,
-                                            long long i, double& dtd, double& gd, MinPair& mn) {
+                                            long long i, A& dtd, A& gd, QuotMin<R>& mn) {
   const R big = (R)1.0e10;
   const R d = rsub(zi, xi);
-  dtd = fma((double)d, (double)d, dtd);
-  gd = fma((double)gi, (double)d, gd);
+  dtd = fma((A)d, (A)d, dtd);
+  gd = fma((A)gi, (A)d, gd);
   if (!want_stpmx || nb == 0) return;
   double cand = INFINITY;
   bool skip = false;  // a candidate that cannot reach the running minimum
@@ -779,7 +790,7 @@ __device__ __forceinline__ void lnsrlb_elem(R zi, R xi, R gi, R li, R ui, int nb
     if (a2 >= R(0))
       cand = 0.0;
     else if (rmul(d, big) < a2) {
-      skip = quotient_exceeds(a2, d, mn.v);
+      skip = quotient_exceeds(a2, d, mn.thr);
       if (!skip) cand = (double)rdiv(a2, d);
     }
   } else if (d > R(0) && nb >= 2) {
@@ -787,11 +798,11 @@ __device__ __forceinline__ void lnsrlb_elem(R zi, R xi, R gi, R li, R ui, int nb
     if (a2 <= R(0))
       cand = 0.0;
     else if (rmul(d, big) > a2) {
-      skip = quotient_exceeds(a2, d, mn.v);
+      skip = quotient_exceeds(a2, d, mn.thr);
       if (!skip) cand = (double)rdiv(a2, d);
     }
   }
-  if (!skip) mn = minpair(mn, MinPair{cand, i});
+  if (!skip) mn.offer(cand, i);
 }
 
 // lnsrlb with task != 1 (1263-1311), then its first dcsrch call (1312-1338), from
@@ -870,10 +881,12 @@ __device__ __forceinline__ void subsm_dir_pass(const Ctx<R, H, S>& c, CtaPos cp,
     w2[j] = (j < col) ? st->wv[col + 1 + j] : S(0);
     if (j == 0) a1[kMaxM] = theta;
   }
-  // mn[0]: the step to the first bound (alpha); the speculative lnsrlb start at the
-  // untruncated step (alpha = 1): sums d'd, g'd and mn[1] the smallest step to a bound
-  MinPair mn[2] = {MinPair{INFINITY, kNoIndex}, MinPair{INFINITY, kNoIndex}};
-  double sl[2] = {0.0, 0.0};
+  // mb: the step to the first bound (alpha); the speculative lnsrlb start at the
+  // untruncated step (alpha = 1): sums d'd, g'd and ms the smallest step to a bound
+  QuotMin<S> mb;
+  QuotMin<R> ms;
+  using A = typename AccOf<S>::type;
+  A sl[2] = {A(0), A(0)};
   const bool want_stpmx = st->cnstnd && st->iter > 0;
   // speculate unless the last step was truncated (then this one likely is too); the 3.0
   // step always needs the projected point
@@ -934,7 +947,7 @@ __device__ __forceinline__ void subsm_dir_pass(const Ctx<R, H, S>& c, CtaPos cp,
         // an active variable: z is its Cauchy point
         const R zi = gcp_point<R, S>(code, v.x, v.g, v.l, v.u, tsum);
         z[i] = zi;
-        lnsrlb_elem<R>(zi, v.x, v.g, v.l, v.u, v.nb, want_stpmx, i, sl[0], sl[1], mn[1]);
+        lnsrlb_elem<R, A>(zi, v.x, v.g, v.l, v.u, v.nb, want_stpmx, i, sl[0], sl[1], ms);
         return;
       }
       const S(&yv)[kMaxM] = v.yv;
@@ -983,7 +996,7 @@ __device__ __forceinline__ void subsm_dir_pass(const Ctx<R, H, S>& c, CtaPos cp,
           if (temp2 >= S(0))
             cand = 0.0;
           else if (dk * S(1) < temp2) {
-            skip = quotient_exceeds(temp2, dk, mn[0].v);
+            skip = quotient_exceeds(temp2, dk, mb.thr);
             if (!skip) cand = (double)(temp2 / dk);
           }
         } else if (dk > S(0) && nb >= 2) {
@@ -991,11 +1004,11 @@ __device__ __forceinline__ void subsm_dir_pass(const Ctx<R, H, S>& c, CtaPos cp,
           if (temp2 <= S(0))
             cand = 0.0;
           else if (dk * S(1) > temp2) {
-            skip = quotient_exceeds(temp2, dk, mn[0].v);
+            skip = quotient_exceeds(temp2, dk, mb.thr);
             if (!skip) cand = (double)(temp2 / dk);
           }
         }
-        if (!skip) mn[0] = minpair(mn[0], MinPair{cand, i});
+        if (!skip) mb.offer(cand, i);
       }
       // the subspace step with alpha = 1 (1517-1533): z = xcp + d; with the 3.0 step,
       // projected onto the box (the lower bound, then the upper one)
@@ -1008,7 +1021,7 @@ __device__ __forceinline__ void subsm_dir_pass(const Ctx<R, H, S>& c, CtaPos cp,
           if ((lo && zs == li) || (hi && zs == ui)) s_projected = 1;
         }
         z[i] = zs;
-        lnsrlb_elem<R>(zs, xi, gi, li, ui, nb, want_stpmx, i, sl[0], sl[1], mn[1]);
+        lnsrlb_elem<R, A>(zs, xi, gi, li, ui, nb, want_stpmx, i, sl[0], sl[1], ms);
       }
     });
   });
@@ -1016,8 +1029,10 @@ __device__ __forceinline__ void subsm_dir_pass(const Ctx<R, H, S>& c, CtaPos cp,
   // (value, index) ]
   constexpr int W = 7;
   // (the pipeline ends with a block barrier, so every thread's flag store is visible)
-  double xm[1] = {s_projected ? 1.0 : 0.0}, ldum[1] = {0.0};
-  cta_reduce_to_row<CONS + 32, 2, 1, 2, 0>(sl, xm, mn, ldum, c.part, W, cp.rank, cp.count);
+  double xm[1] = {s_projected ? 1.0 : 0.0}, ldum[1] = {0.0}, sld[2];
+  MinPair mn[2] = {mb.mp, ms.mp};
+  sums_to_double(sl, sld);
+  cta_reduce_to_row<CONS + 32, 2, 1, 2, 0>(sld, xm, mn, ldum, c.part, W, cp.rank, cp.count);
   if (!last_cta(c.ticket, cp.count)) return;
   __shared__ double red[W];
   __shared__ double rl[3];
@@ -1075,8 +1090,9 @@ __device__ __forceinline__ void subsm_apply_pass(const Ctx<R, H, S>& c, CtaPos c
   const S alpha = sub ? st->alpha : S(1), tsum = st->tsum;
   const long long ibd = sub ? st->ibd : -1;
   const bool want_stpmx = st->cnstnd && st->iter > 0;
-  double s[2] = {0.0, 0.0};
-  MinPair mn[1] = {MinPair{INFINITY, kNoIndex}};
+  using A = typename AccOf<S>::type;
+  A s[2] = {A(0), A(0)};
+  QuotMin<R> ms;
 
   extern __shared__ __align__(128) unsigned char dyn[];
   __shared__ StreamSet ss;
@@ -1117,12 +1133,14 @@ __device__ __forceinline__ void subsm_apply_pass(const Ctx<R, H, S>& c, CtaPos c
       zi = (R)((S)zi + alpha * dk);
     }
     z[i] = zi;
-    lnsrlb_elem<R>(zi, xi, gi, li, ui, want_stpmx ? stage_at<int>(buf, o_nb, e) : 0, want_stpmx, i,
-                   s[0], s[1], mn[0]);
+    lnsrlb_elem<R, A>(zi, xi, gi, li, ui, want_stpmx ? stage_at<int>(buf, o_nb, e) : 0, want_stpmx,
+                      i, s[0], s[1], ms);
   });
   constexpr int W = 4;
-  double xdum[1] = {0.0}, ldum[1] = {0.0};
-  cta_reduce_to_row<CONS + 32, 2, 0, 1, 0>(s, xdum, mn, ldum, c.part, W, cp.rank, cp.count);
+  double xdum[1] = {0.0}, ldum[1] = {0.0}, sd[2];
+  MinPair mn[1] = {ms.mp};
+  sums_to_double(s, sd);
+  cta_reduce_to_row<CONS + 32, 2, 0, 1, 0>(sd, xdum, mn, ldum, c.part, W, cp.rank, cp.count);
   if (!last_cta(c.ticket, cp.count)) return;
   __shared__ double red[W];
   fold_rows<CONS + 32>(c.part, cp.count, W, 2, 0, 1, red);
@@ -1292,9 +1310,10 @@ __device__ __forceinline__ void post_eval_pass(const Ctx<R, H, S>& c, CtaPos cp,
   H* ssp = c.ws + (size_t)st->spare * (size_t)c.ld;
   // sums: [0] g'd, [1] |xold - x|^2, [2] y'y, [3..10] s'y_j, [11..18] s_j's; max: |proj g|
   constexpr int NS = 19, NX = 1;
-  double s[NS], xm[NX] = {0.0};
+  using A = typename AccOf<S>::type;
+  A s[NS], xa = A(0);
 #pragma unroll
-  for (int k = 0; k < NS; k++) s[k] = 0.0;
+  for (int k = 0; k < NS; k++) s[k] = A(0);
 
   extern __shared__ __align__(128) unsigned char dyn[];
   __shared__ StreamSet ss;
@@ -1329,7 +1348,7 @@ __device__ __forceinline__ void post_eval_pass(const Ctx<R, H, S>& c, CtaPos cp,
       const R xi = stage_at<R>(buf, o_xt, e), gi = stage_at<R>(buf, o_g, e);
       const R gold = stage_at<R>(buf, o_go, e);
       const R d = rsub(zi, ti);
-      s[0] = fma((double)gi, (double)d, s[0]);
+      s[0] = fma((A)gi, (A)d, s[0]);
       // projgr (1389-1414)
       const int nb = stage_at<int>(buf, o_nb, e);
       R pg = gi;
@@ -1340,28 +1359,29 @@ __device__ __forceinline__ void post_eval_pass(const Ctx<R, H, S>& c, CtaPos cp,
           if (nb <= 2) pg = smin<R>(rsub(xi, stage_at<R>(buf, o_l, e)), gi);
         }
       }
-      const double apg = fabs((double)pg);
-      xm[0] = (apg > xm[0]) ? apg : xm[0];
+      const A apg = fabs((A)pg);
+      xa = (apg > xa) ? apg : xa;
       const R xd = rsub(ti, xi);
-      s[1] = fma((double)xd, (double)xd, s[1]);
+      s[1] = fma((A)xd, (A)xd, s[1]);
       const R y = rsub(gi, gold);
-      s[2] = fma((double)y, (double)y, s[2]);
+      s[2] = fma((A)y, (A)y, s[2]);
       const R sv = unit ? d : rmul(d, stp);
   #pragma unroll
       for (int j = 0; j < kMaxM; j++) {
         if (kFull || j < col) {
-          s[3 + j] = fma((double)sv, hist_at<H>(buf, hy + j * hb, e), s[3 + j]);
-          s[11 + j] = fma(hist_at<H>(buf, hs + j * hb, e), (double)sv, s[11 + j]);
+          s[3 + j] = fma((A)sv, hist_at<H, A>(buf, hy + j * hb, e), s[3 + j]);
+          s[11 + j] = fma(hist_at<H, A>(buf, hs + j * hb, e), (A)sv, s[11 + j]);
         }
       }
-      ssp[i] = HistTraits<H>::from((double)sv);
-      ysp[i] = HistTraits<H>::from((double)y);
+      ssp[i] = HistTraits<H>::from(sv);
+      ysp[i] = HistTraits<H>::from(y);
     });
   });
   constexpr int W = NS + NX;
   MinPair mdum[1] = {MinPair{0.0, 0}};
-  double ldum[1] = {0.0};
-  cta_reduce_to_row<CONS + 32, NS, NX, 0, 0>(s, xm, mdum, ldum, c.part, W, cp.rank, cp.count);
+  double ldum[1] = {0.0}, sd[NS], xm[NX] = {(double)xa};
+  sums_to_double(s, sd);
+  cta_reduce_to_row<CONS + 32, NS, NX, 0, 0>(sd, xm, mdum, ldum, c.part, W, cp.rank, cp.count);
   if (!last_cta(c.ticket, cp.count)) return;
   __shared__ double red[W];
   fold_rows<CONS + 32>(c.part, cp.count, W, NS, NX, 0, red);
@@ -1491,13 +1511,13 @@ __global__ void k_begin_iteration(DevState<S>* st, int reset) {
 
 
 // The value a history element holds once stored (the history precision H), as a double.
-template <typename H>
-__device__ __forceinline__ double stored_value(double v) {
+template <typename H, typename A, typename R>
+__device__ __forceinline__ A stored_value(R v) {
   const H h = HistTraits<H>::from(v);
   if constexpr (sizeof(H) == 2) {
-    return (double)__bfloat162float(h);
+    return (A)__bfloat162float(h);
   } else {
-    return (double)h;
+    return (A)h;
   }
 }
 
@@ -1550,11 +1570,12 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
   //   position, [17] / [18] y'(-g) / s'(-g) of the new pair, [19] nbreak, [20] movable
   //   without breakpoint; xmx: any of those with g != 0; mn: smallest breakpoint.
   constexpr int NP = 19, NG = 21;
-  double acc[NG];
+  using A = typename AccOf<S>::type;
+  A acc[NG];
 #pragma unroll
-  for (int k = 0; k < NG; k++) acc[k] = 0.0;
-  double xmx = 0.0;
-  MinPair mn = MinPair{INFINITY, kNoIndex};
+  for (int k = 0; k < NG; k++) acc[k] = A(0);
+  A xmx = A(0);
+  QuotMin<R> bp;  // role G: the smallest breakpoint
 
   extern __shared__ __align__(128) unsigned char dyn[];
   __shared__ StreamSet ss;
@@ -1588,7 +1609,7 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
       const R xi = stage_at<R>(buf, o_xt, e), gi = stage_at<R>(buf, o_g, e);
       const R gold = stage_at<R>(buf, o_go, e);
       const R d = rsub(zi, ti);
-      acc[0] = fma((double)gi, (double)d, acc[0]);
+      acc[0] = fma((A)gi, (A)d, acc[0]);
       // projgr (1389-1414)
       const int nb = stage_at<int>(buf, o_nb, e);
       R pg = gi;
@@ -1599,22 +1620,22 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
           if (nb <= 2) pg = smin<R>(rsub(xi, stage_at<R>(buf, o_l, e)), gi);
         }
       }
-      const double apg = fabs((double)pg);
+      const A apg = fabs((A)pg);
       xmx = (apg > xmx) ? apg : xmx;
       const R xd = rsub(ti, xi);
-      acc[1] = fma((double)xd, (double)xd, acc[1]);
+      acc[1] = fma((A)xd, (A)xd, acc[1]);
       const R y = rsub(gi, gold);
-      acc[2] = fma((double)y, (double)y, acc[2]);
+      acc[2] = fma((A)y, (A)y, acc[2]);
       const R sv = unit ? d : rmul(d, stp);
 #pragma unroll
       for (int j = 0; j < kMaxM; j++) {
         if (kFull || j < col) {
-          acc[3 + j] = fma((double)sv, hist_at<H>(buf, hy + j * hb, e), acc[3 + j]);
-          acc[11 + j] = fma(hist_at<H>(buf, hs + j * hb, e), (double)sv, acc[11 + j]);
+          acc[3 + j] = fma((A)sv, hist_at<H, A>(buf, hy + j * hb, e), acc[3 + j]);
+          acc[11 + j] = fma(hist_at<H, A>(buf, hs + j * hb, e), (A)sv, acc[11 + j]);
         }
       }
-      ssp[i] = HistTraits<H>::from((double)sv);
-      ysp[i] = HistTraits<H>::from((double)y);
+      ssp[i] = HistTraits<H>::from(sv);
+      ysp[i] = HistTraits<H>::from(y);
     };
     auto gcp_elem = [&](const unsigned char* buf, long long tt, int valid, int e) {
       if (e >= valid) return;
@@ -1627,13 +1648,13 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
       const int code = classify_q(xi, gi, li, ui, nb, has_bp, tnum, tden);
       c.code[i] = (int8_t)code;
       if (code == IW_FREE || code == IW_UNB) {
-        const double neggi = -(double)gi;
+        const A neggi = -(A)gi;
         acc[0] = fma(neggi, neggi, acc[0]);
 #pragma unroll
         for (int j = 0; j < kMaxM; j++) {
           if (kFull || j < col) {
-            acc[1 + j] = fma(hist_at<H>(buf, hy + j * hb, e), neggi, acc[1 + j]);
-            acc[9 + j] = fma(hist_at<H>(buf, hs + j * hb, e), neggi, acc[9 + j]);
+            acc[1 + j] = fma(hist_at<H, A>(buf, hy + j * hb, e), neggi, acc[1 + j]);
+            acc[9 + j] = fma(hist_at<H, A>(buf, hs + j * hb, e), neggi, acc[9 + j]);
           }
         }
         // the new pair as the ring will hold it
@@ -1641,15 +1662,14 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
         const R d = rsub(zi, ti);
         const R sv = unit ? d : rmul(d, stp);
         const R y = rsub(gi, stage_at<R>(buf, o_go, e));
-        acc[17] = fma(stored_value<H>((double)y), neggi, acc[17]);
-        acc[18] = fma(stored_value<H>((double)sv), neggi, acc[18]);
+        acc[17] = fma(stored_value<H, A>(y), neggi, acc[17]);
+        acc[18] = fma(stored_value<H, A>(sv), neggi, acc[18]);
         if (has_bp) {
-          acc[19] += 1.0;
-          if (!quotient_exceeds(tnum, tden, mn.v))
-            mn = minpair(mn, MinPair{(double)rdiv(tnum, tden), i});
+          acc[19] += A(1);
+          bp.offer_quotient(tnum, tden, i);
         } else {
-          acc[20] += 1.0;
-          if (neggi != 0.0) xmx = 1.0;
+          acc[20] += A(1);
+          if (neggi != A(0)) xmx = A(1);
         }
       }
     };
@@ -1677,11 +1697,11 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
     const int cnt = role == 0 ? NP : role == 1 ? NG : 0;
 #pragma unroll
     for (int k = 0; k < NG; k++) {
-      const double v = warp_sum(acc[k]);
+      const double v = warp_sum((double)acc[k]);
       if (lane == 0 && k < cnt) wsum[warp][off + k] = v;
     }
-    const double xv = warp_max(xmx);
-    const MinPair mv = warp_min(mn);
+    const double xv = warp_max((double)xmx);
+    const MinPair mv = warp_min(bp.mp);
     if (lane == 0) {
       if (role < 2) wsum[warp][NS + role] = xv;
       wsum[warp][NS + 2] = role == 1 ? mv.v : INFINITY;

@@ -110,4 +110,24 @@ __host__ __device__ __forceinline__ MinPair minpair(MinPair a, MinPair b) {
   return a;
 }
 
+// A running arg-min of quotients with the filter bound of its value in the quotients'
+// type T (quotient_exceeds), updated only when the minimum changes.
+template <typename T>
+struct QuotMin {
+  MinPair mp;
+  T thr;
+  __device__ __forceinline__ QuotMin() : mp{INFINITY, kNoIndex}, thr(T(INFINITY)) {}
+  __device__ __forceinline__ void offer(double v, long long i) {
+    const MinPair nm = minpair(mp, MinPair{v, i});
+    if (nm.i != mp.i || nm.v != mp.v) {
+      mp = nm;
+      thr = quotient_bound<T>(mp.v);
+    }
+  }
+  // the candidate num/den, formed (correctly rounded) only when it may be the minimum
+  __device__ __forceinline__ void offer_quotient(T num, T den, long long i) {
+    if (!quotient_exceeds(num, den, thr)) offer((double)rdiv(num, den), i);
+  }
+};
+
 }  // namespace lbfgsb_b200

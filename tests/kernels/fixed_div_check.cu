@@ -1,8 +1,9 @@
 // Compares the fixed-divisor quotient of csrc/common.cuh (FixedDiv64 / FixedDiv32) with
 // CUDA's correctly rounded division (__ddiv_rn / __fdiv_rn) bit for bit on random and
-// constructed inputs, and checks that the arg-min filter quotient_exceeds(num, den, best)
-// never reports a quotient that is <= best (with best at, just below and just above the
-// correctly rounded quotient, and far from it).  Prints the number of mismatches /
+// constructed inputs, and checks that the arg-min filter
+// quotient_exceeds(num, den, quotient_bound<T>(best)) never reports a quotient whose
+// correctly rounded value is <= best (with best at, just below and just above that value,
+// and far from it).  Prints the number of mismatches /
 // violations per family and exits 1 if any.
 //   argv[1] = millions of random pairs per family (default 64)
 #include <cuda_runtime.h>
@@ -135,7 +136,7 @@ __global__ void k_check_filter(long long count, unsigned long long seed, unsigne
     else if (mode == 3) best = (double)q * 0.5;
     else if (mode == 4) best = (double)q * 2.0;
     else best = (double)q * (1.0 - 1e-6);
-    if (quotient_exceeds(num, den, best)) {
+    if (quotient_exceeds(num, den, quotient_bound<T>(best))) {
       atomicAdd(&bad[1], 1ULL);
       if (!((double)q > best)) atomicAdd(&bad[0], 1ULL);
     }
