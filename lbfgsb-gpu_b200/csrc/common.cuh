@@ -109,9 +109,8 @@ struct FixedDiv32 {
 };
 // Filter for arg-min reductions of quotients num/den (breakpoints, steps to a bound):
 // true when the correctly rounded num/den certainly exceeds the running minimum `best`, so
-// that it need not be formed.  thr = quotient_bound<T>(best) is the least value of the
-// quotients' type T above best; the exact quotient above thr rounds to thr or more, so
-// above best.  num/den > thr is tested as num > thr*den (den > 0) or num < thr*den
+// that it need not be formed.  thr = next_up(best) is the least value of the quotients'
+// type T above best; the exact quotient above thr rounds to thr or more, so above best.  num/den > thr is tested as num > thr*den (den > 0) or num < thr*den
 // (den < 0), the product rounded toward the side that keeps the candidate (up, or down),
 // so that no candidate whose rounded quotient could equal or undercut best is skipped.  A
 // NaN operand or den = 0 compares false (kept).  One multiplication, no reciprocal.  A
@@ -128,17 +127,6 @@ __device__ __forceinline__ float next_up(float v) {
   if (v == 0.0f) return __int_as_float(1);
   const int b = __float_as_int(v);
   return __int_as_float(v > 0.0f ? b + 1 : b - 1);
-}
-template <typename T>
-__device__ __forceinline__ T quotient_bound(double best);
-template <>
-__device__ __forceinline__ double quotient_bound<double>(double best) {
-  return next_up(best);
-}
-template <>
-__device__ __forceinline__ float quotient_bound<float>(double best) {
-  const float f = __double2float_ru(best);
-  return (double)f > best ? f : next_up(f);
 }
 __device__ __forceinline__ bool quotient_exceeds(double num, double den, double thr) {
   if (den > 0.0) return num > __dmul_ru(thr, den);

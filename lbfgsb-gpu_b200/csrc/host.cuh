@@ -355,6 +355,7 @@ static void prepare(Workspace<R, H, S>& w, Ctx<R, H, S>& c, Plan& p, int n, int 
   c.wl_i = nullptr;
   c.wl_n = nullptr;
   c.rounds = 0;
+  c.hash_free = (ext && ext->trace) ? 1 : 0;
   for (int k = 0; k < 3; k++) c.X[k] = w.X[k];
   for (int k = 0; k < 2; k++) c.G[k] = w.G[k];
   c.gdummy = nullptr;

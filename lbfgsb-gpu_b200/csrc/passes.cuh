@@ -73,6 +73,7 @@ struct Ctx {
   // device-driven solves: rounds = 1 makes every pass gate itself on the round plan in the
   // state and take its vectors from the buffers below by the roles st->xr / st->gr
   int rounds;
+  int hash_free;     // 1: form the free-set hash (reported only by the per-iteration trace)
   R* X[3];
   R* G[2];
   R* gdummy;         // g of evaluations whose result is not used
@@ -187,36 +188,25 @@ __device__ __forceinline__ void dispatch_cols(int col, F&& f) {
 template <typename R>
 __device__ __forceinline__ int classify_q(R x, R g, R l, R u, int nb, bool& has_bp, R& num,
                                           R& den) {
+  // written with selects rather than branches (the lanes of a warp take different ones):
+  // every value is the reference's, formed from the same operands; bounds that nb does
+  // not declare are read but never selected
   const R neggi = -g;
-  has_bp = false;
-  num = R(0);
-  den = R(1);
-  if (nb == 0) return IW_UNB;
-  if (nb == 2 && rsub(u, l) <= R(0)) return IW_FIX;
-  R tl = 0, tu = 0;
-  if (nb <= 2) tl = rsub(x, l);
-  if (nb >= 2) tu = rsub(u, x);
-  const bool xlower = nb <= 2 && tl <= R(0);
-  const bool xupper = nb >= 2 && tu <= R(0);
-  int code = IW_FREE;
-  if (xlower) {
-    if (neggi <= R(0)) code = IW_LOW;
-  } else if (xupper) {
-    if (neggi >= R(0)) code = IW_UPP;
-  } else if (fabs(neggi) <= R(0)) {
-    code = IW_ZERO;
-  }
-  if (code == IW_FREE) {
-    if (nb <= 2 && neggi < R(0)) {
-      has_bp = true;
-      num = tl;
-      den = -neggi;
-    } else if (nb >= 2 && neggi > R(0)) {
-      has_bp = true;
-      num = tu;
-      den = neggi;
-    }
-  }
+  const bool hl = nb <= 2, hu = nb >= 2;
+  const R tl = rsub(x, l), tu = rsub(u, x);
+  const bool xlower = hl && tl <= R(0);
+  const bool xupper = hu && tu <= R(0);
+  int code = xlower   ? (neggi <= R(0) ? IW_LOW : IW_FREE)
+             : xupper ? (neggi >= R(0) ? IW_UPP : IW_FREE)
+                      : (fabs(neggi) <= R(0) ? IW_ZERO : IW_FREE);
+  const bool fixed = nb == 2 && rsub(u, l) <= R(0);
+  code = nb == 0 ? IW_UNB : fixed ? IW_FIX : code;
+  const bool isfree = code == IW_FREE;
+  const bool bl = isfree && hl && neggi < R(0);
+  const bool bu = isfree && !bl && hu && neggi > R(0);
+  has_bp = bl || bu;
+  num = bl ? tl : bu ? tu : R(0);
+  den = bl ? -neggi : bu ? neggi : R(1);
   return code;
 }
 // classify_q with the breakpoint t = num/den correctly rounded.
@@ -233,13 +223,12 @@ __device__ __forceinline__ int classify(R x, R g, R l, R u, int nb, bool& has_bp
 // fixed it (755-761), x otherwise.
 template <typename R, typename S>
 __device__ __forceinline__ R gcp_point(int code, R x, R g, R l, R u, S tsum) {
-  if (code == IW_FREE || code == IW_UNB) {
-    const S d = (S)(-g);
-    return (R)((S)x + tsum * d);
-  }
-  if (code == IW_WALK_LOW) return l;
-  if (code == IW_WALK_UPP) return u;
-  return x;
+  const S d = (S)(-g);
+  const R moved = (R)((S)x + tsum * d);
+  return (code == IW_FREE || code == IW_UNB) ? moved
+         : code == IW_WALK_LOW             ? l
+         : code == IW_WALK_UPP             ? u
+                                           : x;
 }
 
 // cmprlb's reduced gradient of one free variable (lbfgsbcpu.cpp:842-867), in the
@@ -370,7 +359,7 @@ __device__ __forceinline__ void gcp_scan_pass(const Ctx<R, H, S>& c, CtaPos cp, 
   using A = typename AccOf<S>::type;
   A s[NS];
   double xm[NX];
-  QuotMin<R> bp;  // the smallest breakpoint
+  ArgMin<R> bp;  // the smallest breakpoint
 #pragma unroll
   for (int k = 0; k < NS; k++) s[k] = A(0);
   xm[0] = 0.0;
@@ -397,7 +386,7 @@ __device__ __forceinline__ void gcp_scan_pass(const Ctx<R, H, S>& c, CtaPos cp, 
     run_tiles<CONS>(ss, n, stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)stages * cap),
               &st->device_error, cp, [&](const unsigned char* buf, long long t, int valid, int e) {
       if (e >= valid) return;
-      const long long i = t * kTile + e;
+      const int i = (int)(t * kTile) + e;
       const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
       const R li = stage_at<R>(buf, o_l, e), ui = stage_at<R>(buf, o_u, e);
       const int nb = stage_at<int>(buf, o_nb, e);
@@ -428,7 +417,7 @@ __device__ __forceinline__ void gcp_scan_pass(const Ctx<R, H, S>& c, CtaPos cp, 
   });
   constexpr int W = NS + NX + 2 * NM;
   double lo[1] = {0.0}, sd[NS];
-  MinPair mn[NM] = {bp.mp};
+  MinPair mn[NM] = {bp.pair()};
   sums_to_double(s, sd);
   cta_reduce_to_row<CONS + 32, NS, NX, NM, 0>(sd, xm, mn, lo, c.part, W, cp.rank, cp.count);
   if (!last_cta(c.ticket, cp.count)) return;
@@ -546,7 +535,7 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
     constexpr bool kFull = decltype(cols_tag)::value == kMaxM;
     auto role0 = [&](const unsigned char* buf, long long t, int valid, int e) {
       // the whole warp runs every call (ballots); word e/32 of the tile's free-set bits
-      const long long i = t * kTile + e;
+      const int i = (int)(t * kTile) + e;
       const bool ok = e < valid;
       int code = IW_LOW;
       if (ok) code = stage_at<int8_t>(buf, o_code, e);
@@ -561,7 +550,7 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
       if (ok) {
         if (fnow) {
           cnt[0]++;
-          hash += mix64((unsigned long long)i);
+          if (c.hash_free) hash += mix64((unsigned long long)i);
           const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
           const R zi = uncon ? xi : gcp_point<R, S>(code, xi, gi, R(0), R(0), tsum);
           // cmprlb's r (842-867).  Here it only feeds the W'r reductions (the subspace
@@ -574,8 +563,8 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
   #pragma unroll
             for (int j = 0; j < kMaxM; j++)
               if (kFull || j < col) {
-                ry = fma((S)hist_at<H>(buf, hy + j * hb, e), a1[j], ry);
-                rs = fma((S)hist_at<H>(buf, hs + j * hb, e), a2[j], rs);
+                ry = fma(hist_at<H, S>(buf, hy + j * hb, e), a1[j], ry);
+                rs = fma(hist_at<H, S>(buf, hs + j * hb, e), a2[j], rs);
               }
             r = ry + rs;
           }
@@ -777,32 +766,26 @@ __global__ void __launch_bounds__(CONS + 32) k_freev_formk(Ctx<R, H, S> c,
 // candidates that cannot reach the running minimum skip the exact division.
 template <typename R, typename A>
 __device__ __forceinline__ void lnsrlb_elem(R zi, R xi, R gi, R li, R ui, int nb, bool want_stpmx,
-                                            long long i, A& dtd, A& gd, QuotMin<R>& mn) {
+                                            int i, A& dtd, A& gd, ArgMin<R>& mn) {
   const R big = (R)1.0e10;
   const R d = rsub(zi, xi);
   dtd = fma((A)d, (A)d, dtd);
   gd = fma((A)gi, (A)d, gd);
-  if (!want_stpmx || nb == 0) return;
-  double cand = INFINITY;
-  bool skip = false;  // a candidate that cannot reach the running minimum
-  if (d < R(0) && nb <= 2) {
-    const R a2 = rsub(li, xi);
-    if (a2 >= R(0))
-      cand = 0.0;
-    else if (rmul(d, big) < a2) {
-      skip = quotient_exceeds(a2, d, mn.thr);
-      if (!skip) cand = (double)rdiv(a2, d);
-    }
-  } else if (d > R(0) && nb >= 2) {
-    const R a2 = rsub(ui, xi);
-    if (a2 <= R(0))
-      cand = 0.0;
-    else if (rmul(d, big) > a2) {
-      skip = quotient_exceeds(a2, d, mn.thr);
-      if (!skip) cand = (double)rdiv(a2, d);
-    }
+  if (!want_stpmx) return;
+  // the two cases as selects (the lanes of a warp take different ones); a variable with
+  // neither has no candidate
+  const bool lo = nb != 0 && d < R(0) && nb <= 2;
+  const bool hi = nb != 0 && !lo && d > R(0) && nb >= 2;
+  const R a2 = rsub(lo ? li : ui, xi);
+  const R db = rmul(d, big);
+  const bool at = lo ? a2 >= R(0) : a2 <= R(0);
+  const bool reach = lo ? db < a2 : db > a2;
+  if (lo || hi) {
+    if (at)
+      mn.offer(R(0), i);
+    else if (reach)
+      mn.offer_quotient(a2, d, i);
   }
-  if (!skip) mn.offer(cand, i);
 }
 
 // lnsrlb with task != 1 (1263-1311), then its first dcsrch call (1312-1338), from
@@ -883,8 +866,8 @@ __device__ __forceinline__ void subsm_dir_pass(const Ctx<R, H, S>& c, CtaPos cp,
   }
   // mb: the step to the first bound (alpha); the speculative lnsrlb start at the
   // untruncated step (alpha = 1): sums d'd, g'd and ms the smallest step to a bound
-  QuotMin<S> mb;
-  QuotMin<R> ms;
+  ArgMin<S> mb;
+  ArgMin<R> ms;
   using A = typename AccOf<S>::type;
   A sl[2] = {A(0), A(0)};
   const bool want_stpmx = st->cnstnd && st->iter > 0;
@@ -932,15 +915,15 @@ __device__ __forceinline__ void subsm_dir_pass(const Ctx<R, H, S>& c, CtaPos cp,
         if (uncon || iw_free(v.code)) {
   #pragma unroll
           for (int j = 0; j < kMaxM; j++) {
-            v.yv[j] = (kFull || j < col) ? (S)hist_at<H>(buf, hy + j * hb, e) : S(0);
-            v.sv[j] = (kFull || j < col) ? (S)hist_at<H>(buf, hs + j * hb, e) : S(0);
+            v.yv[j] = (kFull || j < col) ? hist_at<H, S>(buf, hy + j * hb, e) : S(0);
+            v.sv[j] = (kFull || j < col) ? hist_at<H, S>(buf, hs + j * hb, e) : S(0);
           }
         }
       }
       return v;
     }, [&](const DirElem<R, S>& v, long long t, int valid, int e) {
       if (e >= valid) return;
-      const long long i = t * kTile + e;
+      const int i = (int)(t * kTile) + e;
       const int code = v.code;
       if (!(uncon || iw_free(code))) {
         if (!spec) return;
@@ -954,61 +937,72 @@ __device__ __forceinline__ void subsm_dir_pass(const Ctx<R, H, S>& c, CtaPos cp,
       const S(&sv)[kMaxM] = v.sv;
       const R xi = v.x, gi = v.g, li = v.l, ui = v.u;
       const R zi = uncon ? xi : gcp_point<R, S>(code, xi, gi, li, ui, tsum);
-      S d = reduced_grad<R, S>(uncon, xi, zi, gi, kFull ? kMaxM : col, yv, sv, a1, a2);
-      // ... + wy*wv(jy)/theta + ws*wv(js), then d/theta (1472-1483): the divisions by the
-      // pass-constant theta use its reciprocal with Markstein's correction (FixedDiv), which
-      // rounds exactly like the division
-      // the quotients do not depend on d: they are formed side by side without branches,
-      // the rare out-of-range ones redone with the full division, then summed in order
-      S q[kMaxM];
-      bool ok = true;
+      S d;
+      if constexpr (sizeof(S) == 4) {
+        // The FP32 form: r, then d = (r + sum_j wy_j wv_j / theta + ws_j wv_j) / theta
+        // (1472-1483) with fused multiply-adds and the reciprocal of theta, one rounding
+        // more per quotient than the division (the form is held to the FP32 tolerance)
+        const S rth = divt.y;
+        d = uncon ? -(S)gi : -a1[kMaxM] * ((S)zi - (S)xi) - (S)gi;
+        if (!uncon) {
   #pragma unroll
-      for (int j = 0; j < kMaxM; j++) {
-        if (kFull || j < col) {
-          const S a = yv[j] * w1[j];
-          q[j] = divt.markstein(a);
-          ok = ok && divt.in_range(a);
+          for (int j = 0; j < kMaxM; j++)
+            if (kFull || j < col) d = fmaf(sv[j], a2[j], fmaf(yv[j], a1[j], d));
         }
-      }
-      if (!ok) {
+  #pragma unroll
+        for (int j = 0; j < kMaxM; j++)
+          if (kFull || j < col) d = fmaf(sv[j], w2[j], fmaf(yv[j] * w1[j], rth, d));
+        d = d * rth;
+      } else {
+        d = reduced_grad<R, S>(uncon, xi, zi, gi, kFull ? kMaxM : col, yv, sv, a1, a2);
+        // ... + wy*wv(jy)/theta + ws*wv(js), then d/theta (1472-1483): the divisions by
+        // the pass-constant theta use its reciprocal with Markstein's correction (FixedDiv),
+        // which rounds exactly like the division; the quotients do not depend on d: they are
+        // formed side by side without branches, the rare out-of-range ones redone with the
+        // full division, then summed in order
+        S q[kMaxM];
+        bool ok = true;
   #pragma unroll
         for (int j = 0; j < kMaxM; j++) {
           if (kFull || j < col) {
             const S a = yv[j] * w1[j];
-            if (!divt.in_range(a)) q[j] = divt.full(a);
+            q[j] = divt.markstein(a);
+            ok = ok && divt.in_range(a);
           }
         }
-      }
+        if (!ok) {
   #pragma unroll
-      for (int j = 0; j < kMaxM; j++)
-        if (kFull || j < col) d = d + q[j] + sv[j] * w2[j];
-      d = divt(d);
+          for (int j = 0; j < kMaxM; j++) {
+            if (kFull || j < col) {
+              const S a = yv[j] * w1[j];
+              if (!divt.in_range(a)) q[j] = divt.full(a);
+            }
+          }
+        }
+  #pragma unroll
+        for (int j = 0; j < kMaxM; j++)
+          if (kFull || j < col) d = d + q[j] + sv[j] * w2[j];
+        d = divt(d);
+      }
       const R dr = (R)d;
       c.dsub[i] = dr;
-      // candidate step to the bound (1486-1516), filtered as for alpha = 1
+      // candidate step to the bound (1486-1516), filtered as for alpha = 1; the two cases
+      // as selects
       const int nb = v.nb;
       const S dk = (S)dr;
-      if (nb != 0) {
-        double cand = INFINITY;
-        bool skip = false;  // a candidate that cannot reach the running minimum
-        if (dk < S(0) && nb <= 2) {
-          const S temp2 = (S)li - (S)zi;
-          if (temp2 >= S(0))
-            cand = 0.0;
-          else if (dk * S(1) < temp2) {
-            skip = quotient_exceeds(temp2, dk, mb.thr);
-            if (!skip) cand = (double)(temp2 / dk);
-          }
-        } else if (dk > S(0) && nb >= 2) {
-          const S temp2 = (S)ui - (S)zi;
-          if (temp2 <= S(0))
-            cand = 0.0;
-          else if (dk * S(1) > temp2) {
-            skip = quotient_exceeds(temp2, dk, mb.thr);
-            if (!skip) cand = (double)(temp2 / dk);
-          }
+      {
+        const bool lo = nb != 0 && dk < S(0) && nb <= 2;
+        const bool hi = nb != 0 && !lo && dk > S(0) && nb >= 2;
+        const S temp2 = (S)(lo ? li : ui) - (S)zi;
+        const S dk1 = dk * S(1);
+        const bool at = lo ? temp2 >= S(0) : temp2 <= S(0);
+        const bool reach = lo ? dk1 < temp2 : dk1 > temp2;
+        if (lo || hi) {
+          if (at)
+            mb.offer(S(0), i);
+          else if (reach && !quotient_exceeds(temp2, dk, mb.thr))
+            mb.offer(temp2 / dk, i);
         }
-        if (!skip) mb.offer(cand, i);
       }
       // the subspace step with alpha = 1 (1517-1533): z = xcp + d; with the 3.0 step,
       // projected onto the box (the lower bound, then the upper one)
@@ -1030,7 +1024,7 @@ __device__ __forceinline__ void subsm_dir_pass(const Ctx<R, H, S>& c, CtaPos cp,
   constexpr int W = 7;
   // (the pipeline ends with a block barrier, so every thread's flag store is visible)
   double xm[1] = {s_projected ? 1.0 : 0.0}, ldum[1] = {0.0}, sld[2];
-  MinPair mn[2] = {mb.mp, ms.mp};
+  MinPair mn[2] = {mb.pair(), ms.pair()};
   sums_to_double(sl, sld);
   cta_reduce_to_row<CONS + 32, 2, 1, 2, 0>(sld, xm, mn, ldum, c.part, W, cp.rank, cp.count);
   if (!last_cta(c.ticket, cp.count)) return;
@@ -1092,7 +1086,7 @@ __device__ __forceinline__ void subsm_apply_pass(const Ctx<R, H, S>& c, CtaPos c
   const bool want_stpmx = st->cnstnd && st->iter > 0;
   using A = typename AccOf<S>::type;
   A s[2] = {A(0), A(0)};
-  QuotMin<R> ms;
+  ArgMin<R> ms;
 
   extern __shared__ __align__(128) unsigned char dyn[];
   __shared__ StreamSet ss;
@@ -1114,7 +1108,7 @@ __device__ __forceinline__ void subsm_apply_pass(const Ctx<R, H, S>& c, CtaPos c
   run_tiles<CONS>(ss, n, stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)stages * cap),
             &st->device_error, cp, [&](const unsigned char* buf, long long t, int valid, int e) {
     if (e >= valid) return;
-    const long long i = t * kTile + e;
+    const int i = (int)(t * kTile) + e;
     const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
     const R li = stage_at<R>(buf, o_l, e), ui = stage_at<R>(buf, o_u, e);
     const int code = stage_at<int8_t>(buf, o_code, e);
@@ -1138,7 +1132,7 @@ __device__ __forceinline__ void subsm_apply_pass(const Ctx<R, H, S>& c, CtaPos c
   });
   constexpr int W = 4;
   double xdum[1] = {0.0}, ldum[1] = {0.0}, sd[2];
-  MinPair mn[1] = {ms.mp};
+  MinPair mn[1] = {ms.pair()};
   sums_to_double(s, sd);
   cta_reduce_to_row<CONS + 32, 2, 0, 1, 0>(sd, xdum, mn, ldum, c.part, W, cp.rank, cp.count);
   if (!last_cta(c.ticket, cp.count)) return;
@@ -1343,22 +1337,18 @@ __device__ __forceinline__ void post_eval_pass(const Ctx<R, H, S>& c, CtaPos cp,
     run_tiles<CONS>(ss, n, stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)stages * cap),
               &st->device_error, cp, [&](const unsigned char* buf, long long tt, int valid, int e) {
       if (e >= valid) return;
-      const long long i = tt * kTile + e;
+      const int i = (int)(tt * kTile) + e;
       const R ti = stage_at<R>(buf, o_t, e), zi = stage_at<R>(buf, o_z, e);
       const R xi = stage_at<R>(buf, o_xt, e), gi = stage_at<R>(buf, o_g, e);
       const R gold = stage_at<R>(buf, o_go, e);
       const R d = rsub(zi, ti);
       s[0] = fma((A)gi, (A)d, s[0]);
-      // projgr (1389-1414)
+      // projgr (1389-1414), its cases as selects
       const int nb = stage_at<int>(buf, o_nb, e);
-      R pg = gi;
-      if (nb != 0) {
-        if (gi < R(0)) {
-          if (nb >= 2) pg = smax<R>(rsub(xi, stage_at<R>(buf, o_u, e)), gi);
-        } else {
-          if (nb <= 2) pg = smin<R>(rsub(xi, stage_at<R>(buf, o_l, e)), gi);
-        }
-      }
+      const bool neg = gi < R(0);
+      const R tb = rsub(xi, stage_at<R>(buf, neg ? o_u : o_l, e));
+      const bool clip = nb != 0 && (neg ? nb >= 2 : nb <= 2);
+      const R pg = clip ? (neg ? smax<R>(tb, gi) : smin<R>(tb, gi)) : gi;
       const A apg = fabs((A)pg);
       xa = (apg > xa) ? apg : xa;
       const R xd = rsub(ti, xi);
@@ -1575,7 +1565,7 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
 #pragma unroll
   for (int k = 0; k < NG; k++) acc[k] = A(0);
   A xmx = A(0);
-  QuotMin<R> bp;  // role G: the smallest breakpoint
+  ArgMin<R> bp;  // role G: the smallest breakpoint
 
   extern __shared__ __align__(128) unsigned char dyn[];
   __shared__ StreamSet ss;
@@ -1604,22 +1594,18 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
     constexpr bool kFull = decltype(cols_tag)::value == kMaxM;
     auto post_elem = [&](const unsigned char* buf, long long tt, int valid, int e) {
       if (e >= valid) return;
-      const long long i = tt * kTile + e;
+      const int i = (int)(tt * kTile) + e;
       const R ti = stage_at<R>(buf, o_t, e), zi = stage_at<R>(buf, o_z, e);
       const R xi = stage_at<R>(buf, o_xt, e), gi = stage_at<R>(buf, o_g, e);
       const R gold = stage_at<R>(buf, o_go, e);
       const R d = rsub(zi, ti);
       acc[0] = fma((A)gi, (A)d, acc[0]);
-      // projgr (1389-1414)
+      // projgr (1389-1414), its cases as selects
       const int nb = stage_at<int>(buf, o_nb, e);
-      R pg = gi;
-      if (nb != 0) {
-        if (gi < R(0)) {
-          if (nb >= 2) pg = smax<R>(rsub(xi, stage_at<R>(buf, o_u, e)), gi);
-        } else {
-          if (nb <= 2) pg = smin<R>(rsub(xi, stage_at<R>(buf, o_l, e)), gi);
-        }
-      }
+      const bool neg = gi < R(0);
+      const R tb = rsub(xi, stage_at<R>(buf, neg ? o_u : o_l, e));
+      const bool clip = nb != 0 && (neg ? nb >= 2 : nb <= 2);
+      const R pg = clip ? (neg ? smax<R>(tb, gi) : smin<R>(tb, gi)) : gi;
       const A apg = fabs((A)pg);
       xmx = (apg > xmx) ? apg : xmx;
       const R xd = rsub(ti, xi);
@@ -1639,7 +1625,7 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
     };
     auto gcp_elem = [&](const unsigned char* buf, long long tt, int valid, int e) {
       if (e >= valid) return;
-      const long long i = tt * kTile + e;
+      const int i = (int)(tt * kTile) + e;
       const R xi = stage_at<R>(buf, o_xt, e), gi = stage_at<R>(buf, o_g, e);
       const R li = stage_at<R>(buf, o_l, e), ui = stage_at<R>(buf, o_u, e);
       const int nb = stage_at<int>(buf, o_nb, e);
@@ -1701,7 +1687,7 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
       if (lane == 0 && k < cnt) wsum[warp][off + k] = v;
     }
     const double xv = warp_max((double)xmx);
-    const MinPair mv = warp_min(bp.mp);
+    const MinPair mv = warp_min(bp.pair());
     if (lane == 0) {
       if (role < 2) wsum[warp][NS + role] = xv;
       wsum[warp][NS + 2] = role == 1 ? mv.v : INFINITY;

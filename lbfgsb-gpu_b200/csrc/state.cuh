@@ -110,23 +110,31 @@ __host__ __device__ __forceinline__ MinPair minpair(MinPair a, MinPair b) {
   return a;
 }
 
-// A running arg-min of quotients with the filter bound of its value in the quotients'
-// type T (quotient_exceeds), updated only when the minimum changes.
+// One thread's running arg-min of candidate values in their own type T (breakpoints,
+// steps to a bound), with the filter bound thr = the least T above the minimum
+// (quotient_exceeds).  A thread meets its elements in increasing index order, so a
+// candidate replaces the minimum only when it is strictly smaller; across threads the
+// reductions break ties by the lower index (minpair).  A thread without a candidate
+// reports (+inf, kNoIndex).
 template <typename T>
-struct QuotMin {
-  MinPair mp;
+struct ArgMin {
+  T v;
+  int i;
   T thr;
-  __device__ __forceinline__ QuotMin() : mp{INFINITY, kNoIndex}, thr(T(INFINITY)) {}
-  __device__ __forceinline__ void offer(double v, long long i) {
-    const MinPair nm = minpair(mp, MinPair{v, i});
-    if (nm.i != mp.i || nm.v != mp.v) {
-      mp = nm;
-      thr = quotient_bound<T>(mp.v);
+  __device__ __forceinline__ ArgMin() : v(T(INFINITY)), i(-1), thr(T(INFINITY)) {}
+  __device__ __forceinline__ void offer(T c, int k) {
+    if (c < v) {
+      v = c;
+      i = k;
+      thr = next_up(c);
     }
   }
   // the candidate num/den, formed (correctly rounded) only when it may be the minimum
-  __device__ __forceinline__ void offer_quotient(T num, T den, long long i) {
-    if (!quotient_exceeds(num, den, thr)) offer((double)rdiv(num, den), i);
+  __device__ __forceinline__ void offer_quotient(T num, T den, int k) {
+    if (!quotient_exceeds(num, den, thr)) offer(rdiv(num, den), k);
+  }
+  __device__ __forceinline__ MinPair pair() const {
+    return MinPair{(double)v, i < 0 ? kNoIndex : (long long)i};
   }
 };
 

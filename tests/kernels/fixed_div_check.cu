@@ -1,9 +1,9 @@
 // Compares the fixed-divisor quotient of csrc/common.cuh (FixedDiv64 / FixedDiv32) with
 // CUDA's correctly rounded division (__ddiv_rn / __fdiv_rn) bit for bit on random and
 // constructed inputs, and checks that the arg-min filter
-// quotient_exceeds(num, den, quotient_bound<T>(best)) never reports a quotient whose
-// correctly rounded value is <= best (with best at, just below and just above that value,
-// and far from it).  Prints the number of mismatches /
+// quotient_exceeds(num, den, next_up(best)) never reports a quotient whose correctly
+// rounded value is <= best (with best at, just below and just above that value, and far
+// from it).  Prints the number of mismatches /
 // violations per family and exits 1 if any.
 //   argv[1] = millions of random pairs per family (default 64)
 #include <cuda_runtime.h>
@@ -128,17 +128,18 @@ __global__ void k_check_filter(long long count, unsigned long long seed, unsigne
     const T num = rand_real<T>(s, -wide, wide);
     const T den = rand_real<T>(s, -wide, wide);
     const T q = num / den;  // correctly rounded
-    double best;
+    // the running minimum in the quotients' type, as the passes keep it
+    T best;
     const int mode = (int)(k % 6);
-    if (mode == 0) best = (double)q;
-    else if (mode == 1) best = (double)q * (1.0 - 1e-12);
-    else if (mode == 2) best = (double)q * (1.0 + 1e-12);
-    else if (mode == 3) best = (double)q * 0.5;
-    else if (mode == 4) best = (double)q * 2.0;
-    else best = (double)q * (1.0 - 1e-6);
-    if (quotient_exceeds(num, den, quotient_bound<T>(best))) {
+    if (mode == 0) best = q;
+    else if (mode == 1) best = -next_up(-q);  // the value just below q
+    else if (mode == 2) best = next_up(q);
+    else if (mode == 3) best = q * T(0.5);
+    else if (mode == 4) best = q * T(2);
+    else best = (T)((double)q * (1.0 - 1e-6));
+    if (quotient_exceeds(num, den, next_up(best))) {
       atomicAdd(&bad[1], 1ULL);
-      if (!((double)q > best)) atomicAdd(&bad[0], 1ULL);
+      if (!(q > best)) atomicAdd(&bad[0], 1ULL);
     }
   }
 }
