@@ -647,7 +647,7 @@ class BatchRunner {
     kb_gcp_scan<R, H, S, kConsWide><<<ctas_pass_, thr, ring_bytes(2, cap_gcp_), s_>>>(bp);
     kb_walk_gather<R, H, S><<<ctas_elem_, kThreads, 0, s_>>>(be);
     kb_walk<R, H, S><<<cnt, kWalkThreads, 0, s_>>>(table_);
-    kb_freev_formk<R, H, S, kConsWide><<<ctas_pass_, thr, ring_bytes(2, cap_freev_), s_>>>(bp);
+    kb_freev_formk<R, H, S, kConsWide><<<ctas_pass_, thr, ring_bytes(2, cap_freev_) + freev_extra_smem<S>(), s_>>>(bp);
     kb_subsm_dir<R, H, S, kConsWide><<<ctas_pass_, thr, ring_bytes(2, cap_dir_), s_>>>(bp);
     kb_subsm_apply<R, H, S, kConsWide><<<ctas_pass_, thr, ring_bytes(2, cap_apply_), s_>>>(bp);
     kb_round<R, H, S, RK_PRE><<<rb, 128, 0, s_>>>(table_, cnt);

@@ -205,8 +205,9 @@ struct PassCfg {
 constexpr int kConsWide = 512;    // consumer threads of the staged passes
 constexpr int kRingBudget = 176 * 1024;
 
+// extra: dynamic shared memory the pass uses after its ring (freev_extra_smem).
 template <typename K>
-static PassCfg pass_cfg(K kernel, int cap, long long n, int threads) {
+static PassCfg pass_cfg(K kernel, int cap, long long n, int threads, int extra = 0) {
   PassCfg p;
   p.threads = threads;
   // a CTA never has more tiles in flight than it processes: small problems take fewer
@@ -214,7 +215,6 @@ static PassCfg pass_cfg(K kernel, int cap, long long n, int threads) {
   const long long tiles = (n + kTile - 1) / kTile;
   const long long per_cta = (tiles + device_sms() - 1) / device_sms();
   p.stages = std::max(2, std::min<int>(std::min(kMaxStages, kRingBudget / cap), (int)per_cta + 1));
-  p.smem = ring_bytes(p.stages, cap);
   // the attribute is per kernel and process-wide, while solves of different sizes may run
   // concurrently on other threads: it is always set to the full opt-in allowance (the same
   // value from every thread), and each launch asks only for its own ring
@@ -224,6 +224,8 @@ static PassCfg pass_cfg(K kernel, int cap, long long n, int threads) {
   cudaFuncAttributes fa;
   CK(cudaFuncGetAttributes(&fa, kernel));
   const int allowance = optin - (int)fa.sharedSizeBytes;
+  while (p.stages > 2 && ring_bytes(p.stages, cap) + extra > allowance) p.stages--;
+  p.smem = ring_bytes(p.stages, cap) + extra;
   if (p.smem > allowance) throw CudaFailure{cudaErrorInvalidValue, "stage ring exceeds shared memory", __LINE__};
   CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, allowance));
   int per_sm = 0;
@@ -370,7 +372,8 @@ static void prepare(Workspace<R, H, S>& w, Ctx<R, H, S>& c, Plan& p, int n, int 
   p.gcp = pass_cfg(k_gcp_scan<R, H, S, kConsWide>,
                    stage_capacity(StageBytes<R>::gcp, 0, m, hsz), n, kConsWide + 32);
   p.freev = pass_cfg(k_freev_formk<R, H, S, kConsWide>,
-                     stage_capacity(StageBytes<R>::freev, kTile / 8, m, hsz), n, kConsWide + 32);
+                     stage_capacity(StageBytes<R>::freev, kTile / 8, m, hsz), n, kConsWide + 32,
+                     freev_extra_smem<S>());
   p.dir = pass_cfg(k_subsm_dir<R, H, S, kConsWide>,
                    stage_capacity(StageBytes<R>::dir, 0, m, hsz), n, kConsWide + 32);
   p.apply = pass_cfg(k_subsm_apply<R, H, S, kConsWide>,

@@ -113,6 +113,12 @@ __host__ __device__ inline int stage_capacity(int scalar, int extra_tile, int m,
   return kTile * scalar + extra_tile + 2 * m * kTile * hsize;
 }
 __host__ __device__ inline int ring_bytes(int stages, int cap) { return stages * cap + 16 * stages; }
+// Dynamic shared memory the free-set pass needs after its stage ring: the per-thread
+// active-set sums of its one-role form (float sums), 16 floats for each of kTile threads.
+template <typename S>
+__host__ __device__ constexpr int freev_extra_smem() {
+  return sizeof(typename AccOf<S>::type) == 4 ? 16 * kTile * (int)sizeof(float) : 0;
+}
 
 __device__ __forceinline__ int add_stream(StreamSet& ss, const void* base, int tile_bytes) {
   const int j = ss.count++;
@@ -491,19 +497,36 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
   //   role 1 (warps 8..11, 4 elements per thread), when a pair was just added:
   //     acc[0..7] sum_F y_col y_j, acc[8..15] sum_F s_j y_col;
   //   role 2 (warps 12..15): acc[0..7] sum_A s_col s_j, acc[8..15] sum_A s_col y_j.
+  //
+  // With float sums (the FP32 plain form) the accumulators are small enough for one role:
+  // every consumer thread does all of one element's work per tile (kOneRole), so that the
+  // work stays balanced over the 16 warps whatever the share of free variables (with the
+  // role split, the warps of the role that has no variables in a tile wait for the others).
   static_assert(CONS == 512, "the role split assumes 16 consumer warps");
-  constexpr int kRole0Warps = 8, kRole12Warps = 4;
+  using A = typename AccOf<S>::type;
+  constexpr bool kOneRole = sizeof(A) == 4;
+  static_assert(!kOneRole || CONS == kTile, "one element per consumer thread and tile");
+  constexpr int kRole0Warps = kOneRole ? CONS / 32 : 8, kRole12Warps = 4;
   constexpr int NA = 2 * kMaxM + 5, NB = 2 * kMaxM, NC = 2 * kMaxM;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int role = warp < kRole0Warps ? 0
+                 : kOneRole ? 3
                  : warp < kRole0Warps + kRole12Warps ? 1
                  : warp < kRole0Warps + 2 * kRole12Warps ? 2 : 3;  // 3: the producer
   const int rt = role == 0 ? (int)threadIdx.x
                : (int)threadIdx.x - 32 * (kRole0Warps + (role - 1) * kRole12Warps);
-  using A = typename AccOf<S>::type;
   A acc[2 * kMaxM];
 #pragma unroll
   for (int k = 0; k < 2 * kMaxM; k++) acc[k] = A(0);
+  // kOneRole: the new row's products (roles 1 and 2 of the split): [0..7] sum_F y_col y_j,
+  // [8..15] sum_F s_j y_col in registers; sum_A s_col s_j and sum_A s_col y_j per thread in
+  // shared memory after the stage ring (entry q of thread e at nra[(q / 4) * CONS + e],
+  // component q % 4), which keeps the thread within the register file's share of a
+  // 17-warp CTA
+  A nrow[kOneRole ? 2 * kMaxM : 1];
+#pragma unroll
+  for (int k = 0; k < (kOneRole ? 2 * kMaxM : 1); k++) nrow[k] = A(0);
+
   int cnt[5] = {0, 0, 0, 0, 0};
   unsigned long long hash = 0;
   __shared__ double corr_sm[kRole0Warps][32 * kLaneOwned];
@@ -513,6 +536,7 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
     for (int k = 0; k < kLaneOwned; k++) corr_sm[warp][32 * k + lane] = 0.0;
   }
   const int newest = col - 1;
+  const bool need_row = updatd && col > 0;
 
   extern __shared__ __align__(128) unsigned char dyn[];
   __shared__ StreamSet ss;
@@ -530,6 +554,11 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
   const int o_code = ss.off[0], o_bits = ss.off[1], o_x = ss.off[2], o_g = ss.off[3];
   const int hy = s_hy, hs = s_hs, hb = kTile * (int)sizeof(H);
   const int cap = stage_capacity(StageBytes<R>::freev, kTile / 8, st->m, (int)sizeof(H));
+  float4* nra = reinterpret_cast<float4*>(dyn + ring_bytes(stages, cap));
+  if (kOneRole && threadIdx.x < CONS) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) nra[q * CONS + threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
 
   dispatch_cols(col, [&](auto cols_tag) {
     constexpr bool kFull = decltype(cols_tag)::value == kMaxM;
@@ -610,6 +639,118 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
         __syncwarp();
       }
     };
+    // kOneRole: all of element e's work.  Its 2*col history values are read from the stage
+    // once, into registers; the sums are those of roles 0, 1 and 2 below, with the same
+    // operands in each fma.
+    auto one_role = [&](const unsigned char* buf, long long t, int valid, int e) {
+      const int i = (int)(t * kTile) + e;
+      const bool ok = e < valid;
+      int code = IW_LOW;
+      if (ok) code = stage_at<int8_t>(buf, o_code, e);
+      const bool fnow = ok && (uncon || iw_free(code));
+      const int wi = e >> 5;
+      const uint32_t word = stage_at<uint32_t>(buf, o_bits, wi);
+      const bool fprev = (word >> lane) & 1u;
+      const bool enter = track && ok && !fprev && fnow;
+      const bool leave = track && ok && fprev && !fnow;
+      const uint32_t newword = __ballot_sync(0xffffffffu, fnow);
+      if (!uncon && lane == 0 && wi * 32 < valid) c.fbits[t * (kTile / 32) + wi] = newword;
+      if (ok) {
+        A yv[kMaxM], sv[kMaxM];
+  #pragma unroll
+        for (int j = 0; j < kMaxM; j++) {
+          const bool live = kFull || j < col;
+          yv[j] = live ? hist_at<H, A>(buf, hy + j * hb, e) : A(0);
+          sv[j] = live ? hist_at<H, A>(buf, hs + j * hb, e) : A(0);
+        }
+        // the newest column, selected without a runtime register index
+        const int nw = kFull ? kMaxM - 1 : newest;
+        A ynew = A(0), snew = A(0);
+  #pragma unroll
+        for (int j = 0; j < kMaxM; j++)
+          if (j == nw) {
+            ynew = yv[j];
+            snew = sv[j];
+          }
+        if (fnow) {
+          cnt[0]++;
+          if (c.hash_free) hash += mix64((unsigned long long)i);
+          const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
+          const R zi = uncon ? xi : gcp_point<R, S>(code, xi, gi, R(0), R(0), tsum);
+          S r = -(S)gi;
+          if (!uncon) {
+            S ry = -a1[kMaxM] * ((S)zi - (S)xi) - (S)gi, rs = S(0);
+  #pragma unroll
+            for (int j = 0; j < kMaxM; j++)
+              if (kFull || j < col) {
+                ry = fma((S)yv[j], a1[j], ry);
+                rs = fma((S)sv[j], a2[j], rs);
+              }
+            r = ry + rs;
+          }
+  #pragma unroll
+          for (int j = 0; j < kMaxM; j++) {
+            if (kFull || j < col) {
+              acc[j] = fma(yv[j], (A)r, acc[j]);
+              acc[8 + j] = fma(sv[j], (A)r, acc[8 + j]);
+            }
+          }
+          if (need_row) {
+  #pragma unroll
+            for (int j = 0; j < kMaxM; j++) {
+              if (kFull || j < col) {
+                nrow[j] = fma(ynew, yv[j], nrow[j]);
+                nrow[8 + j] = fma(sv[j], ynew, nrow[8 + j]);
+              }
+            }
+          }
+        } else {
+          if (code == IW_LOW || code == IW_WALK_LOW) cnt[3]++;
+          if (code == IW_UPP || code == IW_WALK_UPP) cnt[4]++;
+          if (need_row) {
+            // columns past col hold zeros and add nothing
+  #pragma unroll
+            for (int q = 0; q < 4; q++) {
+              float4 v = nra[q * CONS + e];
+              const A* src = q < 2 ? sv : yv;
+              const int j0 = (q & 1) * 4;
+              v.x = fmaf((float)snew, (float)src[j0 + 0], v.x);
+              v.y = fmaf((float)snew, (float)src[j0 + 1], v.y);
+              v.z = fmaf((float)snew, (float)src[j0 + 2], v.z);
+              v.w = fmaf((float)snew, (float)src[j0 + 3], v.w);
+              nra[q * CONS + e] = v;
+            }
+          }
+        }
+        if (enter) cnt[1]++;
+        if (leave) cnt[2]++;
+      }
+      // entering (+) / leaving (-) variables, as in role 0
+      uint32_t pick = __ballot_sync(0xffffffffu, enter || leave);
+      while (pick) {
+        const int src = __ffs(pick) - 1;
+        pick &= pick - 1;
+        const double sign = __shfl_sync(0xffffffffu, enter ? 1.0 : -1.0, src);
+        const int es = e - lane + src;
+        if (lane < kMaxM)
+          bc[warp][lane] = lane < col ? hist_at<H>(buf, hy + lane * hb, es) : 0.0;
+        else if (lane < 2 * kMaxM)
+          bc[warp][lane] = lane - kMaxM < col ? hist_at<H>(buf, hs + (lane - kMaxM) * hb, es) : 0.0;
+        __syncwarp();
+  #pragma unroll
+        for (int k = 0; k < kLaneOwned; k++) {
+          int kind, a, b;
+          corr_map(lane + 32 * k, kind, a, b);
+          if (kind < 3) {
+            const int oa = kind == 0 ? a : kMaxM + a;
+            const int ob = kind == 1 ? kMaxM + b : b;
+            double& cq = corr_sm[warp][32 * k + lane];
+            cq = fma(sign * bc[warp][oa], bc[warp][ob], cq);
+          }
+        }
+        __syncwarp();
+      }
+    };
     // roles 1 and 2: the new row's products over the free (role 1) or active (role 2) set
     auto rowprod = [&](const unsigned char* buf, int valid, int e) {
       if (e >= valid) return;
@@ -627,11 +768,12 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
         }
       }
     };
-    const bool need_row = updatd && col > 0;
     run_stages<CONS>(ss, n, stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)stages * cap),
                      &st->device_error, cp, [&](const unsigned char* buf, long long t, int valid,
                                             auto release) {
-      if (role == 0) {
+      if constexpr (kOneRole) {
+        one_role(buf, t, valid, (int)threadIdx.x);
+      } else if (role == 0) {
   #pragma unroll
         for (int h = 0; h < kTile / (32 * kRole0Warps); h++)
           role0(buf, t, valid, rt + h * 32 * kRole0Warps);
@@ -662,6 +804,24 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
     for (int k = 0; k < 2 * kMaxM; k++) {
       const double v = warp_sum((double)acc[k]);
       if (lane == 0 && role < 3) wsum[warp][off + k] = v;
+    }
+    if constexpr (kOneRole) {
+#pragma unroll
+      for (int k = 0; k < 2 * kMaxM; k++) {
+        const double v = warp_sum((double)nrow[k]);
+        if (lane == 0 && role == 0) wsum[warp][NA + k] = v;
+      }
+      const int me = role == 0 ? (int)threadIdx.x : 0;
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const float4 a = nra[q * CONS + me];
+        const float comp[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const double v = warp_sum(role == 0 ? (double)comp[k] : 0.0);
+          if (lane == 0 && role == 0) wsum[warp][NA + NB + 4 * q + k] = v;
+        }
+      }
     }
 #pragma unroll
     for (int k = 0; k < 5; k++) {
@@ -1550,21 +1710,30 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
   const bool unit = st->stp == S(1);
   H* ysp = c.wy + (size_t)st->spare * (size_t)c.ld;
   H* ssp = c.ws + (size_t)st->spare * (size_t)c.ld;
-  constexpr int kRoleWarps = 8, kRoleThreads = 32 * kRoleWarps;
+  // With float sums (the FP32 plain form) one role does both (kOneRole): every consumer
+  // thread runs role P and role G on one element per tile, reading the element's inputs
+  // and history values from the stage once.
+  using A = typename AccOf<S>::type;
+  constexpr bool kOneRole = sizeof(A) == 4;
+  static_assert(!kOneRole || CONS == kTile, "one element per consumer thread and tile");
+  constexpr int kRoleWarps = kOneRole ? CONS / 32 : 8, kRoleThreads = 32 * kRoleWarps;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int role = warp < kRoleWarps ? 0 : warp < 2 * kRoleWarps ? 1 : 2;  // 2: producer
+  const int role = warp < kRoleWarps ? 0 : (!kOneRole && warp < 2 * kRoleWarps) ? 1 : 2;  // 2: producer
   const int rt = (int)threadIdx.x - (role == 1 ? kRoleThreads : 0);
   // role P: acc[0] g'd, [1] |xold - x|^2, [2] y'y, [3..10] s'y_j, [11..18] s_j's;
   //   xmx |proj g|.
   // role G: acc[0] sum g^2 (movable), [1..8] / [9..16] y_j'(-g) / s_j'(-g) by old ring
   //   position, [17] / [18] y'(-g) / s'(-g) of the new pair, [19] nbreak, [20] movable
   //   without breakpoint; xmx: any of those with g != 0; mn: smallest breakpoint.
+  //   kOneRole: role G's sums in accg, its xmx in xmxg.
   constexpr int NP = 19, NG = 21;
-  using A = typename AccOf<S>::type;
   A acc[NG];
 #pragma unroll
   for (int k = 0; k < NG; k++) acc[k] = A(0);
-  A xmx = A(0);
+  A accg[kOneRole ? NG : 1];
+#pragma unroll
+  for (int k = 0; k < (kOneRole ? NG : 1); k++) accg[k] = A(0);
+  A xmx = A(0), xmxg = A(0);
   ArgMin<R> bp;  // role G: the smallest breakpoint
 
   extern __shared__ __align__(128) unsigned char dyn[];
@@ -1659,10 +1828,77 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
         }
       }
     };
+    // kOneRole: post_elem and gcp_elem on one element, each input read from the stage once
+    auto one_role = [&](const unsigned char* buf, long long tt, int valid, int e) {
+      if (e >= valid) return;
+      const int i = (int)(tt * kTile) + e;
+      const R ti = stage_at<R>(buf, o_t, e), zi = stage_at<R>(buf, o_z, e);
+      const R xi = stage_at<R>(buf, o_xt, e), gi = stage_at<R>(buf, o_g, e);
+      const R gold = stage_at<R>(buf, o_go, e);
+      const R li = stage_at<R>(buf, o_l, e), ui = stage_at<R>(buf, o_u, e);
+      const int nb = stage_at<int>(buf, o_nb, e);
+      A yv[kMaxM], sh[kMaxM];
+#pragma unroll
+      for (int j = 0; j < kMaxM; j++) {
+        const bool live = kFull || j < col;
+        yv[j] = live ? hist_at<H, A>(buf, hy + j * hb, e) : A(0);
+        sh[j] = live ? hist_at<H, A>(buf, hs + j * hb, e) : A(0);
+      }
+      // role P
+      const R d = rsub(zi, ti);
+      acc[0] = fma((A)gi, (A)d, acc[0]);
+      const bool neg = gi < R(0);
+      const R tb = rsub(xi, neg ? ui : li);
+      const bool clip = nb != 0 && (neg ? nb >= 2 : nb <= 2);
+      const R pg = clip ? (neg ? smax<R>(tb, gi) : smin<R>(tb, gi)) : gi;
+      const A apg = fabs((A)pg);
+      xmx = (apg > xmx) ? apg : xmx;
+      const R xd = rsub(ti, xi);
+      acc[1] = fma((A)xd, (A)xd, acc[1]);
+      const R y = rsub(gi, gold);
+      acc[2] = fma((A)y, (A)y, acc[2]);
+      const R sv = unit ? d : rmul(d, stp);
+#pragma unroll
+      for (int j = 0; j < kMaxM; j++) {
+        if (kFull || j < col) {
+          acc[3 + j] = fma((A)sv, yv[j], acc[3 + j]);
+          acc[11 + j] = fma(sh[j], (A)sv, acc[11 + j]);
+        }
+      }
+      ssp[i] = HistTraits<H>::from(sv);
+      ysp[i] = HistTraits<H>::from(y);
+      // role G
+      bool has_bp;
+      R tnum, tden;
+      const int code = classify_q(xi, gi, li, ui, nb, has_bp, tnum, tden);
+      c.code[i] = (int8_t)code;
+      if (code == IW_FREE || code == IW_UNB) {
+        const A neggi = -(A)gi;
+        accg[0] = fma(neggi, neggi, accg[0]);
+#pragma unroll
+        for (int j = 0; j < kMaxM; j++) {
+          if (kFull || j < col) {
+            accg[1 + j] = fma(yv[j], neggi, accg[1 + j]);
+            accg[9 + j] = fma(sh[j], neggi, accg[9 + j]);
+          }
+        }
+        accg[17] = fma(stored_value<H, A>(y), neggi, accg[17]);
+        accg[18] = fma(stored_value<H, A>(sv), neggi, accg[18]);
+        if (has_bp) {
+          accg[19] += A(1);
+          bp.offer_quotient(tnum, tden, i);
+        } else {
+          accg[20] += A(1);
+          if (neggi != A(0)) xmxg = A(1);
+        }
+      }
+    };
     run_stages<CONS>(ss, n, stages, dyn,
                      reinterpret_cast<uint64_t*>(dyn + (size_t)stages * cap), &st->device_error, cp,
                      [&](const unsigned char* buf, long long tt, int valid, auto release) {
-      if (role == 0) {
+      if constexpr (kOneRole) {
+        one_role(buf, tt, valid, (int)threadIdx.x);
+      } else if (role == 0) {
 #pragma unroll
         for (int h = 0; h < kTile / kRoleThreads; h++) post_elem(buf, tt, valid, rt + h * kRoleThreads);
       } else {
@@ -1686,12 +1922,23 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
       const double v = warp_sum((double)acc[k]);
       if (lane == 0 && k < cnt) wsum[warp][off + k] = v;
     }
+    // the warps that ran role G (kOneRole: role 0 ran both)
+    const int grole = kOneRole ? 0 : 1;
+    if constexpr (kOneRole) {
+#pragma unroll
+      for (int k = 0; k < NG; k++) {
+        const double v = warp_sum((double)accg[k]);
+        if (lane == 0 && role == 0) wsum[warp][NP + k] = v;
+      }
+    }
     const double xv = warp_max((double)xmx);
+    const double xvg = warp_max((double)xmxg);
     const MinPair mv = warp_min(bp.pair());
     if (lane == 0) {
       if (role < 2) wsum[warp][NS + role] = xv;
-      wsum[warp][NS + 2] = role == 1 ? mv.v : INFINITY;
-      wsum[warp][NS + 3] = role == 1 ? (double)mv.i : (double)kNoIndex;
+      if (kOneRole && role == 0) wsum[warp][NS + 1] = xvg;
+      wsum[warp][NS + 2] = role == grole ? mv.v : INFINITY;
+      wsum[warp][NS + 3] = role == grole ? (double)mv.i : (double)kNoIndex;
     }
     __syncthreads();
     double* row = c.part + cp.rank;  // entry k at row[k * cp.count] (reduce.cuh)

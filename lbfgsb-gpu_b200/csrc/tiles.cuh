@@ -19,7 +19,7 @@ namespace lbfgsb_b200 {
 
 constexpr int kTile = 512;          // elements per tile
 constexpr int kMaxStreams = 24;
-constexpr long long kWaitPolls = 1LL << 24;
+constexpr int kWaitPolls = 1 << 24;
 
 // Bulk copies need 16-byte aligned addresses and sizes; the host pads the history slot
 // stride to a multiple of kTile elements and checks the user's arrays.
@@ -65,7 +65,7 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 
 // Bounded wait; false after kWaitPolls polls.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (long long k = 0; k < kWaitPolls; k++)
+  for (int k = 0; k < kWaitPolls; k++)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -172,15 +172,18 @@ __device__ __forceinline__ bool run_stages(const StreamSet& ss, long long n, int
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // The k-th tile of the CTA goes to stage s = k mod stages in round k / stages; both are
+  // stepped along (no division per tile), with ph the parity of the round.
   if (warp == kConsumerWarps) {
     // producer
-    long long k = 0;
-    for (long long t = cp.rank; t < ntiles; t += cp.count, k++) {
-      const int s = (int)(k % stages);
-      if (k >= stages) {
-        const uint32_t parity = (uint32_t)(((k / stages) - 1) & 1);
+    int s = 0;
+    uint32_t ph = 0;
+    bool wrapped = false;
+    for (long long t = cp.rank; t < ntiles; t += cp.count) {
+      if (wrapped) {
+        // the stage's previous tile (one round earlier) must have been released
         bool ok = true;
-        if (lane == 0) ok = mbar_wait(&empty[s], parity);
+        if (lane == 0) ok = mbar_wait(&empty[s], ph ^ 1u);
         ok = __shfl_sync(0xffffffffu, ok, 0);
         if (!ok || *(volatile int*)&timed_out) {
           if (lane == 0) timed_out = 1;
@@ -188,14 +191,19 @@ __device__ __forceinline__ bool run_stages(const StreamSet& ss, long long n, int
         }
       }
       load_tile(ss, t, n, ring + (size_t)s * ss.stage_bytes, &full[s]);
+      if (++s == stages) {
+        s = 0;
+        ph ^= 1u;
+        wrapped = true;
+      }
     }
   } else {
     // consumers
-    long long k = 0;
-    for (long long t = cp.rank; t < ntiles; t += cp.count, k++) {
-      const int s = (int)(k % stages);
+    int s = 0;
+    uint32_t ph = 0;
+    for (long long t = cp.rank; t < ntiles; t += cp.count) {
       const unsigned char* buf = ring + (size_t)s * ss.stage_bytes;
-      const bool ok = __all_sync(0xffffffffu, mbar_wait(&full[s], (uint32_t)((k / stages) & 1)));
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(&full[s], ph));
       if (!ok) {
         if (lane == 0) timed_out = 1;
         break;
@@ -205,6 +213,10 @@ __device__ __forceinline__ bool run_stages(const StreamSet& ss, long long n, int
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);
       });
+      if (++s == stages) {
+        s = 0;
+        ph ^= 1u;
+      }
     }
   }
   __syncthreads();
