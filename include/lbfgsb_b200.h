@@ -220,6 +220,55 @@ int lbfgsb_b200_minimize_ext_f32(int n, float* x, const int* nbd, const float* l
                                  void* stream, const lbfgsb_b200_ext* ext,
                                  lbfgsb_b200_summary_f32* summary);
 
+/* ---- sharded solves: one problem over several GPUs (no counterpart in the reference) --
+ * The reference solves one problem on one GPU (lbfgsbcuda.cpp:39-441).  Here a problem of
+ * n_global variables can be split by index range over `world` ranks, one process (or
+ * thread) per GPU: rank r holds the n_local variables offset .. offset + n_local - 1 (its
+ * slices of x, nbd, l and u, and its rows of the S/Y history).  Every pass of an iteration
+ * sweeps only the local variables; its small reductions (about 200 doubles) are combined
+ * over the ranks through `allgather`, and every rank then runs the same scalar steps, so
+ * every rank keeps the same solver state and takes the same decisions.
+ *
+ * allgather(user, send, recv, count, stream): every rank passes `count` doubles at send
+ * (device memory); when the work the call enqueues on `stream` completes, recv (device
+ * memory, world * count doubles) holds rank r's values at recv[r * count].  It may enqueue
+ * the exchange (an NCCL all-gather on `stream`) or complete it before returning; it
+ * returns 0 on success.  Every rank makes the same calls in the same order.
+ *
+ * funcgrad evaluates this rank's part: it receives the local x (n_local values), writes
+ * the local g, and returns in *f this rank's share of f (the solver adds the shares of the
+ * ranks in rank order; a rank may return the whole f and the others 0).  after_iteration and
+ * customized_stopping receive the local x and g and the whole f.  ext->trace reports the
+ * whole problem's counts (the free-set hash over global indices).  If one rank fails, the
+ * others wait in their next allgather: the allgather should carry a timeout. */
+typedef int (*lbfgsb_b200_allgather_fn)(void* user, const double* send, double* recv, int count,
+                                        void* stream);
+typedef struct {
+  int rank;
+  int world;
+  int n_global;   /* variables of the whole problem */
+  int offset;     /* global index of this rank's first variable */
+  lbfgsb_b200_allgather_fn allgather;
+  void* allgather_user;
+} lbfgsb_b200_shard;
+
+int lbfgsb_b200_minimize_sharded_f64(const lbfgsb_b200_shard* shard, int n_local, double* x,
+                                     const int* nbd, const double* l, const double* u,
+                                     const lbfgsb_b200_option_f64* option,
+                                     lbfgsb_b200_callback_f64 funcgrad,
+                                     lbfgsb_b200_callback_f64 after_iteration,
+                                     lbfgsb_b200_callback_f64 customized_stopping, void* user,
+                                     void* stream, const lbfgsb_b200_ext* ext,
+                                     lbfgsb_b200_summary_f64* summary);
+int lbfgsb_b200_minimize_sharded_f32(const lbfgsb_b200_shard* shard, int n_local, float* x,
+                                     const int* nbd, const float* l, const float* u,
+                                     const lbfgsb_b200_option_f32* option,
+                                     lbfgsb_b200_callback_f32 funcgrad,
+                                     lbfgsb_b200_callback_f32 after_iteration,
+                                     lbfgsb_b200_callback_f32 customized_stopping, void* user,
+                                     void* stream, const lbfgsb_b200_ext* ext,
+                                     lbfgsb_b200_summary_f32* summary);
+
 /* ---- device-driven solves (no counterpart in the reference) ------------------------
  * The reference's funcgrad returns f on the host, so every evaluation costs the solver a
  * device-to-host synchronisation and the host must steer each step.  An objective that

@@ -21,7 +21,7 @@ SOURCES = [os.path.join(HERE, "csrc", f) for f in
            ("driver.cu", "batch.cu", "objective.cu", "dsscfg.cu", "noalloc.cu")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in
            ("common.cuh", "small.cuh", "state.cuh", "reduce.cuh", "tiles.cuh", "warp_small.cuh",
-            "passes.cuh", "walk.cuh", "rounds.cuh", "host.cuh", "batch_tune.h")]
+            "passes.cuh", "walk.cuh", "rounds.cuh", "host.cuh", "batch_tune.h", "shard.cuh")]
 HEADERS.append(os.path.join(REPO, "include", "lbfgsb_b200.h"))
 
 NVCC_FLAGS = [

@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <deque>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -23,11 +24,28 @@
 
 #include "../../include/lbfgsb_b200.h"
 #include "host.cuh"
+#include "shard.cuh"
 
 namespace lbfgsb_b200 {
 
 thread_local std::string g_last_error;
 thread_local lbfgsb_b200_stats g_last_stats;
+
+// A sharded solve's all-gather returned an error code.
+struct ShardFailure {
+  int rc;
+};
+
+// Page-locked host doubles for a sharded solve's small exchanges.
+struct PinnedDoubles {
+  double* p = nullptr;
+  explicit PinnedDoubles(size_t n) { CK(cudaMallocHost(&p, n * sizeof(double))); }
+  ~PinnedDoubles() {
+    if (p) cudaFreeHost(p);
+  }
+  PinnedDoubles(const PinnedDoubles&) = delete;
+  PinnedDoubles& operator=(const PinnedDoubles&) = delete;
+};
 
 constexpr int kMaxDevices = 64;
 static std::mutex g_pool_mu;
@@ -58,7 +76,7 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
                  const typename Api<R>::Opt* opt, typename Api<R>::Cb funcgrad,
                  typename Api<R>::Cb after_iter, typename Api<R>::Cb custom_stop, void* user,
                  cudaStream_t stream, const lbfgsb_b200_ext* ext,
-                 typename Api<R>::Sum* summary) {
+                 typename Api<R>::Sum* summary, const lbfgsb_b200_shard* sh = nullptr) {
   using Sum = typename Api<R>::Sum;
   g_last_error.clear();
   std::memset(&g_last_stats, 0, sizeof(g_last_stats));
@@ -68,8 +86,14 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
     return LBFGSB_B200_ERR_ARGUMENT;
   }
   const int m = std::min(opt->hessian_approximate_dimension, kMaxM);
+  // a sharded solve: this rank's n variables start at global index sh->offset
+  if (sh && (sh->world < 1 || sh->rank < 0 || sh->rank >= sh->world || !sh->allgather ||
+             sh->offset < 0 || n <= 0 || (long long)sh->offset + n > (long long)sh->n_global ||
+             sh->world * kShardRow > (1 << 30)))
+    return LBFGSB_B200_ERR_ARGUMENT;
+  const int n_all = sh ? sh->n_global : n;
   // errclb's scalar checks and the driver's option checks (lbfgsbcpu.cpp:258-264, 879-890)
-  if (n <= 0 || m <= 0 || m > n || opt->eps_f < 0 || opt->max_iteration < 0 ||
+  if (n <= 0 || m <= 0 || m > n_all || opt->eps_f < 0 || opt->max_iteration < 0 ||
       opt->eps_g < 0 || opt->eps_x < 0) {
     summary->info = -1;
     return LBFGSB_B200_OK;
@@ -101,6 +125,24 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
     const int g_proj = p.g_proj, g_elem = p.g_elem;
     const int g_walk = walk_coop_grid<R, H, S>();
     DevState<S>& hs = *w.hs;
+    // sharded: the buffers of the rank rows (shard.cuh, reduce.cuh) and of the walk records
+    const int world = sh ? sh->world : 1;
+    const int walk_chunk = kWalkChunk / world;
+    std::unique_ptr<PinnedDoubles> pin;
+    double *f_send = nullptr, *f_recv = nullptr, *rows_recv = nullptr;
+    double *walk_send = nullptr, *walk_recv = nullptr;
+    ShardWalk<S>* swk = nullptr;
+    if (sh) {
+      hs.n = sh->n_global;
+      c.shard_world = world;
+      c.ioff = sh->offset;
+      c.shard_send = w.template alloc<double>(kShardRow);
+      rows_recv = w.template alloc<double>((size_t)world * kShardRow);
+      c.shard_recv = rows_recv;
+      f_send = w.template alloc<double>(2);
+      f_recv = w.template alloc<double>((size_t)world * 2);
+      pin.reset(new PinnedDoubles((size_t)world * 2 + 4));
+    }
     CK(cudaMemcpyAsync(w.st, &hs, sizeof(hs), cudaMemcpyHostToDevice, stream));
     const size_t header = offsetof(DevState<S>, big);
     auto pull = [&]() {
@@ -109,6 +151,58 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
       syncs++;
       if (w.hs->device_error) throw CudaFailure{cudaErrorLaunchTimeout, "staged-tile wait", __LINE__};
     };
+    auto exchange = [&](const double* send, double* recv, int count) {
+      const int rc = sh->allgather(sh->allgather_user, send, recv, count, (void*)stream);
+      if (rc != 0) throw ShardFailure{rc};
+    };
+    // two values of every rank (host side, in rank order) into pin->p[2 + 2r .. 3 + 2r]
+    auto gather2 = [&](double a, double b) {
+      pin->p[0] = a;
+      pin->p[1] = b;
+      CK(cudaMemcpyAsync(f_send, pin->p, 2 * sizeof(double), cudaMemcpyHostToDevice, stream));
+      exchange(f_send, f_recv, 2);
+      CK(cudaMemcpyAsync(pin->p + 2, f_recv, (size_t)world * 2 * sizeof(double),
+                         cudaMemcpyDeviceToHost, stream));
+      CK(cudaStreamSynchronize(stream));
+      syncs++;
+    };
+    // the function value of a sharded solve: the ranks' shares added in rank order
+    auto total_f = [&](R part) -> R {
+      if (!sh) return part;
+      gather2((double)part, 0.0);
+      double a = 0.0;
+      for (int r = 0; r < world; r++) a += pin->p[2 + 2 * r];
+      return (R)a;
+    };
+    // a pass: the streaming launch, and for a sharded solve the exchange of the rank rows
+    // and the one-CTA launch that folds them and runs the epilogue
+    auto run_pass = [&](int kid, int grid, auto launch) {
+      L.run(kid, [&] {
+        launch(c, grid);
+        if (sh) {
+          exchange(c.shard_send, rows_recv, kShardRow);
+          Ctx<R, H, S> e = c;
+          e.epi_only = 1;
+          launch(e, 1);
+        }
+      });
+    };
+    if (sh) {
+      // the ranks' index ranges must tile 0 .. n_global in rank order
+      gather2((double)n, (double)sh->offset);
+      long long next = 0;
+      bool tiled = true;
+      for (int r = 0; r < world; r++) {
+        const long long nr = (long long)pin->p[2 + 2 * r], orr = (long long)pin->p[3 + 2 * r];
+        if (nr < 1 || orr != next) tiled = false;
+        next += nr;
+      }
+      if (!tiled || next != sh->n_global) {
+        summary->info = -1;
+        CK(cudaStreamSynchronize(stream));
+        return LBFGSB_B200_ERR_ARGUMENT;
+      }
+    }
 
     R* xcur = w.X[0];
     R* zb = w.X[1];
@@ -126,6 +220,11 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
     L.run(KID_INIT, [&] {
       k_init<R, S><<<g_elem, 256, 0, stream>>>(n, x_user, xcur, nbd, l, u, w.st);
     });
+    if (sh) {
+      k_shard_flags_put<S><<<1, 32, 0, stream>>>(w.st, c.shard_send);
+      exchange(c.shard_send, rows_recv, kShardRow);
+      k_shard_flags_get<S><<<1, 32, 0, stream>>>(w.st, rows_recv, world);
+    }
     pull();
     if (hs.input_error) {
       summary->info = -1;  // x is left as given (lbfgsbcpu.cpp:259-264)
@@ -137,8 +236,9 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
       R f = 0;
       funcgrad(user, xcur, &f, gcur, (void*)stream, summary);
       evals++;
-      L.run(KID_PROJGR, [&] {
-        k_projgr<R, H, S><<<g_proj, kThreads, 0, stream>>>(c, xcur, gcur, (S)f);
+      f = total_f(f);
+      run_pass(KID_PROJGR, g_proj, [&](const Ctx<R, H, S>& cc, int grid) {
+        k_projgr<R, H, S><<<grid, kThreads, 0, stream>>>(cc, xcur, gcur, (S)f);
       });
       pull();
       summary->residual_g = (R)hs.sbgnrm;
@@ -160,29 +260,29 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
         const int col_now = reset_before ? 0 : hs.col;
         const bool uncon = !cnstnd && col_now > 0;
         auto subspace = [&]() {
-          L.run(KID_FREEV, [&] {
-            c.stages = p_freev.stages;
-            k_freev_formk<R, H, S, kConsWide><<<p_freev.grid, p_freev.threads, p_freev.smem, stream>>>(c, xcur, gcur);
+          c.stages = p_freev.stages;
+          run_pass(KID_FREEV, p_freev.grid, [&](const Ctx<R, H, S>& cc, int grid) {
+            k_freev_formk<R, H, S, kConsWide><<<grid, p_freev.threads, p_freev.smem, stream>>>(cc, xcur, gcur);
           });
-          L.run(KID_SUBDIR, [&] {
-            c.stages = p_dir.stages;
-            k_subsm_dir<R, H, S, kConsWide><<<p_dir.grid, p_dir.threads, p_dir.smem, stream>>>(c, xcur, gcur, zb);
+          c.stages = p_dir.stages;
+          run_pass(KID_SUBDIR, p_dir.grid, [&](const Ctx<R, H, S>& cc, int grid) {
+            k_subsm_dir<R, H, S, kConsWide><<<grid, p_dir.threads, p_dir.smem, stream>>>(cc, xcur, gcur, zb);
           });
           // the direction pass applies an untruncated step itself (spec_apply); the apply
           // pass runs only when it has work, which the host learns from the state
           pull();
           if (!(hs.gcp_state == GCP_WALK || hs.internal_fail != 0 || hs.spec_apply)) {
-            L.run(KID_SUBAPPLY, [&] {
-              c.stages = p_apply.stages;
-              k_subsm_apply<R, H, S, kConsWide><<<p_apply.grid, p_apply.threads, p_apply.smem, stream>>>(c, xcur, gcur, zb);
+            c.stages = p_apply.stages;
+            run_pass(KID_SUBAPPLY, p_apply.grid, [&](const Ctx<R, H, S>& cc, int grid) {
+              k_subsm_apply<R, H, S, kConsWide><<<grid, p_apply.threads, p_apply.smem, stream>>>(cc, xcur, gcur, zb);
             });
             pull();
           }
         };
         if (!uncon && start_here) {
-          L.run(KID_GCP, [&] {
-            c.stages = p_gcp.stages;
-            k_gcp_scan<R, H, S, kConsWide><<<p_gcp.grid, p_gcp.threads, p_gcp.smem, stream>>>(c, xcur, gcur);
+          c.stages = p_gcp.stages;
+          run_pass(KID_GCP, p_gcp.grid, [&](const Ctx<R, H, S>& cc, int grid) {
+            k_gcp_scan<R, H, S, kConsWide><<<grid, p_gcp.threads, p_gcp.smem, stream>>>(cc, xcur, gcur);
           });
         }
         auto count_dir = [&]() {
@@ -197,7 +297,36 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
           if (!c.wl_t) walk_buffers(w, c, N);
           CK(cudaMemsetAsync(w.wl_n, 0, sizeof(unsigned int), stream));
           CK(cudaMemsetAsync(&c.wsc->bar, 0, sizeof(unsigned int), stream));
-          L.run(KID_WALK, [&] { launch_walk_coop<R, H, S>(c, xcur, gcur, g_walk, stream); });
+          if (!sh) {
+            L.run(KID_WALK, [&] { launch_walk_coop<R, H, S>(c, xcur, gcur, g_walk, stream); });
+          } else {
+            // the walk over every rank's breakpoints (shard.cuh): select, gather, walk up to
+            // the frontier, until the walk ends; then each rank marks what it owns
+            if (!swk) {
+              swk = w.template alloc<ShardWalk<S>>(1);
+              walk_send = w.template alloc<double>(shard_walk_block(walk_chunk));
+              walk_recv = w.template alloc<double>((size_t)world * shard_walk_block(walk_chunk));
+            }
+            L.run(KID_WALK, [&] {
+              k_walk_gather<R, H, S><<<g_elem, kThreads, 0, stream>>>(c, xcur, gcur);
+              CK(cudaMemsetAsync(swk, 0, sizeof(ShardWalk<S>), stream));
+              int* h_done = reinterpret_cast<int*>(pin->p);
+              while (true) {
+                k_shard_walk_select<R, H, S><<<1, kWalkThreads, 0, stream>>>(c, xcur, gcur, swk,
+                                                                             walk_chunk, walk_send);
+                exchange(walk_send, walk_recv, shard_walk_block(walk_chunk));
+                k_shard_walk_merge<R, H, S><<<1, kWalkThreads, 0, stream>>>(c, walk_recv, world,
+                                                                            walk_chunk, swk);
+                CK(cudaMemcpyAsync(h_done, reinterpret_cast<char*>(swk) + offsetof(ShardWalk<S>, done),
+                                   sizeof(int), cudaMemcpyDeviceToHost, stream));
+                CK(cudaStreamSynchronize(stream));
+                syncs++;
+                if (*h_done) break;
+              }
+              k_shard_walk_end<S><<<1, 32, 0, stream>>>(w.st, swk);
+              k_shard_walk_mark<R, H, S><<<g_elem, 256, 0, stream>>>(c, gcur, swk);
+            });
+          }
           subspace();
           count_dir();
         }
@@ -221,16 +350,16 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
         }
         auto post = [&](R* xt_, R fval, int force) {
           if (fused) {
-            L.run(KID_POSTGCP, [&] {
-              c.stages = p_pgcp.stages;
-              k_post_gcp<R, H, S, kConsWide><<<p_pgcp.grid, p_pgcp.threads, p_pgcp.smem, stream>>>(
-                  c, xcur, zb, xt_, gnew, gcur, (S)fval, force);
+            c.stages = p_pgcp.stages;
+            run_pass(KID_POSTGCP, p_pgcp.grid, [&](const Ctx<R, H, S>& cc, int grid) {
+              k_post_gcp<R, H, S, kConsWide><<<grid, p_pgcp.threads, p_pgcp.smem, stream>>>(
+                  cc, xcur, zb, xt_, gnew, gcur, (S)fval, force);
             });
           } else {
-            L.run(KID_POST, [&] {
-              c.stages = p_post.stages;
-              k_post_eval<R, H, S, kConsWide><<<p_post.grid, p_post.threads, p_post.smem, stream>>>(
-                  c, xcur, zb, xt_, gnew, gcur, (S)fval, force);
+            c.stages = p_post.stages;
+            run_pass(KID_POST, p_post.grid, [&](const Ctx<R, H, S>& cc, int grid) {
+              k_post_eval<R, H, S, kConsWide><<<grid, p_post.threads, p_post.smem, stream>>>(
+                  cc, xcur, zb, xt_, gnew, gcur, (S)fval, force);
             });
           }
         };
@@ -248,6 +377,7 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
           }
           funcgrad(user, xt, &f, gnew, (void*)stream, summary);
           evals++;
+          f = total_f(f);
           post(xt, f, 0);
           pull();
           if (hs.ls_task != 1) break;
@@ -388,6 +518,9 @@ static int solve(int n, R* x_user, const int* nbd, const R* l, const R* u,
                   cudaGetErrorString(e.err));
     g_last_error = buf;
     return LBFGSB_B200_ERR_CUDA;
+  } catch (const ShardFailure& e) {
+    g_last_error = "the sharded solve's allgather returned " + std::to_string(e.rc);
+    return LBFGSB_B200_ERR_CALLBACK;
   }
   return LBFGSB_B200_OK;
 }
@@ -773,6 +906,42 @@ int lbfgsb_b200_minimize_ext_f32(int n, float* x, const int* nbd, const float* l
                                                ext, summary);
   return solve<float, float, float>(n, x, nbd, l, u, option, funcgrad, after_iteration,
                                     customized_stopping, user, s, ext, summary);
+}
+
+int lbfgsb_b200_minimize_sharded_f64(const lbfgsb_b200_shard* shard, int n_local, double* x,
+                                     const int* nbd, const double* l, const double* u,
+                                     const lbfgsb_b200_option_f64* option,
+                                     lbfgsb_b200_callback_f64 funcgrad,
+                                     lbfgsb_b200_callback_f64 after_iteration,
+                                     lbfgsb_b200_callback_f64 customized_stopping, void* user,
+                                     void* stream, const lbfgsb_b200_ext* ext,
+                                     lbfgsb_b200_summary_f64* summary) {
+  if (!shard) return LBFGSB_B200_ERR_ARGUMENT;
+  return solve<double, double, double>(n_local, x, nbd, l, u, option, funcgrad, after_iteration,
+                                       customized_stopping, user, (cudaStream_t)stream, ext,
+                                       summary, shard);
+}
+
+int lbfgsb_b200_minimize_sharded_f32(const lbfgsb_b200_shard* shard, int n_local, float* x,
+                                     const int* nbd, const float* l, const float* u,
+                                     const lbfgsb_b200_option_f32* option,
+                                     lbfgsb_b200_callback_f32 funcgrad,
+                                     lbfgsb_b200_callback_f32 after_iteration,
+                                     lbfgsb_b200_callback_f32 customized_stopping, void* user,
+                                     void* stream, const lbfgsb_b200_ext* ext,
+                                     lbfgsb_b200_summary_f32* summary) {
+  if (!shard) return LBFGSB_B200_ERR_ARGUMENT;
+  const int form = ext ? ext->form : LBFGSB_B200_FORM_PLAIN;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (form == LBFGSB_B200_FORM_MIXED)
+    return solve<float, float, double>(n_local, x, nbd, l, u, option, funcgrad, after_iteration,
+                                       customized_stopping, user, s, ext, summary, shard);
+  if (form == LBFGSB_B200_FORM_MIXED_BF16)
+    return solve<float, __nv_bfloat16, double>(n_local, x, nbd, l, u, option, funcgrad,
+                                               after_iteration, customized_stopping, user, s,
+                                               ext, summary, shard);
+  return solve<float, float, float>(n_local, x, nbd, l, u, option, funcgrad, after_iteration,
+                                    customized_stopping, user, s, ext, summary, shard);
 }
 
 int lbfgsb_b200_minimize_device_f64(int n, double* x, const int* nbd, const double* l,

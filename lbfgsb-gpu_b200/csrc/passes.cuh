@@ -25,6 +25,8 @@
 // contracted); reductions accumulate in double with explicit fma().
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "reduce.cuh"
 #include "small.cuh"
@@ -84,6 +86,14 @@ struct Ctx {
   R** ev_g;
   double* ev_f;
   int* ev_act;
+  // sharded solves (reduce.cuh): this rank's variables are global indices ioff .. ioff + n;
+  // shard_send / shard_recv hold the rank rows of a pass's reduction (null and 0 otherwise),
+  // epi_only = 1 in the one-CTA launch that folds the gathered rows and runs the epilogue
+  int shard_world = 0;
+  int ioff = 0;
+  int epi_only = 0;
+  double* shard_send = nullptr;
+  const double* shard_recv = nullptr;
 };
 
 // Physical slot pointers of ring positions 1..kMaxM counted from head.
@@ -357,7 +367,7 @@ __device__ __forceinline__ void gcp_scan_pass(const Ctx<R, H, S>& c, CtaPos cp, 
     x = c.X[st->xr[0]];
     g = c.G[st->gr[0]];
   }
-  const int n = c.n, col = st->col;
+  const int n = c.epi_only ? 0 : c.n, col = st->col;
   // sums: [0] sum neggi^2, [1..16] p (y part 1..8, s part 9..16), [17] nbreak,
   // [18] movable variables without breakpoint; max: [0] any such with g != 0;
   // min pair: smallest breakpoint
@@ -413,7 +423,7 @@ __device__ __forceinline__ void gcp_scan_pass(const Ctx<R, H, S>& c, CtaPos cp, 
         if (has_bp) {
           s[17] += A(1);
           // the smallest breakpoint: only candidates that can reach it are divided exactly
-          bp.offer_quotient(tnum, tden, i);
+          bp.offer_quotient(tnum, tden, i + c.ioff);
         } else {
           s[18] += A(1);
           if (neggi != A(0)) xm[0] = 1.0;
@@ -425,10 +435,9 @@ __device__ __forceinline__ void gcp_scan_pass(const Ctx<R, H, S>& c, CtaPos cp, 
   double lo[1] = {0.0}, sd[NS];
   MinPair mn[NM] = {bp.pair()};
   sums_to_double(s, sd);
-  cta_reduce_to_row<CONS + 32, NS, NX, NM, 0>(sd, xm, mn, lo, c.part, W, cp.rank, cp.count);
-  if (!last_cta(c.ticket, cp.count)) return;
+  if (!c.epi_only) cta_reduce_to_row<CONS + 32, NS, NX, NM, 0>(sd, xm, mn, lo, c.part, W, cp.rank, cp.count);
   __shared__ double red[W];
-  fold_rows<CONS + 32>(c.part, cp.count, W, NS, NX, NM, red);
+  if (!pass_fold<CONS + 32>(c, cp, W, NS, NX, NM, red)) return;
   __shared__ SmallWork<S> sw;
   epilogue_on_shared_warp<S>(st, [&](DevState<S>* st, int lane) {
     gcp_epilogue<S>(st, red, col, sw, lane);
@@ -476,7 +485,7 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
     g = c.G[st->gr[0]];
   }
   if (st->gcp_state == GCP_WALK || st->internal_fail != 0) return;
-  const int n = c.n, col = st->col, iter = st->iter;
+  const int n = c.epi_only ? 0 : c.n, col = st->col, iter = st->iter;
   const bool uncon = st->uncon_branch != 0;
   const bool track = !uncon && iter > 0 && st->cnstnd;
   const bool updatd = st->updatd != 0;
@@ -579,7 +588,7 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
       if (ok) {
         if (fnow) {
           cnt[0]++;
-          if (c.hash_free) hash += mix64((unsigned long long)i);
+          if (c.hash_free) hash += mix64((unsigned long long)(i + c.ioff));
           const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
           const R zi = uncon ? xi : gcp_point<R, S>(code, xi, gi, R(0), R(0), tsum);
           // cmprlb's r (842-867).  Here it only feeds the W'r reductions (the subspace
@@ -642,27 +651,40 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
     // kOneRole: all of element e's work.  Its 2*col history values are read from the stage
     // once, into registers; the sums are those of roles 0, 1 and 2 below, with the same
     // operands in each fma.
-    auto one_role = [&](const unsigned char* buf, long long t, int valid, int e) {
+    // fast: the steady state of a bounded problem (every column live, the free set tracked,
+    // a new pair to multiply, no hash), compiled with those flags as constants
+    // Every input of the element is read into registers first and the stage released, so
+    // that the producer refills it while the sums are formed.
+    auto one_role = [&](const unsigned char* buf, long long t, int valid, int e, auto fast,
+                        auto release) {
+      constexpr bool F = decltype(fast)::value;
+      const bool uncon_ = F ? false : uncon;
+      const bool track_ = F ? true : track;
+      const bool need_row_ = F ? true : need_row;
+      const bool hash_ = F ? false : c.hash_free != 0;
       const int i = (int)(t * kTile) + e;
       const bool ok = e < valid;
       int code = IW_LOW;
       if (ok) code = stage_at<int8_t>(buf, o_code, e);
-      const bool fnow = ok && (uncon || iw_free(code));
       const int wi = e >> 5;
       const uint32_t word = stage_at<uint32_t>(buf, o_bits, wi);
-      const bool fprev = (word >> lane) & 1u;
-      const bool enter = track && ok && !fprev && fnow;
-      const bool leave = track && ok && fprev && !fnow;
-      const uint32_t newword = __ballot_sync(0xffffffffu, fnow);
-      if (!uncon && lane == 0 && wi * 32 < valid) c.fbits[t * (kTile / 32) + wi] = newword;
-      if (ok) {
-        A yv[kMaxM], sv[kMaxM];
+      // past the tile's end the values are stale stage bytes, never used
+      const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
+      A yv[kMaxM], sv[kMaxM];
   #pragma unroll
-        for (int j = 0; j < kMaxM; j++) {
-          const bool live = kFull || j < col;
-          yv[j] = live ? hist_at<H, A>(buf, hy + j * hb, e) : A(0);
-          sv[j] = live ? hist_at<H, A>(buf, hs + j * hb, e) : A(0);
-        }
+      for (int j = 0; j < kMaxM; j++) {
+        const bool live = kFull || j < col;
+        yv[j] = live ? hist_at<H, A>(buf, hy + j * hb, e) : A(0);
+        sv[j] = live ? hist_at<H, A>(buf, hs + j * hb, e) : A(0);
+      }
+      release();
+      const bool fnow = ok && (uncon_ || iw_free(code));
+      const bool fprev = (word >> lane) & 1u;
+      const bool enter = track_ && ok && !fprev && fnow;
+      const bool leave = track_ && ok && fprev && !fnow;
+      const uint32_t newword = __ballot_sync(0xffffffffu, fnow);
+      if (!uncon_ && lane == 0 && wi * 32 < valid) c.fbits[t * (kTile / 32) + wi] = newword;
+      if (ok) {
         // the newest column, selected without a runtime register index
         const int nw = kFull ? kMaxM - 1 : newest;
         A ynew = A(0), snew = A(0);
@@ -674,11 +696,10 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
           }
         if (fnow) {
           cnt[0]++;
-          if (c.hash_free) hash += mix64((unsigned long long)i);
-          const R xi = stage_at<R>(buf, o_x, e), gi = stage_at<R>(buf, o_g, e);
-          const R zi = uncon ? xi : gcp_point<R, S>(code, xi, gi, R(0), R(0), tsum);
+          if (hash_) hash += mix64((unsigned long long)(i + c.ioff));
+          const R zi = uncon_ ? xi : gcp_point<R, S>(code, xi, gi, R(0), R(0), tsum);
           S r = -(S)gi;
-          if (!uncon) {
+          if (!uncon_) {
             S ry = -a1[kMaxM] * ((S)zi - (S)xi) - (S)gi, rs = S(0);
   #pragma unroll
             for (int j = 0; j < kMaxM; j++)
@@ -695,7 +716,7 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
               acc[8 + j] = fma(sv[j], (A)r, acc[8 + j]);
             }
           }
-          if (need_row) {
+          if (need_row_) {
   #pragma unroll
             for (int j = 0; j < kMaxM; j++) {
               if (kFull || j < col) {
@@ -707,7 +728,7 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
         } else {
           if (code == IW_LOW || code == IW_WALK_LOW) cnt[3]++;
           if (code == IW_UPP || code == IW_WALK_UPP) cnt[4]++;
-          if (need_row) {
+          if (need_row_) {
             // columns past col hold zeros and add nothing
   #pragma unroll
             for (int q = 0; q < 4; q++) {
@@ -731,11 +752,16 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
         const int src = __ffs(pick) - 1;
         pick &= pick - 1;
         const double sign = __shfl_sync(0xffffffffu, enter ? 1.0 : -1.0, src);
-        const int es = e - lane + src;
-        if (lane < kMaxM)
-          bc[warp][lane] = lane < col ? hist_at<H>(buf, hy + lane * hb, es) : 0.0;
-        else if (lane < 2 * kMaxM)
-          bc[warp][lane] = lane - kMaxM < col ? hist_at<H>(buf, hs + (lane - kMaxM) * hb, es) : 0.0;
+        // the source variable's rows, from its lane's registers (columns past col are 0)
+  #pragma unroll
+        for (int j = 0; j < kMaxM; j++) {
+          const A vy = __shfl_sync(0xffffffffu, yv[j], src);
+          const A vs = __shfl_sync(0xffffffffu, sv[j], src);
+          if (lane == 0) {
+            bc[warp][j] = (double)vy;
+            bc[warp][kMaxM + j] = (double)vs;
+          }
+        }
         __syncwarp();
   #pragma unroll
         for (int k = 0; k < kLaneOwned; k++) {
@@ -768,11 +794,13 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
         }
       }
     };
+    auto stream_tiles = [&](auto fast) {
     run_stages<CONS>(ss, n, stages, dyn, reinterpret_cast<uint64_t*>(dyn + (size_t)stages * cap),
                      &st->device_error, cp, [&](const unsigned char* buf, long long t, int valid,
                                             auto release) {
       if constexpr (kOneRole) {
-        one_role(buf, t, valid, (int)threadIdx.x);
+        one_role(buf, t, valid, (int)threadIdx.x, fast, release);
+        return;
       } else if (role == 0) {
   #pragma unroll
         for (int h = 0; h < kTile / (32 * kRole0Warps); h++)
@@ -784,6 +812,15 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
       }
       release();
     });
+    };
+    if constexpr (kOneRole) {
+      if (kFull && !uncon && track && need_row && !c.hash_free)
+        stream_tiles(std::true_type{});
+      else
+        stream_tiles(std::false_type{});
+    } else {
+      stream_tiles(std::false_type{});
+    }
   });
   // the free-set hash sums mod 2^64 (order free), one atomic per warp
 #pragma unroll
@@ -795,7 +832,7 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
   constexpr int NS = NA + NB + NC;
   constexpr int W = NS + 32 * kLaneOwned;
   constexpr int kAllWarps = CONS / 32 + 1;
-  {
+  if (!c.epi_only) {
     __shared__ double wsum[kAllWarps][NS];
     for (int k = lane; k < NS; k += 32) wsum[warp][k] = 0.0;
     __syncwarp();
@@ -840,9 +877,8 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
       row[(size_t)k * cp.count] = a;
     }
   }
-  if (!last_cta(c.ticket, cp.count)) return;
   __shared__ double red[W];
-  fold_rows<CONS + 32>(c.part, cp.count, W, W, 0, 0, red);
+  if (!pass_fold<CONS + 32>(c, cp, W, W, 0, 0, red, &st->free_hash_acc)) return;
   __shared__ SmallWork<S> sw;
   __shared__ S wn1_snap[4 * kMaxM * kMaxM];
   epilogue_on_shared_warp<S>(st, [&](DevState<S>* st, int lane) {
@@ -1012,7 +1048,7 @@ __device__ __forceinline__ void subsm_dir_pass(const Ctx<R, H, S>& c, CtaPos cp,
     z = c.X[st->xr[1]];
   }
   if (st->gcp_state == GCP_WALK || st->internal_fail != 0 || !st->subsm_active) return;
-  const int n = c.n, col = st->col;
+  const int n = c.epi_only ? 0 : c.n, col = st->col;
   const bool uncon = st->uncon_branch != 0;
   const S theta = st->theta, tsum = st->tsum;
   __shared__ __align__(16) S a1[kMaxM + 1], a2[kMaxM], w1[kMaxM], w2[kMaxM];  // uniform
@@ -1090,7 +1126,7 @@ __device__ __forceinline__ void subsm_dir_pass(const Ctx<R, H, S>& c, CtaPos cp,
         // an active variable: z is its Cauchy point
         const R zi = gcp_point<R, S>(code, v.x, v.g, v.l, v.u, tsum);
         z[i] = zi;
-        lnsrlb_elem<R, A>(zi, v.x, v.g, v.l, v.u, v.nb, want_stpmx, i, sl[0], sl[1], ms);
+        lnsrlb_elem<R, A>(zi, v.x, v.g, v.l, v.u, v.nb, want_stpmx, i + c.ioff, sl[0], sl[1], ms);
         return;
       }
       const S(&yv)[kMaxM] = v.yv;
@@ -1159,9 +1195,9 @@ __device__ __forceinline__ void subsm_dir_pass(const Ctx<R, H, S>& c, CtaPos cp,
         const bool reach = lo ? dk1 < temp2 : dk1 > temp2;
         if (lo || hi) {
           if (at)
-            mb.offer(S(0), i);
+            mb.offer(S(0), i + c.ioff);
           else if (reach && !quotient_exceeds(temp2, dk, mb.thr))
-            mb.offer(temp2 / dk, i);
+            mb.offer(temp2 / dk, i + c.ioff);
         }
       }
       // the subspace step with alpha = 1 (1517-1533): z = xcp + d; with the 3.0 step,
@@ -1175,7 +1211,7 @@ __device__ __forceinline__ void subsm_dir_pass(const Ctx<R, H, S>& c, CtaPos cp,
           if ((lo && zs == li) || (hi && zs == ui)) s_projected = 1;
         }
         z[i] = zs;
-        lnsrlb_elem<R, A>(zs, xi, gi, li, ui, nb, want_stpmx, i, sl[0], sl[1], ms);
+        lnsrlb_elem<R, A>(zs, xi, gi, li, ui, nb, want_stpmx, i + c.ioff, sl[0], sl[1], ms);
       }
     });
   });
@@ -1186,11 +1222,10 @@ __device__ __forceinline__ void subsm_dir_pass(const Ctx<R, H, S>& c, CtaPos cp,
   double xm[1] = {s_projected ? 1.0 : 0.0}, ldum[1] = {0.0}, sld[2];
   MinPair mn[2] = {mb.pair(), ms.pair()};
   sums_to_double(sl, sld);
-  cta_reduce_to_row<CONS + 32, 2, 1, 2, 0>(sld, xm, mn, ldum, c.part, W, cp.rank, cp.count);
-  if (!last_cta(c.ticket, cp.count)) return;
+  if (!c.epi_only) cta_reduce_to_row<CONS + 32, 2, 1, 2, 0>(sld, xm, mn, ldum, c.part, W, cp.rank, cp.count);
   __shared__ double red[W];
   __shared__ double rl[3];
-  fold_rows<CONS + 32>(c.part, cp.count, W, 2, 1, 2, red);
+  if (!pass_fold<CONS + 32>(c, cp, W, 2, 1, 2, red)) return;
   epilogue_on_shared<S>(st, [&](DevState<S>* st) {
     // the 3.0 step keeps the projected point when it gives a descent direction from x
     // (g'd <= 0 over the written z); otherwise, and always with the 2.1 step, the step is
@@ -1238,7 +1273,7 @@ __device__ __forceinline__ void subsm_apply_pass(const Ctx<R, H, S>& c, CtaPos c
     z = c.X[st->xr[1]];
   }
   if (st->gcp_state == GCP_WALK || st->internal_fail != 0 || st->spec_apply) return;
-  const int n = c.n;
+  const int n = c.epi_only ? 0 : c.n;
   const bool uncon = st->uncon_branch != 0;
   const bool sub = st->subsm_active != 0;
   const S alpha = sub ? st->alpha : S(1), tsum = st->tsum;
@@ -1275,7 +1310,7 @@ __device__ __forceinline__ void subsm_apply_pass(const Ctx<R, H, S>& c, CtaPos c
     R zi = uncon ? xi : gcp_point<R, S>(code, xi, gi, li, ui, tsum);
     if (sub && (uncon || iw_free(code))) {
       S dk = (S)stage_at<R>(buf, o_ds, e);
-      if (i == ibd) {
+      if (i + c.ioff == ibd) {
         if (dk > S(0)) {
           zi = ui;
           dk = 0;
@@ -1288,16 +1323,15 @@ __device__ __forceinline__ void subsm_apply_pass(const Ctx<R, H, S>& c, CtaPos c
     }
     z[i] = zi;
     lnsrlb_elem<R, A>(zi, xi, gi, li, ui, want_stpmx ? stage_at<int>(buf, o_nb, e) : 0, want_stpmx,
-                      i, s[0], s[1], ms);
+                      i + c.ioff, s[0], s[1], ms);
   });
   constexpr int W = 4;
   double xdum[1] = {0.0}, ldum[1] = {0.0}, sd[2];
   MinPair mn[1] = {ms.pair()};
   sums_to_double(s, sd);
-  cta_reduce_to_row<CONS + 32, 2, 0, 1, 0>(sd, xdum, mn, ldum, c.part, W, cp.rank, cp.count);
-  if (!last_cta(c.ticket, cp.count)) return;
+  if (!c.epi_only) cta_reduce_to_row<CONS + 32, 2, 0, 1, 0>(sd, xdum, mn, ldum, c.part, W, cp.rank, cp.count);
   __shared__ double red[W];
-  fold_rows<CONS + 32>(c.part, cp.count, W, 2, 0, 1, red);
+  if (!pass_fold<CONS + 32>(c, cp, W, 2, 0, 1, red)) return;
   epilogue_on_shared<S>(st, [&](DevState<S>* st) {
 
     lnsrlb_start<S>(st, red);
@@ -1457,7 +1491,7 @@ __device__ __forceinline__ void post_eval_pass(const Ctx<R, H, S>& c, CtaPos cp,
     force_accept = st->ev_force;
     f = st->ev_force ? st->f : (S)(R)*c.ev_f;
   }
-  const int n = c.n, col = st->col;
+  const int n = c.epi_only ? 0 : c.n, col = st->col;
   const R stp = (R)st->stp;
   const bool unit = st->stp == S(1);
   H* ysp = c.wy + (size_t)st->spare * (size_t)c.ld;
@@ -1531,10 +1565,9 @@ __device__ __forceinline__ void post_eval_pass(const Ctx<R, H, S>& c, CtaPos cp,
   MinPair mdum[1] = {MinPair{0.0, 0}};
   double ldum[1] = {0.0}, sd[NS], xm[NX] = {(double)xa};
   sums_to_double(s, sd);
-  cta_reduce_to_row<CONS + 32, NS, NX, 0, 0>(sd, xm, mdum, ldum, c.part, W, cp.rank, cp.count);
-  if (!last_cta(c.ticket, cp.count)) return;
+  if (!c.epi_only) cta_reduce_to_row<CONS + 32, NS, NX, 0, 0>(sd, xm, mdum, ldum, c.part, W, cp.rank, cp.count);
   __shared__ double red[W];
-  fold_rows<CONS + 32>(c.part, cp.count, W, NS, NX, 0, red);
+  if (!pass_fold<CONS + 32>(c, cp, W, NS, NX, 0, red)) return;
   epilogue_on_shared_warp<S>(st, [&](DevState<S>* st, int lane) {
     post_epilogue<S>(st, red, f, force_accept, lane);
   });
@@ -1597,7 +1630,8 @@ __device__ __forceinline__ void projgr_pass(const Ctx<R, H, S>& c, CtaPos cp, co
     f = (S)(R)*c.ev_f;
   }
   double xm[1] = {0.0};
-  for (long long i = (long long)cp.rank * kThreads + threadIdx.x; i < c.n;
+  const int n = c.epi_only ? 0 : c.n;
+  for (long long i = (long long)cp.rank * kThreads + threadIdx.x; i < n;
        i += (long long)cp.count * kThreads) {
     const R xi = x[i], gi = g[i];
     const int nb = c.nbd[i];
@@ -1614,10 +1648,9 @@ __device__ __forceinline__ void projgr_pass(const Ctx<R, H, S>& c, CtaPos cp, co
   }
   double sdum[1] = {0.0}, ldum[1] = {0.0};
   MinPair mdum[1] = {MinPair{0.0, 0}};
-  cta_reduce_to_row<kThreads, 0, 1, 0, 0>(sdum, xm, mdum, ldum, c.part, 1, cp.rank, cp.count);
-  if (!last_cta(c.ticket, cp.count)) return;
+  if (!c.epi_only) cta_reduce_to_row<kThreads, 0, 1, 0, 0>(sdum, xm, mdum, ldum, c.part, 1, cp.rank, cp.count);
   __shared__ double red[1];
-  fold_rows<kThreads>(c.part, cp.count, 1, 0, 1, 0, red);
+  if (!pass_fold<kThreads>(c, cp, 1, 0, 1, 0, red)) return;
   if (threadIdx.x != 0) return;
   c.st->sbgnrm = (S)red[0];
   c.st->f = f;
@@ -1705,7 +1738,7 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
     force_accept = st->ev_force;
     f = st->ev_force ? st->f : (S)(R)*c.ev_f;
   }
-  const int n = c.n, col = st->col;
+  const int n = c.epi_only ? 0 : c.n, col = st->col;
   const R stp = (R)st->stp;
   const bool unit = st->stp == S(1);
   H* ysp = c.wy + (size_t)st->spare * (size_t)c.ld;
@@ -1821,7 +1854,7 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
         acc[18] = fma(stored_value<H, A>(sv), neggi, acc[18]);
         if (has_bp) {
           acc[19] += A(1);
-          bp.offer_quotient(tnum, tden, i);
+          bp.offer_quotient(tnum, tden, i + c.ioff);
         } else {
           acc[20] += A(1);
           if (neggi != A(0)) xmx = A(1);
@@ -1829,11 +1862,16 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
       }
     };
     // kOneRole: post_elem and gcp_elem on one element, each input read from the stage once
-    auto one_role = [&](const unsigned char* buf, long long tt, int valid, int e) {
-      if (e >= valid) return;
+    // fast: every column live and a unit step (the trial point is z), as constants
+    // Every input of the element is read into registers first and the stage released.
+    auto one_role = [&](const unsigned char* buf, long long tt, int valid, int e, auto fast,
+                        auto release) {
+      constexpr bool F = decltype(fast)::value;
+      const bool unit_ = F ? true : unit;
       const int i = (int)(tt * kTile) + e;
       const R ti = stage_at<R>(buf, o_t, e), zi = stage_at<R>(buf, o_z, e);
-      const R xi = stage_at<R>(buf, o_xt, e), gi = stage_at<R>(buf, o_g, e);
+      const R xi = F ? zi : stage_at<R>(buf, o_xt, e);
+      const R gi = stage_at<R>(buf, o_g, e);
       const R gold = stage_at<R>(buf, o_go, e);
       const R li = stage_at<R>(buf, o_l, e), ui = stage_at<R>(buf, o_u, e);
       const int nb = stage_at<int>(buf, o_nb, e);
@@ -1844,6 +1882,8 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
         yv[j] = live ? hist_at<H, A>(buf, hy + j * hb, e) : A(0);
         sh[j] = live ? hist_at<H, A>(buf, hs + j * hb, e) : A(0);
       }
+      release();
+      if (e >= valid) return;  // (stale stage bytes past the tile's end)
       // role P
       const R d = rsub(zi, ti);
       acc[0] = fma((A)gi, (A)d, acc[0]);
@@ -1857,7 +1897,7 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
       acc[1] = fma((A)xd, (A)xd, acc[1]);
       const R y = rsub(gi, gold);
       acc[2] = fma((A)y, (A)y, acc[2]);
-      const R sv = unit ? d : rmul(d, stp);
+      const R sv = unit_ ? d : rmul(d, stp);
 #pragma unroll
       for (int j = 0; j < kMaxM; j++) {
         if (kFull || j < col) {
@@ -1886,18 +1926,20 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
         accg[18] = fma(stored_value<H, A>(sv), neggi, accg[18]);
         if (has_bp) {
           accg[19] += A(1);
-          bp.offer_quotient(tnum, tden, i);
+          bp.offer_quotient(tnum, tden, i + c.ioff);
         } else {
           accg[20] += A(1);
           if (neggi != A(0)) xmxg = A(1);
         }
       }
     };
+    auto stream_tiles = [&](auto fast) {
     run_stages<CONS>(ss, n, stages, dyn,
                      reinterpret_cast<uint64_t*>(dyn + (size_t)stages * cap), &st->device_error, cp,
                      [&](const unsigned char* buf, long long tt, int valid, auto release) {
       if constexpr (kOneRole) {
-        one_role(buf, tt, valid, (int)threadIdx.x);
+        one_role(buf, tt, valid, (int)threadIdx.x, fast, release);
+        return;
       } else if (role == 0) {
 #pragma unroll
         for (int h = 0; h < kTile / kRoleThreads; h++) post_elem(buf, tt, valid, rt + h * kRoleThreads);
@@ -1907,11 +1949,20 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
       }
       release();
     });
+    };
+    if constexpr (kOneRole) {
+      if (kFull && unit && xt_is_z)
+        stream_tiles(std::true_type{});
+      else
+        stream_tiles(std::false_type{});
+    } else {
+      stream_tiles(std::false_type{});
+    }
   });
   // CTA row: [ role P sums (19) | role G sums (21) | role P max | role G max | min pair ]
   constexpr int NS = NP + NG, W = NS + 2 + 2;
   constexpr int kAllWarps = CONS / 32 + 1;
-  {
+  if (!c.epi_only) {
     __shared__ double wsum[kAllWarps][W];
     for (int k = lane; k < W; k += 32) wsum[warp][k] = 0.0;
     __syncwarp();
@@ -1960,9 +2011,8 @@ __device__ __forceinline__ void post_gcp_pass(const Ctx<R, H, S>& c, CtaPos cp, 
       }
     }
   }
-  if (!last_cta(c.ticket, cp.count)) return;
   __shared__ double red[W];
-  fold_rows<CONS + 32>(c.part, cp.count, W, NS, 2, 1, red);
+  if (!pass_fold<CONS + 32>(c, cp, W, NS, 2, 1, red)) return;
   __shared__ SmallWork<S> sw;
   __shared__ double rp[NP + 1], rg[22];  // epilogue temporaries (shared, as all of them)
   epilogue_on_shared_warp<S>(st, [&](DevState<S>* st, int lane) {

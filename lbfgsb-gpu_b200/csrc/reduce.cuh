@@ -185,4 +185,75 @@ __device__ __forceinline__ void fold_rows(const double* part, int rows, int widt
   __syncthreads();
 }
 
+// ---- sharded solves: one problem over several ranks, each holding an index range ----
+//
+// A pass's reduction then spans the ranks.  Each rank's last CTA folds its own rows
+// (fold_rows) and, instead of running the epilogue, writes the folded row to c.shard_send
+// (kShardRow doubles: the row, then one extra slot) and returns.  The host gathers every
+// rank's row into c.shard_recv (rank r at r * kShardRow, the caller's all-gather) and
+// launches the pass again in one CTA with c.epi_only set: that CTA folds the rank rows in
+// rank order and runs the epilogue, so every rank runs it on the same values.
+constexpr int kShardRow = 256;
+
+// out[k] from the world rank rows of recv, column kinds as in fold_rows, each column
+// folded in rank order.
+template <int NT>
+__device__ __forceinline__ void fold_rank_rows(const double* recv, int world, int width, int ns,
+                                               int nx, int nm, double* out) {
+  for (int k = threadIdx.x; k < width; k += NT) {
+    if (k >= ns && k < ns + nx) {
+      double a = -INFINITY;
+      for (int r = 0; r < world; r++) {
+        const double v = recv[(size_t)r * kShardRow + k];
+        a = (v > a) ? v : a;
+      }
+      out[k] = a;
+    } else if (k >= ns + nx && k < ns + nx + 2 * nm) {
+      if (((k - ns - nx) & 1) != 0) continue;  // the index column of a min pair
+      MinPair a{INFINITY, kNoIndex};
+      for (int r = 0; r < world; r++) {
+        const double* row = recv + (size_t)r * kShardRow;
+        a = minpair(a, MinPair{row[k], (long long)row[k + 1]});
+      }
+      out[k] = a.v;
+      out[k + 1] = (double)a.i;
+    } else {
+      double a = 0.0;
+      for (int r = 0; r < world; r++) a += recv[(size_t)r * kShardRow + k];
+      out[k] = a;
+    }
+  }
+  __syncthreads();
+}
+
+// The fold of a pass's rows before its epilogue.  Returns true in the one CTA that runs
+// the epilogue, with the folded row in red.  hash: a 64-bit sum the pass's CTAs added up
+// in device memory (the free-set hash), carried in the extra slot of a rank row and summed
+// (mod 2^64) over the ranks.
+template <int NT, typename C>
+__device__ __forceinline__ bool pass_fold(const C& c, CtaPos cp, int width, int ns, int nx,
+                                          int nm, double* red,
+                                          unsigned long long* hash = nullptr) {
+  if (c.epi_only) {
+    fold_rank_rows<NT>(c.shard_recv, c.shard_world, width, ns, nx, nm, red);
+    if (hash && threadIdx.x == 0) {
+      unsigned long long h = 0;
+      for (int r = 0; r < c.shard_world; r++)
+        h += (unsigned long long)__double_as_longlong(c.shard_recv[(size_t)r * kShardRow + width]);
+      *hash = h;
+    }
+    __syncthreads();
+    return true;
+  }
+  if (!last_cta(c.ticket, cp.count)) return false;
+  fold_rows<NT>(c.part, cp.count, width, ns, nx, nm, red);
+  if (c.shard_send) {
+    for (int k = threadIdx.x; k < width; k += NT) c.shard_send[k] = red[k];
+    if (threadIdx.x == 0)
+      c.shard_send[width] = hash ? __longlong_as_double((long long)*(volatile unsigned long long*)hash) : 0.0;
+    return false;
+  }
+  return true;
+}
+
 }  // namespace lbfgsb_b200

@@ -113,10 +113,11 @@ __device__ __forceinline__ Key96 key_prev(Key96 k) {
 
 // One level of the radix select, from the level's histogram (the same in every thread that
 // runs it): the boundary digit d, the keys below it, and whether the select may stop here
-// with the chunk "every candidate below bucket d" (at least kChunkMin keys in all).  taken:
+// with the chunk "every candidate below bucket d" (at least chunk_min keys in all).  taken:
 // keys already below the prefix from earlier levels; kk: keys still wanted.
 __device__ __forceinline__ void select_level(const unsigned int* hist, long long taken,
-                                             long long kk, int& d, long long& cum, bool& stop) {
+                                             long long kk, long long chunk_min, int& d,
+                                             long long& cum, bool& stop) {
   cum = 0;
   d = 255;
   for (int b = 0; b < 256; b++) {
@@ -126,7 +127,7 @@ __device__ __forceinline__ void select_level(const unsigned int* hist, long long
     }
     cum += hist[b];
   }
-  stop = taken + cum >= kChunkMin;
+  stop = taken + cum >= chunk_min;
 }
 
 // Thread 0's running walk (lbfgsbcpu.cpp:725-809) across chunks.
@@ -151,16 +152,10 @@ struct WalkSmem {
   S work[kBatch][kMaxM + 1];
 };
 
-// Sort the cnt keys in sm.k_hi / k_lo and walk them (all threads of the CTA).  Sets sm.done:
-// 1 the walk ended, 2 a step of M*wbp failed (the driver resets the memory).
-template <typename R, typename H, typename S>
-__device__ void walk_chunk(const Ctx<R, H, S>& c, const R* __restrict__ x, const R* __restrict__ g,
-                           const H* const (&Y)[kMaxM], const H* const (&Sl)[kMaxM], WalkSmem<S>& sm,
-                           int cnt, WalkCarry<S>& w) {
-  DevState<S>* st = c.st;
-  const int n = c.n, col = st->col, col2 = 2 * col, nbreak = st->nbreak, bnded = st->bnded;
-  const S theta = st->theta;
-  // ---- bitonic sort of the chunk by (hi, lo), padded with maximal keys ----
+// Bitonic sort of the cnt keys in sm.k_hi / k_lo by (hi, lo), padded with maximal keys
+// (all threads of the CTA).
+template <typename S>
+__device__ void sort_chunk(WalkSmem<S>& sm, int cnt) {
   for (int e = cnt + threadIdx.x; e < kChunk; e += blockDim.x) {
     sm.k_hi[e] = ~0ull;
     sm.k_lo[e] = ~0u;
@@ -184,22 +179,23 @@ __device__ void walk_chunk(const Ctx<R, H, S>& c, const R* __restrict__ x, const
       __syncthreads();
     }
   }
-  // ---- walk the chunk in batches ----
+}
+
+// Walk the cnt sorted keys of sm (all threads of the CTA) with the reference's recurrence
+// (lbfgsbcpu.cpp:725-809).  prep(q, k) fills sm.dibp[q], sm.zibp[q] and sm.wbp[q][1..2col]
+// for key k of the chunk (run by thread q of a batch); pass(k, dibp) records that the walk
+// passed key k (thread 0).  Sets sm.done: 1 the walk ended, 2 a step of M*wbp failed (the
+// driver resets the memory).
+template <typename S, typename Prep, typename Pass>
+__device__ void walk_sorted(DevState<S>* st, WalkSmem<S>& sm, int cnt, WalkCarry<S>& w,
+                            Prep&& prep, Pass&& pass) {
+  const int n = st->n, col = st->col, col2 = 2 * col, nbreak = st->nbreak, bnded = st->bnded;
+  const S theta = st->theta;
   for (int b0 = 0; b0 < cnt; b0 += kBatch) {
     const int nb = (cnt - b0) < kBatch ? (cnt - b0) : kBatch;
     if (threadIdx.x < nb) {
-      const int k = b0 + threadIdx.x;
-      const int i = (int)sm.k_lo[k];
-      const R xi = x[i], gi = g[i];
-      const R dibp = -gi;
-      const R zibp = (dibp > R(0)) ? rsub(c.u[i], xi) : rsub(c.l[i], xi);
-      sm.dibp[threadIdx.x] = (S)dibp;
-      sm.zibp[threadIdx.x] = (S)zibp;
-      S* wbp = sm.wbp[threadIdx.x];
-      for (int j = 0; j < col; j++) {
-        wbp[1 + j] = (S)HistTraits<H>::load(Y[j] + i);
-        wbp[1 + col + j] = theta * (S)HistTraits<H>::load(Sl[j] + i);
-      }
+      prep((int)threadIdx.x, b0 + (int)threadIdx.x);
+      const S* wbp = sm.wbp[threadIdx.x];
       if (col > 0) {
         int info = 0;
         sbmv(st->sy, st->wt, col, wbp, sm.v[threadIdx.x], &info, sm.work[threadIdx.x]);
@@ -216,7 +212,6 @@ __device__ void walk_chunk(const Ctx<R, H, S>& c, const R* __restrict__ x, const
       for (int q = 0; q < nb && sm.done == 0; q++) {
         const int k = b0 + q;
         const S tk = (S)__longlong_as_double((long long)sm.k_hi[k]);
-        const int ibp = (int)sm.k_lo[k];
         const S tj0 = w.tj;
         w.tj = tk;
         const S dt = w.tj - tj0;
@@ -227,7 +222,7 @@ __device__ void walk_chunk(const Ctx<R, H, S>& c, const R* __restrict__ x, const
         w.tsum = w.tsum + dt;
         w.nleft = w.nleft - 1;
         const S dibp = sm.dibp[q];
-        c.code[ibp] = (int8_t)(dibp > S(0) ? IW_WALK_UPP : IW_WALK_LOW);
+        pass(k, dibp);
         if (w.nleft == 0 && nbreak == n) {
           w.dtm = dt;
           for (int j = 1; j <= col2; j++) st->c[j] += w.dtm * st->p[j];
@@ -267,6 +262,35 @@ __device__ void walk_chunk(const Ctx<R, H, S>& c, const R* __restrict__ x, const
     __syncthreads();
     if (sm.done) break;
   }
+}
+
+// Sort the cnt keys in sm.k_hi / k_lo and walk them, reading each candidate's x, g, bounds
+// and history row from the solve's arrays (all threads of the CTA).
+template <typename R, typename H, typename S>
+__device__ void walk_chunk(const Ctx<R, H, S>& c, const R* __restrict__ x, const R* __restrict__ g,
+                           const H* const (&Y)[kMaxM], const H* const (&Sl)[kMaxM], WalkSmem<S>& sm,
+                           int cnt, WalkCarry<S>& w) {
+  DevState<S>* st = c.st;
+  const int col = st->col;
+  const S theta = st->theta;
+  sort_chunk(sm, cnt);
+  walk_sorted(st, sm, cnt, w,
+      [&](int q, int k) {
+        const int i = (int)sm.k_lo[k];
+        const R xi = x[i], gi = g[i];
+        const R dibp = -gi;
+        const R zibp = (dibp > R(0)) ? rsub(c.u[i], xi) : rsub(c.l[i], xi);
+        sm.dibp[q] = (S)dibp;
+        sm.zibp[q] = (S)zibp;
+        S* wbp = sm.wbp[q];
+        for (int j = 0; j < col; j++) {
+          wbp[1 + j] = (S)HistTraits<H>::load(Y[j] + i);
+          wbp[1 + col + j] = theta * (S)HistTraits<H>::load(Sl[j] + i);
+        }
+      },
+      [&](int k, S dibp) {
+        c.code[(int)sm.k_lo[k]] = (int8_t)(dibp > S(0) ? IW_WALK_UPP : IW_WALK_LOW);
+      });
 }
 
 // The walk's start from the state and its end into it (thread 0).
@@ -365,7 +389,7 @@ __device__ __forceinline__ void walk_pass(const Ctx<R, H, S>& c, const R* __rest
           int d;
           long long cum;
           bool stop;
-          select_level(sm.hist, sm.taken, sm.kk, d, cum, stop);
+          select_level(sm.hist, sm.taken, sm.kk, kChunkMin, d, cum, stop);
           Key96 p = sm.prefix;
           key_set_digit(p, level, d);
           if (stop) {
@@ -516,7 +540,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_coop(Ctx<R, H, S> c, cons
         int d;
         long long cum;
         bool stop;
-        select_level(s_hist, taken, kk, d, cum, stop);
+        select_level(s_hist, taken, kk, kChunkMin, d, cum, stop);
         __syncthreads();  // every thread has read s_hist before the next level clears it
         key_set_digit(prefix, level, d);
         if (stop) {

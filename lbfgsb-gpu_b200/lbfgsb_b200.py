@@ -74,6 +74,15 @@ class Stats(C.Structure):
                 ("bytes_per_iteration_model", C.c_double), ("rounds", C.c_longlong)]
 
 
+# allgather(user, send, recv, count, stream) of a sharded solve (device pointers)
+ALLGATHER_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p)
+
+
+class Shard(C.Structure):
+    _fields_ = [("rank", C.c_int), ("world", C.c_int), ("n_global", C.c_int),
+                ("offset", C.c_int), ("allgather", C.c_void_p), ("allgather_user", C.c_void_p)]
+
+
 CB64 = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
                    C.POINTER(C.c_double), C.c_void_p, C.POINTER(SummaryF64))
 CB32 = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float),
@@ -136,6 +145,11 @@ def load() -> C.CDLL:
         fn.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                        C.POINTER(opt), C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Ext),
                        C.POINTER(summ)]
+        fn = getattr(lib, f"lbfgsb_b200_minimize_sharded_{sfx}")
+        fn.restype = C.c_int
+        fn.argtypes = [C.POINTER(Shard), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                       C.c_void_p, C.POINTER(opt), C.c_void_p, C.c_void_p, C.c_void_p,
+                       C.c_void_p, C.c_void_p, C.POINTER(Ext), C.POINTER(summ)]
     lib.lbfgsb_b200_last_stats.restype = C.c_int
     lib.lbfgsb_b200_last_stats.argtypes = [C.POINTER(Stats)]
     lib.lbfgsb_b200_last_error.restype = C.c_char_p
@@ -639,3 +653,213 @@ def solve(prob: dict, dtype=np.float64, x0=None, option=None, objective: str = "
     res.residual_x = float(summ.residual_x)
     res.stats = last_stats()
     return res
+
+
+class ThreadAllGather:
+    """All-gather among `world` threads of one process, for sharded solves whose ranks share
+    one GPU (each rank a thread with its own stream).  Every call waits for the rank's
+    stream, stages its `count` doubles on the host, meets the other ranks at a barrier and
+    copies everyone's values to recv; no kernel waits on another rank's kernels.  A rank that
+    does not arrive within `timeout` seconds breaks the barrier, and the call returns 1."""
+
+    def __init__(self, world: int, timeout: float = 120.0):
+        import threading
+        self.world = world
+        self.barrier = threading.Barrier(world, timeout=timeout)
+        self.slots = [None] * world
+
+    def callback(self, rank: int):
+        import torch
+        lib = load()
+
+        def gather(_user, send, recv, count, stream):
+            try:
+                torch.cuda.ExternalStream(stream).synchronize() if stream else torch.cuda.synchronize()
+                mine = np.empty(count, dtype=np.float64)
+                lib.lbfgsb_b200_copy(mine.ctypes.data, send, mine.nbytes, 2)
+                self.slots[rank] = mine
+                self.barrier.wait()
+                allv = np.concatenate(self.slots)
+                lib.lbfgsb_b200_copy(recv, allv.ctypes.data, allv.nbytes, 1)
+                self.barrier.wait()
+                return 0
+            except Exception:  # a broken barrier: another rank left
+                self.barrier.abort()
+                return 1
+
+        return ALLGATHER_CB(gather)
+
+
+def solve_sharded(prob: dict, world: int, dtype=np.float64, option=None, form: int = FORM_PLAIN,
+                  trace: bool = False, parts=None, timeout: float = 120.0) -> GpuResult:
+    """One problem split by index range over `world` ranks that share cuda:0: each rank is a
+    thread calling lbfgsb_b200_minimize_sharded_* on its own stream, with a ThreadAllGather.
+    The objective is evaluated on the host by the oracle's objective (oracle/objective.c) on
+    the whole x, gathered from the ranks; rank 0 returns f and the others 0.  parts: the
+    ranks' sizes (default: np.array_split's).  Returns rank 0's result with the whole x."""
+    import sys
+    import threading
+
+    import torch
+
+    lib = load()
+    repo = os.path.dirname(HERE)
+    if repo not in sys.path:
+        sys.path.insert(0, repo)
+    from oracle import binding as OB  # test glue: the CPU objective of the oracle
+
+    dtype = np.dtype(dtype)
+    is64 = dtype == np.float64
+    n = int(prob["nbd"].size)
+    sizes = list(parts) if parts is not None else [len(a) for a in np.array_split(np.arange(n), world)]
+    assert len(sizes) == world and sum(sizes) == n
+    offs = [int(v) for v in np.concatenate([[0], np.cumsum(sizes)[:-1]])]
+    real = C.c_double if is64 else C.c_float
+    cbt = CB64 if is64 else CB32
+    sfx = "f64" if is64 else "f32"
+    ev = OB.host_objective(prob, dtype)
+    hx = np.zeros(n, dtype=dtype)
+    hg = np.zeros(n, dtype=dtype)
+    fbox = (real * 1)()
+    bar = threading.Barrier(world, timeout=timeout)
+    ag = ThreadAllGather(world, timeout)
+    results = [None] * world
+    keep = []
+
+    def rank_main(r):
+        torch.cuda.set_device(0)
+        dev = torch.device("cuda:0")
+        stream = torch.cuda.Stream(device=dev)
+        lo, nr = offs[r], sizes[r]
+        with torch.cuda.stream(stream):
+            x = torch.zeros(nr, dtype=torch.float64 if is64 else torch.float32, device=dev)
+            l = torch.from_numpy(np.ascontiguousarray(prob["l"][lo:lo + nr], dtype=dtype)).to(dev)
+            u = torch.from_numpy(np.ascontiguousarray(prob["u"][lo:lo + nr], dtype=dtype)).to(dev)
+            nbd = torch.from_numpy(np.ascontiguousarray(prob["nbd"][lo:lo + nr], dtype=np.int32)).to(dev)
+        stream.synchronize()
+        res = GpuResult(x=None, info=0, num_iteration=0, residual_g=0, residual_f=0,
+                        residual_x=0, status=0)
+
+        def fg(_user, xp, fp, gp, sp, _summ):
+            try:
+                torch.cuda.ExternalStream(sp).synchronize()
+                part = np.empty(nr, dtype=dtype)
+                lib.lbfgsb_b200_copy(part.ctypes.data, C.cast(xp, C.c_void_p), part.nbytes, 2)
+                hx[lo:lo + nr] = part
+                bar.wait()
+                if r == 0:
+                    ev(hx.ctypes.data_as(C.POINTER(real)), fbox, hg.ctypes.data_as(C.POINTER(real)))
+                bar.wait()
+                gpart = np.ascontiguousarray(hg[lo:lo + nr])
+                lib.lbfgsb_b200_copy(C.cast(gp, C.c_void_p), gpart.ctypes.data, gpart.nbytes, 1)
+                fp[0] = fbox[0] if r == 0 else 0.0
+                if r == 0:
+                    res.evals.append(float(fbox[0]))
+                bar.wait()
+                return 0
+            except Exception:
+                bar.abort()
+                return 1
+
+        def tr(_user, rp):
+            rec = rp[0]
+            res.trace.append({k: (list(getattr(rec, k)) if k == 'dbg' else getattr(rec, k))
+                              for k in _TRACE_KEYS})
+
+        cb = cbt(fg)
+        cb_tr = TRACE_CB(tr) if trace else TRACE_CB()
+        gcb = ag.callback(r)
+        keep.extend([cb, cb_tr, gcb])
+        sh = Shard(r, world, n, lo, C.cast(gcb, C.c_void_p).value, None)
+        ext = Ext(form, 0, cb_tr, None, 0)
+        summ = SummaryF64() if is64 else SummaryF32()
+        opt = option if option is not None else default_option(dtype)
+        fn = getattr(lib, f"lbfgsb_b200_minimize_sharded_{sfx}")
+        status = fn(C.byref(sh), nr, x.data_ptr(), nbd.data_ptr(), l.data_ptr(), u.data_ptr(),
+                    C.byref(opt), C.cast(cb, C.c_void_p).value, None, None, None,
+                    C.c_void_p(stream.cuda_stream), C.byref(ext), C.byref(summ))
+        stream.synchronize()
+        res.status = status
+        res.x = x.cpu().numpy()
+        res.info = summ.info
+        res.num_iteration = summ.num_iteration
+        res.residual_g = float(summ.residual_g)
+        res.residual_f = float(summ.residual_f)
+        res.residual_x = float(summ.residual_x)
+        if status != 0:
+            res.stats = {"error": lib.lbfgsb_b200_last_error().decode()}
+            bar.abort()
+        results[r] = res
+
+    threads = [threading.Thread(target=rank_main, args=(r,)) for r in range(world)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for r, res in enumerate(results):
+        if res is None or res.status != 0:
+            raise RuntimeError(f"sharded rank {r} failed: {None if res is None else res.stats}")
+    out = results[0]
+    out.x = np.concatenate([res.x for res in results])
+    out.stats = {"ranks": [(res.info, res.num_iteration, res.residual_g, res.residual_f)
+                           for res in results]}
+    return out
+
+
+class _DeviceArray:
+    """A raw device pointer seen as a 1-D float64 CUDA array (__cuda_array_interface__), so
+    that torch can wrap it without a copy."""
+
+    def __init__(self, ptr: int, count: int):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": "<f8",
+                                         "data": (int(ptr), False), "version": 3,
+                                         "strides": None}
+
+
+def shard_ranges(n: int, world: int) -> list:
+    """The index ranges (offset, size) of `world` ranks over n variables, as contiguous
+    blocks in rank order (sizes differ by at most one)."""
+    base, extra = divmod(n, world)
+    out, off = [], 0
+    for r in range(world):
+        size = base + (1 if r < extra else 0)
+        out.append((off, size))
+        off += size
+    return out
+
+
+class DistAllGather:
+    """The all-gather of a sharded solve over a torch.distributed process group, one process
+    per GPU: with the nccl backend, send and recv are device pointers and the NCCL all-gather
+    is enqueued on the solver's stream (no host synchronisation); with gloo (CPU), send and
+    recv are host pointers and the exchange completes before the call returns."""
+
+    def __init__(self, group=None, device: bool = True):
+        self.group = group
+        self.device = device
+
+    def exchange(self, send: int, recv: int, count: int, stream=None) -> int:
+        import torch
+        import torch.distributed as dist
+        world = dist.get_world_size(self.group)
+        if self.device:
+            s_t = torch.as_tensor(_DeviceArray(send, count), device="cuda")
+            r_t = torch.as_tensor(_DeviceArray(recv, world * count), device="cuda")
+            st = torch.cuda.ExternalStream(stream) if stream else torch.cuda.current_stream()
+            with torch.cuda.stream(st):
+                dist.all_gather_into_tensor(r_t, s_t, group=self.group)
+        else:
+            s_np = np.ctypeslib.as_array(C.cast(send, C.POINTER(C.c_double)), shape=(count,))
+            r_np = np.ctypeslib.as_array(C.cast(recv, C.POINTER(C.c_double)), shape=(world * count,))
+            out = torch.from_numpy(r_np)
+            dist.all_gather_into_tensor(out, torch.from_numpy(s_np).clone(), group=self.group)
+        return 0
+
+    def callback(self):
+        def gather(_user, send, recv, count, stream):
+            try:
+                return self.exchange(send, recv, count, stream)
+            except Exception:
+                return 1
+        self._cb = ALLGATHER_CB(gather)
+        return self._cb
