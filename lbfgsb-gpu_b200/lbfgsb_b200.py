@@ -111,6 +111,7 @@ EXPORTS = [
     "lbfgsb_b200_batch_server_create_f32", "lbfgsb_b200_batch_server_submit_f32",
     "lbfgsb_b200_batch_server_wait", "lbfgsb_b200_batch_server_peak",
     "lbfgsb_b200_batch_server_destroy", "lbfgsb_b200_batch_request_bytes",
+    "lbfgsb_b200_minimize_sharded_f64", "lbfgsb_b200_minimize_sharded_f32",
 ]
 
 _lib = None
