@@ -7,8 +7,9 @@
 // kTile-element tile into a multi-stage shared-memory ring; the CTA's threads compute on
 // stage s while stages s+1.. are in flight.  No multicast is used.
 //
-// Every wait on an mbarrier is bounded: after kWaitPolls failed polls the CTA records
-// the failure in *err and stops issuing; the host turns the flag into an error status.
+// Every wait on an mbarrier is bounded: after kWaitNs nanoseconds without completion the
+// CTA records the failure in *err and stops issuing; the host turns the flag into an error
+// status.
 #pragma once
 
 #include <stdint.h>
@@ -63,11 +64,38 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait; false after kWaitPolls polls.
+// try_wait with a suspend-time hint: a thread whose phase is not complete sleeps until it
+// completes or `ns` nanoseconds pass, instead of returning after the system's shorter limit
+// (fewer polls, so fewer issue slots taken from the warps that compute).
+__device__ __forceinline__ bool mbar_try_wait_for(uint64_t* bar, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+constexpr uint32_t kSuspendNs = 1000000;            // 1 ms per try_wait at most
+constexpr unsigned long long kWaitNs = 2000000000;  // give up after 2 s
+
+// Bounded wait; false after kWaitNs nanoseconds (device global timer) without completion.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (int k = 0; k < kWaitPolls; k++)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  while (true) {
+    if (mbar_try_wait_for(bar, parity, kSuspendNs)) return true;
+    if (global_ns() - t0 > kWaitNs) return false;
+  }
 }
 
 // L2 policy of the streamed tiles: evict first.  An n-vector is read once or twice per
