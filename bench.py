@@ -17,7 +17,8 @@ ours:      W untimed iterations, then exactly K iterations timed with CUDA event
            both sides), inputs resident in HBM (vectors far larger than the 126 MB L2).
            e2e: one solve of K iterations through the C ABI from pinned host buffers:
            the host-to-device copies of x0, l, u, nbd, the whole call (workspace, start
-           point, K iterations) and the device-to-host copy of x inside the timed region.
+           point, K iterations) and the device-to-host copy of x inside the timed region,
+           after one untimed call of the same (allocator and memory-pool warm-up).
            The objective's fields are the user's problem data and are uploaded before.
 batched:   a 256-instance sample of the batched workload (FP32 solves of n from 1,024 to
            262,144): solves/s one after another on one stream and side by side on 16.
@@ -324,24 +325,30 @@ def run_ours(args, rank: int, world: int, dist):
     # the objective's fields are the user's problem data, set up before the solve call
     so2 = LB.SynthObjective(prob, single_precision_fields=not is64)
     ext2 = LB.Ext(run.form, 0, LB.TRACE_CB(), None)
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    dx = hx.to(dev, non_blocking=True)
-    dl = hl.to(dev, non_blocking=True)
-    du = hu.to(dev, non_blocking=True)
-    dn = hn.to(dev, non_blocking=True)
-    summ2 = run.summ_t()
-    st = run.minimize(n, dx.data_ptr(), dn.data_ptr(), dl.data_ptr(), du.data_ptr(),
-                      C.byref(option(K)), so2.f64 if is64 else so2.f32, None, None, so2.handle,
-                      None, C.byref(ext2), C.byref(summ2))
-    hout.copy_(dx, non_blocking=True)
-    e1.record()
-    e1.synchronize()
-    if st != 0:
-        raise RuntimeError(f"status {st}")
-    e2e_ms = e0.elapsed_time(e1)
+    def e2e_once():
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dx = hx.to(dev, non_blocking=True)
+        dl = hl.to(dev, non_blocking=True)
+        du = hu.to(dev, non_blocking=True)
+        dn = hn.to(dev, non_blocking=True)
+        summ2 = run.summ_t()
+        st = run.minimize(n, dx.data_ptr(), dn.data_ptr(), dl.data_ptr(), du.data_ptr(),
+                          C.byref(option(K)), so2.f64 if is64 else so2.f32, None, None,
+                          so2.handle, None, C.byref(ext2), C.byref(summ2))
+        hout.copy_(dx, non_blocking=True)
+        e1.record()
+        e1.synchronize()
+        if st != 0:
+            raise RuntimeError(f"status {st}")
+        return e0.elapsed_time(e1), summ2
+
+    # one untimed call first: the device buffers of the copies come from torch's caching
+    # allocator and the solver's workspace from its pool, whose first growth maps memory
+    e2e_once()
+    e2e_ms, summ2 = e2e_once()
     so2.close()
     h2d = hx.nbytes + hl.nbytes + hu.nbytes + hn.nbytes
     d2h = hout.nbytes + 8 * summ2.num_iteration  # x and the per-evaluation f

@@ -122,10 +122,13 @@ __device__ __forceinline__ bool last_cta(unsigned int* ticket, int count) {
 // for k < ns and k >= ns + nx + 2*nm (lane-owned block), max for the next nx columns,
 // min pairs for the next 2*nm columns.  Warps take columns round robin; lanes stride over
 // rows; a fixed butterfly finishes each column.  A warp works on kFoldCols of its columns
-// at once (their loads of a row are independent), so that the fold waits about one
-// memory round trip per kFoldCols columns; each column's operations and their order do
-// not depend on that grouping.
+// at once, and a lane issues the loads of all its rows of those columns (kFoldRows of
+// them, 32 * kFoldRows rows a round) before it adds them, so that the fold waits about one
+// memory round trip per kFoldCols columns (one CTA reading the rows is latency-bound);
+// each column's operations and their order (a lane's rows in increasing order, then the
+// butterfly) do not depend on that grouping.
 constexpr int kFoldCols = 4;
+constexpr int kFoldRows = 5;
 template <int NT>
 __device__ __forceinline__ void fold_rows(const double* part, int rows, int width, int ns,
                                           int nx, int nm, double* out) {
@@ -149,18 +152,31 @@ __device__ __forceinline__ void fold_rows(const double* part, int rows, int widt
       acc[u] = kind[u] == 1 ? -INFINITY : 0.0;
       mp[u] = MinPair{INFINITY, kNoIndex};
     }
-    for (int r = lane; r < rows; r += 32) {
-      const double* row = part + r;  // entry k at row[k * rows]
+    for (int r0 = lane; r0 < rows; r0 += 32 * kFoldRows) {
+      double v[kFoldCols][kFoldRows];
+#pragma unroll
+      for (int u = 0; u < kFoldCols; u++) {
+        const double* col = part + (size_t)(k0 + u * kWarps) * rows;  // entry k at [k * rows + r]
+#pragma unroll
+        for (int q = 0; q < kFoldRows; q++) {
+          const int r = r0 + 32 * q;
+          v[u][q] = (kind[u] != 3 && r < rows) ? col[r] : 0.0;
+        }
+      }
 #pragma unroll
       for (int u = 0; u < kFoldCols; u++) {
         const int k = k0 + u * kWarps;
-        if (kind[u] == 0) {
-          acc[u] += row[(size_t)k * rows];
-        } else if (kind[u] == 1) {
-          const double v = row[(size_t)k * rows];
-          acc[u] = (v > acc[u]) ? v : acc[u];
-        } else if (kind[u] == 2) {
-          mp[u] = minpair(mp[u], MinPair{row[(size_t)k * rows], (long long)row[(size_t)(k + 1) * rows]});
+#pragma unroll
+        for (int q = 0; q < kFoldRows; q++) {
+          const int r = r0 + 32 * q;
+          if (r >= rows) break;
+          if (kind[u] == 0) {
+            acc[u] += v[u][q];
+          } else if (kind[u] == 1) {
+            acc[u] = (v[u][q] > acc[u]) ? v[u][q] : acc[u];
+          } else if (kind[u] == 2) {
+            mp[u] = minpair(mp[u], MinPair{v[u][q], (long long)part[(size_t)(k + 1) * rows + r]});
+          }
         }
       }
     }

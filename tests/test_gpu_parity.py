@@ -210,3 +210,15 @@ def test_config0_s256_full_solve(LB, OB):
     has_l = (nbd == 1) | (nbd == 2)
     has_u = (nbd == 2) | (nbd == 3)
     assert np.all(b.x[has_l] >= prob["l"][has_l]) and np.all(b.x[has_u] <= prob["u"][has_u])
+    # final x and ||proj g||_inf, against the spread of the oracle's own ending: the oracle
+    # restarted from x0 moved by 1e-19 gives the scale of the difference that the run's
+    # conditioning allows (every rounding difference acts like such a move)
+    xp = 1e-19 * np.random.default_rng(1).standard_normal(prob["nbd"].size)
+    c = OB.run_cpu("oracle", prob, np.float64, x0=xp,
+                   option=apply_options(OB.default_option(np.float64), over), record=False)
+    dx_ref = float(np.max(np.abs(c.x - a.x)))
+    dx = float(np.max(np.abs(b.x - a.x)))
+    assert dx <= 4.0 * dx_ref + 1e-8, (dx, dx_ref)
+    dg_ref = abs(c.residual_g - a.residual_g)
+    dg = abs(b.residual_g - a.residual_g)
+    assert dg <= 4.0 * max(dg_ref, 1e-3 * abs(a.residual_g)), (dg, dg_ref, a.residual_g)

@@ -115,3 +115,30 @@ def test_sharded_input_errors(LB, OB):
     rank makes every rank return info = -1."""
     a, b = run_pair(LB, OB, "err_nbd4", 2)
     assert a.info == -1 and b.info == -1
+
+
+def test_sharded_four_ranks(LB, OB):
+    """s = 128 (n = 16,384, bounds +-0.05), four ranks of 4096 variables: several tiles and
+    CTAs per rank; the first 40 iterations."""
+    from cases import _synth
+    prob = _synth(128, seed=12, bound=0.05)
+    over = {"eps_f": 1e-8, "eps_g": 1e-8, "eps_x": 1e-8, "max_iteration": 40}
+    a = OB.run_cpu("oracle", prob, np.float64, option=apply_options(OB.default_option(np.float64), over),
+                   trace=True)
+    b = LB.solve_sharded(prob, 4, np.float64,
+                         option=apply_options(LB.default_option(np.float64), over), trace=True)
+    check_fp64(a, b)
+
+
+def test_sharded_mixed_form(LB, OB):
+    """The mixed form (FP32 vectors and history, FP64 scalars) sharded over two ranks ends
+    within 1e-5 of the same form on one GPU."""
+    name = "synth_s32_f32_b002"
+    prob, dt, x0, over, stop = make_case(name)
+    opt = apply_options(LB.default_option(dt), over)
+    one = LB.solve(prob, dt, option=opt, objective="host", form=LB.FORM_MIXED, trace=True)
+    two = LB.solve_sharded(prob, 2, dt, option=apply_options(LB.default_option(dt), over),
+                           form=LB.FORM_MIXED, trace=True)
+    assert two.info == one.info
+    fa, fb = one.trace[-1]["f"], two.trace[-1]["f"]
+    assert abs(fa - fb) / max(1.0, abs(fa)) <= 1e-5
