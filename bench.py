@@ -20,8 +20,13 @@ ours:      W untimed iterations, then exactly K iterations timed with CUDA event
            point, K iterations) and the device-to-host copy of x inside the timed region,
            after one untimed call of the same (allocator and memory-pool warm-up).
            The objective's fields are the user's problem data and are uploaded before.
-batched:   a 256-instance sample of the batched workload (FP32 solves of n from 1,024 to
-           262,144): solves/s one after another on one stream and side by side on 16.
+batched:   the batched workload (4,096 FP32 solves of n from 1,024 to 262,144) in one
+           batched device-driven solve, against a 32-problem sample of plain solves one
+           after another and the reference's CPU path on the host cores.
+serving:   a 400-request sample of the Poisson request stream through the continuous-
+           batching server, with p50 / p99 latency, beside the same requests one at a time.
+forms:     the precision forms at 4096^2 and 2048^2 with each pass's HBM fraction.
+walk:      a first Cauchy step that passes ~9e5 breakpoints (n = 1024^2).
 dsscfg:    the reference's only published workload (its dsscfg example): our GPU path with
            the device dsscfg objective against the reference's CPU path with its own
            objective, at 256^2 FP64 and 2048^2 FP32, beside the published speedups.

@@ -78,15 +78,28 @@ __device__ __forceinline__ void synth_body(int s, const R* __restrict__ x, const
                                            const F* __restrict__ b, R* __restrict__ g,
                                            double* part, unsigned int* ticket, double f0,
                                            double* fout, CtaPos cp) {
-  const long long n = (long long)s * s;
   const R h = R(1) / (R)(s + 1), h2 = h * h;
   double acc = 0.0;
-  for (long long k = (long long)cp.rank * kThreads + threadIdx.x; k < n;
-       k += (long long)cp.count * kThreads) {
-    const int i = (int)(k % s), j = (int)(k / s);
+  // work units: segments of kThreads columns of one row (segs per row), unit u = CTA rank
+  // + m * count for m = 0, 1, ...; the unit's row and segment are stepped along, so no
+  // element needs a division to find its row and column
+  const int segs = (s + kThreads - 1) / kThreads;
+  const long long units = (long long)s * segs;
+  const int dj = cp.count / segs, dseg = cp.count % segs;
+  int j = cp.rank / segs, seg = cp.rank % segs;
+  for (long long u = cp.rank; u < units; u += cp.count) {
+    const int row = j, i = seg * kThreads + (int)threadIdx.x;
+    seg += dseg;
+    j += dj;
+    if (seg >= segs) {
+      seg -= segs;
+      j++;
+    }
+    if (i >= s) continue;
+    const long long k = (long long)row * s + i;
     const R xk = x[k];
     const R xe = (i + 1 < s) ? x[k + 1] : R(0);
-    const R xn = (j + 1 < s) ? x[k + s] : R(0);
+    const R xn = (row + 1 < s) ? x[k + s] : R(0);
     const R de = xe - xk, dn = xn - xk;
     const R kk = (R)kap[k], wk = (R)w[k], bk = (R)b[k];
     const R z = xk - (R)tt[k];
@@ -101,7 +114,7 @@ __device__ __forceinline__ void synth_body(int s, const R* __restrict__ x, const
     acc += (double)term;
     R gk = -kk * (de + dn);
     if (i > 0) gk += (R)kap[k - 1] * (xk - x[k - 1]);
-    if (j > 0) gk += (R)kap[k - s] * (xk - x[k - s]);
+    if (row > 0) gk += (R)kap[k - s] * (xk - x[k - s]);
     gk += h2 * (wk * sigmoid - bk - R(0.15) * s3);
     g[k] = gk;
   }
