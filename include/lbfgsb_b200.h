@@ -29,7 +29,7 @@ extern "C" {
 #define LBFGSB_B200_OK 0
 #define LBFGSB_B200_ERR_ARGUMENT 1   /* null pointer or unsupported mode */
 #define LBFGSB_B200_ERR_CUDA 2       /* a CUDA call failed; see lbfgsb_b200_last_error() */
-#define LBFGSB_B200_ERR_CALLBACK 3   /* reserved */
+#define LBFGSB_B200_ERR_CALLBACK 3   /* a sharded solve's allgather returned nonzero */
 
 /* culbfgsb.h:31 */
 #define LBFGSB_B200_MODE_NO_ACCELERATION 0
@@ -240,7 +240,9 @@ int lbfgsb_b200_minimize_ext_f32(int n, float* x, const int* nbd, const float* l
  * ranks in rank order; a rank may return the whole f and the others 0).  after_iteration and
  * customized_stopping receive the local x and g and the whole f.  ext->trace reports the
  * whole problem's counts (the free-set hash over global indices).  If one rank fails, the
- * others wait in their next allgather: the allgather should carry a timeout. */
+ * others wait in their next allgather: the allgather should carry a timeout.  Sharded
+ * solves are host-driven (this callback API); the device-driven and batched forms run on
+ * one GPU each. */
 typedef int (*lbfgsb_b200_allgather_fn)(void* user, const double* send, double* recv, int count,
                                         void* stream);
 typedef struct {

@@ -684,53 +684,59 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
       const bool leave = track_ && ok && fprev && !fnow;
       const uint32_t newword = __ballot_sync(0xffffffffu, fnow);
       if (!uncon_ && lane == 0 && wi * 32 < valid) c.fbits[t * (kTile / 32) + wi] = newword;
-      if (ok) {
-        // the newest column, selected without a runtime register index
-        const int nw = kFull ? kMaxM - 1 : newest;
-        A ynew = A(0), snew = A(0);
-  #pragma unroll
-        for (int j = 0; j < kMaxM; j++)
-          if (j == nw) {
-            ynew = yv[j];
-            snew = sv[j];
+      // the newest column, selected without a runtime register index
+      const int nw = kFull ? kMaxM - 1 : newest;
+      A ynew = A(0), snew = A(0);
+#pragma unroll
+      for (int j = 0; j < kMaxM; j++)
+        if (j == nw) {
+          ynew = yv[j];
+          snew = sv[j];
+        }
+      // a free variable's sums (cmprlb's r with the W'r sums, the new row over the free set)
+      auto free_elem = [&]() {
+        cnt[0]++;
+        if (hash_) hash += mix64((unsigned long long)(i + c.ioff));
+        const R zi = uncon_ ? xi : gcp_point<R, S>(code, xi, gi, R(0), R(0), tsum);
+        S r = -(S)gi;
+        if (!uncon_) {
+          S ry = -a1[kMaxM] * ((S)zi - (S)xi) - (S)gi, rs = S(0);
+#pragma unroll
+          for (int j = 0; j < kMaxM; j++)
+            if (kFull || j < col) {
+              ry = fma((S)yv[j], a1[j], ry);
+              rs = fma((S)sv[j], a2[j], rs);
+            }
+          r = ry + rs;
+        }
+#pragma unroll
+        for (int j = 0; j < kMaxM; j++) {
+          if (kFull || j < col) {
+            acc[j] = fma(yv[j], (A)r, acc[j]);
+            acc[8 + j] = fma(sv[j], (A)r, acc[8 + j]);
           }
-        if (fnow) {
-          cnt[0]++;
-          if (hash_) hash += mix64((unsigned long long)(i + c.ioff));
-          const R zi = uncon_ ? xi : gcp_point<R, S>(code, xi, gi, R(0), R(0), tsum);
-          S r = -(S)gi;
-          if (!uncon_) {
-            S ry = -a1[kMaxM] * ((S)zi - (S)xi) - (S)gi, rs = S(0);
-  #pragma unroll
-            for (int j = 0; j < kMaxM; j++)
-              if (kFull || j < col) {
-                ry = fma((S)yv[j], a1[j], ry);
-                rs = fma((S)sv[j], a2[j], rs);
-              }
-            r = ry + rs;
-          }
-  #pragma unroll
+        }
+        if (need_row_) {
+#pragma unroll
           for (int j = 0; j < kMaxM; j++) {
             if (kFull || j < col) {
-              acc[j] = fma(yv[j], (A)r, acc[j]);
-              acc[8 + j] = fma(sv[j], (A)r, acc[8 + j]);
+              nrow[j] = fma(ynew, yv[j], nrow[j]);
+              nrow[8 + j] = fma(sv[j], ynew, nrow[8 + j]);
             }
           }
-          if (need_row_) {
-  #pragma unroll
-            for (int j = 0; j < kMaxM; j++) {
-              if (kFull || j < col) {
-                nrow[j] = fma(ynew, yv[j], nrow[j]);
-                nrow[8 + j] = fma(sv[j], ynew, nrow[8 + j]);
-              }
-            }
-          }
+        }
+      };
+      if (F && __all_sync(0xffffffffu, fnow)) {
+        free_elem();  // the steady state: every lane's variable free, no active-set code
+      } else if (ok) {
+        if (fnow) {
+          free_elem();
         } else {
           if (code == IW_LOW || code == IW_WALK_LOW) cnt[3]++;
           if (code == IW_UPP || code == IW_WALK_UPP) cnt[4]++;
           if (need_row_) {
             // columns past col hold zeros and add nothing
-  #pragma unroll
+#pragma unroll
             for (int q = 0; q < 4; q++) {
               float4 v = nra[q * CONS + e];
               const A* src = q < 2 ? sv : yv;
@@ -743,9 +749,9 @@ __device__ __forceinline__ void freev_formk_pass(const Ctx<R, H, S>& c, CtaPos c
             }
           }
         }
-        if (enter) cnt[1]++;
-        if (leave) cnt[2]++;
       }
+      if (enter) cnt[1]++;
+      if (leave) cnt[2]++;
       // entering (+) / leaving (-) variables, as in role 0
       uint32_t pick = __ballot_sync(0xffffffffu, enter || leave);
       while (pick) {
