@@ -142,3 +142,19 @@ def test_sharded_mixed_form(LB, OB):
     assert two.info == one.info
     fa, fb = one.trace[-1]["f"], two.trace[-1]["f"]
     assert abs(fa - fb) / max(1.0, abs(fa)) <= 1e-5
+
+
+def test_one_rank_equals_plain_solve(LB):
+    """A sharded solve of one rank splits every pass into the streaming launch and the
+    one-CTA epilogue launch around an exchange of its own row: the iterates, the trace and
+    the summary equal the plain solve's bit for bit."""
+    prob, dt, x0, over, stop = make_case("synth_s32_f64_b005")
+    a = LB.solve(prob, dt, option=apply_options(LB.default_option(dt), over), objective="host",
+                 trace=True)
+    b = LB.solve_sharded(prob, 1, dt, option=apply_options(LB.default_option(dt), over),
+                         trace=True)
+    assert (a.info, a.num_iteration) == (b.info, b.num_iteration)
+    assert a.residual_g == b.residual_g and a.residual_f == b.residual_f
+    assert np.array_equal(a.x, b.x)
+    for ra, rb in zip(a.trace, b.trace):
+        assert ra == rb, ra["iter"]
