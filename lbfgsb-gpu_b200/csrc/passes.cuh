@@ -277,11 +277,13 @@ __device__ void gcp_epilogue(DevState<S>* st, const double* red, int col, SmallW
   const int col2 = 2 * col;
   const int nbreak = (int)red[17], nfree_mov = (int)red[18];
   if (lane == 0) {
+    #pragma unroll 1
     for (int j = 1; j <= col; j++) {
       st->p[j] = (S)red[j];
       st->p[col + j] = (S)red[8 + j];
     }
     if (theta != S(1))
+      #pragma unroll 1
       for (int j = col + 1; j <= col2; j++) st->p[j] *= theta;
     st->nbreak = nbreak;
     st->nfree_mov = nfree_mov;
@@ -303,6 +305,7 @@ __device__ void gcp_epilogue(DevState<S>* st, const double* red, int col, SmallW
     return;
   }
   if (lane == 0)
+    #pragma unroll 1
     for (int j = 1; j <= col2; j++) st->c[j] = 0;
   S f2 = -theta * f1;
   const S f2org = f2;
@@ -345,6 +348,7 @@ __device__ void gcp_epilogue(DevState<S>* st, const double* red, int col, SmallW
   if (lane == 0) {
     st->dtm = dtm;
     st->tsum = st->tsum + dtm;
+    #pragma unroll 1
     for (int j = 1; j <= col2; j++) st->c[j] += dtm * st->p[j];
   }
   __syncwarp();
@@ -1447,11 +1451,15 @@ __device__ int post_scalar(DevState<S>* st, const double* red, S f, int force_ac
   const int ncol = st->col;
   constexpr int ld = kMaxM;
   if (st->iupdat > m) {
+    #pragma unroll 1
     for (int j = 1; j <= ncol - 1; j++) {
+      #pragma unroll 1
       for (int i = 1; i <= j; i++) LB_AT(st->ss, ld, i, j) = LB_AT(st->ss, ld, i + 1, j + 1);
+      #pragma unroll 1
       for (int i = j; i <= ncol - 1; i++) LB_AT(st->sy, ld, i, j) = LB_AT(st->sy, ld, i + 1, j + 1);
     }
   }
+  #pragma unroll 1
   for (int j = 1; j <= ncol - 1; j++) {
     LB_AT(st->sy, ld, ncol, j) = (S)red[3 + j - 1 + shifted];
     LB_AT(st->ss, ld, j, ncol) = (S)red[11 + j - 1 + shifted];

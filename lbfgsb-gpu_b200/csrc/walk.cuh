@@ -209,6 +209,7 @@ __device__ void walk_sorted(DevState<S>* st, WalkSmem<S>& sm, int cnt, WalkCarry
         st->internal_fail = sm.info;
         sm.done = 2;
       }
+      #pragma unroll 1
       for (int q = 0; q < nb && sm.done == 0; q++) {
         const int k = b0 + q;
         const S tk = (S)__longlong_as_double((long long)sm.k_hi[k]);
@@ -225,6 +226,7 @@ __device__ void walk_sorted(DevState<S>* st, WalkSmem<S>& sm, int cnt, WalkCarry
         pass(k, dibp);
         if (w.nleft == 0 && nbreak == n) {
           w.dtm = dt;
+          #pragma unroll 1
           for (int j = 1; j <= col2; j++) st->c[j] += w.dtm * st->p[j];
           w.all_fixed = true;
           sm.done = 1;
@@ -235,10 +237,12 @@ __device__ void walk_sorted(DevState<S>* st, WalkSmem<S>& sm, int cnt, WalkCarry
         w.f1 = w.f1 + dt * w.f2 + dibp2 - theta * dibp * sm.zibp[q];
         w.f2 = w.f2 - theta * dibp2;
         if (col > 0) {
+          #pragma unroll 1
           for (int j = 1; j <= col2; j++) st->c[j] += dt * st->p[j];
           const S wmc = sdot(&st->c[1], 1, &sm.v[q][1], 1, col2);
           const S wmp = sdot(&st->p[1], 1, &sm.v[q][1], 1, col2);
           const S wmw = sm.wmw[q];
+          #pragma unroll 1
           for (int j = 1; j <= col2; j++) st->p[j] += (-dibp) * sm.wbp[q][j];
           w.f1 = w.f1 + dibp * wmc;
           w.f2 = w.f2 + (S)2.0 * dibp * wmp - dibp2 * wmw;
@@ -283,6 +287,7 @@ __device__ void walk_chunk(const Ctx<R, H, S>& c, const R* __restrict__ x, const
         sm.dibp[q] = (S)dibp;
         sm.zibp[q] = (S)zibp;
         S* wbp = sm.wbp[q];
+        #pragma unroll 1
         for (int j = 0; j < col; j++) {
           wbp[1 + j] = (S)HistTraits<H>::load(Y[j] + i);
           wbp[1 + col + j] = theta * (S)HistTraits<H>::load(Sl[j] + i);
@@ -314,6 +319,7 @@ __device__ __forceinline__ void walk_end(DevState<S>* st, WalkCarry<S>& w, S* wo
   if (!w.all_fixed) {
     if (w.dtm <= S(0)) w.dtm = 0;
     w.tsum = w.tsum + w.dtm;
+    #pragma unroll 1
     for (int j = 1; j <= col2; j++) st->c[j] += w.dtm * st->p[j];
   }
   st->f1 = w.f1;
